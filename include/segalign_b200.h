@@ -1,0 +1,176 @@
+/*
+ * segalign_b200.h — C ABI of the B200 seed-filter path (drop-in for
+ * SegAlign's seed_filter_interface).
+ *
+ * Every entry point mirrors one reference interface (file:line in
+ * thiagogenez/SegAlign) with these deliberate differences:
+ *   - status returns (0 = SA_OK, negative = error, message from
+ *     sa_last_error()) instead of exit()/assert (common/cuda_utils.h:4-37,
+ *     src/seed_filter.cu:660);
+ *   - explicit host pointers instead of the query_DRAM global
+ *     (src/seed_filter.cu:860);
+ *   - results in library-allocated arrays released with sa_free_segments()
+ *     instead of a std::vector returned by value;
+ *   - concurrent sa_seed_and_filter() calls from several host threads each
+ *     take a slot (stream + workspace) from a per-GPU pool, where the
+ *     reference takes a whole GPU (src/seed_filter.cu:667-674).
+ * Records keep the reference layout: sa_segment == segmentPair
+ * (src/graph.h:25-30), element 0 of every SeedAndFilter result is the header
+ * {0, 0, total HSPs, num_hits}.
+ */
+#ifndef SEGALIGN_B200_H
+#define SEGALIGN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    uint32_t ref_start;
+    uint32_t query_start;
+    uint32_t len;
+    int32_t score;
+} sa_segment;
+
+#define SA_OK 0
+#define SA_ERR_ARG -1          /* invalid argument                           */
+#define SA_ERR_STATE -2        /* call order (e.g. no target / table / query)  */
+#define SA_ERR_CUDA -3         /* CUDA runtime error                          */
+#define SA_ERR_NOMEM -4        /* device or host allocation failed            */
+#define SA_ERR_MAX_SEEDS -5    /* more seeds than MAX_SEEDS (ref: assert)      */
+#define SA_ERR_BAD_SEED -6     /* seed key outside the 4^K table              */
+#define SA_ERR_MAX_HITS -7     /* one seed holds >= MAX_HITS hits (ref: UB)   */
+#define SA_ERR_CAPACITY -8     /* survivor workspace exceeded                 */
+#define SA_ERR_NO_DEVICE -9    /* no CUDA device (ref: exit(1))               */
+#define SA_ERR_TOO_MANY_GPUS -10 /* more GPUs requested than present (ref: exit(10)) */
+
+/* ---- device registry and target (common/seed_filter_interface.cu) ---- */
+
+/* InitializeInterface(int num_gpu), common/seed_filter_interface.cu:49-80.
+ * num_gpu = -1 uses every visible GPU.  Returns the GPU count or an error. */
+int sa_initialize_interface(int num_gpu);
+
+/* SendRefWriteRequest(char* seq, size_t start_addr, uint32_t len),
+ * common/seed_filter_interface.cu:82-101: encodes seq[start_addr, +len) and
+ * keeps it resident on every GPU (nibble-packed). */
+int sa_send_ref_write_request(const char* seq, size_t start_addr, uint32_t len);
+
+/* ClearRef(), common/seed_filter_interface.cu:103-113: frees the target and its table. */
+int sa_clear_ref(void);
+
+/* ---- seeds and the target seed-position table ---- */
+
+/* GenerateShapePos(std::string shape), common/ntcoding.cpp:21-37, together
+ * with the shape-name handling of src/main.cpp:152-171: accepts "12of19",
+ * "14of22" or a pattern of 1/0 (or T/0) characters.  Returns K (the number
+ * of sampled positions) or an error.  Default shape: 12of19. */
+int sa_generate_shape_pos(const char* shape);
+
+/* GenerateSeedPosTable(char* ref_str, size_t start_addr, uint32_t ref_length,
+ * uint32_t step, int shape_size, int kmer_size), common/seed_pos_table.cu:49-109.
+ * Built on the GPU from the resident target when (ref_str, start_addr,
+ * ref_length) is what sa_send_ref_write_request() received, else from
+ * ref_str uploaded for the build.  Buckets hold positions in ascending order
+ * (the reference's order inside a bucket is an atomic-add order). */
+int sa_generate_seed_pos_table(const char* ref_str, size_t start_addr, uint32_t ref_length, uint32_t step,
+                               int shape_size, int kmer_size);
+
+/* SendSeedPosTable(uint32_t* index_table, uint32_t index_table_size,
+ * uint32_t* pos_table, uint32_t num_index), common/seed_pos_table.cu:33-47:
+ * uploads a host-built table (index_table[k] = positions with key <= k). */
+int sa_send_seed_pos_table(const uint32_t* index_table, uint32_t index_table_size, const uint32_t* pos_table,
+                           uint32_t num_index);
+
+/* Copy of the resident table of GPU 0 (no reference counterpart; for checks). */
+int sa_get_seed_pos_table(uint32_t* index_table, uint64_t index_cap, uint32_t* pos_table, uint64_t pos_cap,
+                          uint64_t* index_table_size, uint64_t* num_index);
+
+/* ---- seed filter, plain mode (src/seed_filter.cu) ---- */
+
+/* InitializeProcessor(bool transition, uint32_t WGA_CHUNK, uint32_t
+ * input_seed_size, int* sub_mat, int input_xdrop, int input_hspthresh, bool
+ * input_noentropy), src/seed_filter.cu:780-847.  sub_mat is the 8x8 table
+ * (row = target code, column = query code) of src/main.cpp:180-261.
+ * MAX_SEEDS = 13*WGA_CHUNK with transitions else WGA_CHUNK; MAX_HITS as the
+ * reference computes it from the GPU's memory (override: sa_set_max_hits). */
+int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_size, const int* sub_mat, int xdrop,
+                            int hspthresh, int noentropy);
+
+/* SendQueryWriteRequest(size_t start_addr, uint32_t len, uint32_t buffer),
+ * src/seed_filter.cu:849-869.  The reference reads the global
+ * query_DRAM->buffer; here the host block is passed as query_buffer.
+ * Keeps the forward and reverse-complement query of `buffer` resident. */
+int sa_send_query_write_request(const char* query_buffer, size_t start_addr, uint32_t len, uint32_t buffer);
+
+/* SeedAndFilter(std::vector<uint64_t> seed_offset_vector, bool rev, uint32_t
+ * buffer), src/seed_filter.cu:654-778.  seeds are (key << 32) | j words
+ * (src/seeder.cpp:57-74).  *out receives header + HSPs (num_anchors+1
+ * records); free with sa_free_segments().  Thread safe. */
+int sa_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t buffer, sa_segment** out,
+                       uint64_t* out_len);
+
+/* ClearQuery(uint32_t buffer), src/seed_filter.cu:871-880. */
+int sa_clear_query(uint32_t buffer);
+
+/* ShutdownProcessor(), src/seed_filter.cu:882-890.  Frees every device
+ * buffer of the library (the reference calls cudaDeviceReset). */
+int sa_shutdown_processor(void);
+
+/* ---- seed filter, repeat-masker mode (repeat_masker_src/seed_filter.cu) ---- */
+
+/* SendQueryWriteRequest(), repeat_masker_src/seed_filter.cu:925-935: the
+ * query is the resident target; builds its reverse complement. */
+int sa_rm_send_query_write_request(void);
+
+/* SeedAndFilter(seeds, bool rev, uint32_t ref_start, uint32_t ref_end),
+ * repeat_masker_src/seed_filter.cu:723-855.  Hits whose ref_loc is outside
+ * [ref_start, ref_end] are counted but not extended. */
+int sa_rm_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t ref_start, uint32_t ref_end,
+                          sa_segment** out, uint64_t* out_len);
+
+/* ClearQuery(), repeat_masker_src/seed_filter.cu:937-946. */
+int sa_rm_clear_query(void);
+
+/* ---- results, configuration, diagnostics (no reference counterpart) ---- */
+
+void sa_free_segments(sa_segment* segments);
+
+/* MAX_HITS override (src/seed_filter.cu:18,784-791); 0 restores the default. */
+int sa_set_max_hits(uint64_t max_hits);
+
+/* Repeat-masker self alignment: drop forward-strand HSPs on the main
+ * diagonal (ref_start == query_start).  Off by default (the reference never
+ * excludes it). */
+int sa_set_rm_exclude_diagonal(int on);
+
+typedef struct {
+    uint64_t num_seeds;
+    uint64_t num_hits;       /* ungapped extensions (header score)            */
+    uint64_t hits_extended;  /* hits actually extended (rm window)            */
+    uint64_t seeds_with_hits;
+    uint64_t survivors;      /* HSPs kept before dedup                        */
+    uint64_t num_hsps;       /* after dedup                                   */
+    uint64_t long_hits;      /* hits finished by the warp-per-hit kernel       */
+    uint64_t tiles;          /* 32-base tiles the reference would scan          */
+    uint32_t num_iter;       /* MAX_HITS iterations                            */
+    uint32_t pad;
+} sa_call_stats;
+
+/* Statistics of the calling thread's last sa_*seed_and_filter* call. */
+int sa_last_call_stats(sa_call_stats* stats);
+
+/* Message of the calling thread's last error. */
+const char* sa_last_error(void);
+
+/* Tuning knobs of the extension kernels: bases per direction a lane scans
+ * before a hit moves to the warp-per-hit queue, threads per CTA, CTAs per SM,
+ * hits per warp tile.  -1 keeps a value. */
+int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,60 @@
+/*
+ * segalign_b200_host.h — host-side C++ of the seed-filter path behind a C ABI:
+ * query seeding, the scoring table and the multi-threaded seeder pipeline.
+ */
+#ifndef SEGALIGN_B200_HOST_H
+#define SEGALIGN_B200_HOST_H
+
+#include <stdint.h>
+#include "segalign_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Host copy of the seed shape and transition flag used by the seeder
+ * (src/main.cpp:78-80,152-173 with common/ntcoding.cpp:21-37).  Returns K. */
+int sa_host_set_shape(const char* shape, int transition);
+
+/* Seed words of query positions [j0, j1) of `text`, src/seeder.cpp:57-74:
+ * (key << 32) + j for every valid 19-mer window, followed by its K
+ * transition variants when transitions are on.  Writes at most cap words,
+ * returns the full count (call with cap = 0 to size the array). */
+uint64_t sa_host_chunk_seeds(const char* text, uint32_t j0, uint32_t j1, uint64_t* out, uint64_t cap);
+
+/* RevComp, common/ntcoding.cpp:63-105 (characters other than ACGTacgtnN& are
+ * skipped, as in the reference).  Returns the number of characters written. */
+uint64_t sa_host_revcomp(char* dst, const char* src, uint64_t len);
+
+/* Scoring table of src/main.cpp:180-261 (no --scoring file). */
+int sa_build_sub_mat(int xdrop, const char* ambiguous, int* sub_mat);
+
+/* Seeder pipeline over one query block already sent to `buffer`
+ * (src/main.cpp:373-386 intervals of interval_size from 0 to Lq - seed_size;
+ * src/seeder.cpp:47-121 chunks of chunk_size per strand). */
+typedef struct {
+    uint32_t interval_size;    /* 10,000,000 (src/graph.h:11)          */
+    uint32_t interval_overlap; /* extra bases seeded past each interval; 0 in the reference */
+    uint32_t chunk_size;       /* 250,000 (src/graph.h:12)             */
+    int32_t strand;            /* 1 plus, 2 minus, 3 both              */
+    int32_t num_threads;       /* concurrent seeder calls              */
+    uint32_t buffer;           /* query buffer id                      */
+    uint32_t max_chunks;       /* 0 = every chunk; else a bounded sample */
+    uint32_t pad;
+} sa_seeder_cfg;
+
+typedef struct {
+    uint64_t num_seeds;
+    uint64_t num_hits;
+    uint64_t num_hsps;
+    uint64_t num_calls;
+    double seconds;
+} sa_seeder_stats;
+
+int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query_block, uint32_t query_len, sa_segment** fw,
+                  uint64_t* fw_len, sa_segment** rc, uint64_t* rc_len, sa_seeder_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

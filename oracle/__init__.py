@@ -1,0 +1,232 @@
+"""ctypes binding of the CPU oracle (oracle/sa_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs as the checker or the timed CPU
+baseline.  The product path (segalign_b200) never uses it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "build", "libsa_oracle.so")
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libref_ntcoding.so")
+SEGMENT_DTYPE = np.dtype([("ref_start", "<u4"), ("query_start", "<u4"), ("len", "<u4"), ("score", "<i4")])
+_P = C.POINTER
+
+
+class Params(C.Structure):
+    _fields_ = [("sub_mat", C.c_int32 * 64), ("xdrop", C.c_int32), ("hspthresh", C.c_int32),
+                ("noentropy", C.c_int32), ("seed_size", C.c_int32), ("kmer_size", C.c_int32),
+                ("shape_pos", C.c_int32 * 32), ("transition", C.c_int32), ("rm_exclude_diag", C.c_int32),
+                ("max_hits", C.c_uint64)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("hits_extended", C.c_uint64),
+                ("tiles_right", C.c_uint64), ("tiles_left", C.c_uint64), ("survivors", C.c_uint64),
+                ("num_hsps", C.c_uint64), ("unpinned", C.c_uint64), ("base_steps", C.c_uint64),
+                ("num_iter", C.c_int32), ("pad", C.c_int32)]
+
+
+class HitResult(C.Structure):
+    _fields_ = [("right_best", C.c_int32), ("right_pos", C.c_int32), ("left_best", C.c_int32),
+                ("left_pos", C.c_int32), ("total", C.c_int32), ("keep", C.c_int32), ("score", C.c_int32),
+                ("entropy_branch", C.c_int32), ("entropy", C.c_double), ("tiles_right", C.c_uint32),
+                ("tiles_left", C.c_uint32), ("unpinned", C.c_int32), ("pad", C.c_int32)]
+
+
+class PipelineCfg(C.Structure):
+    _fields_ = [("interval_size", C.c_uint32), ("interval_overlap", C.c_uint32), ("chunk_size", C.c_uint32),
+                ("strand", C.c_int32), ("nthreads", C.c_int32), ("max_chunks", C.c_uint32)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        u8p, u32p, u64p = _P(C.c_uint8), _P(C.c_uint32), _P(C.c_uint64)
+        segpp = _P(_P(C.c_uint8))
+        sig = {
+            "or_encode": (None, [C.c_char_p, C.c_uint64, u8p]),
+            "or_encode_rc": (None, [C.c_char_p, C.c_uint64, u8p]),
+            "or_rc_codes": (None, [u8p, C.c_uint64, u8p]),
+            "or_revcomp_text": (C.c_uint64, [C.c_char_p, C.c_char_p, C.c_uint64]),
+            "or_build_sub_mat": (C.c_int, [C.c_int, C.c_char_p, _P(C.c_int32)]),
+            "or_parse_shape": (C.c_int, [C.c_char_p, _P(Params)]),
+            "or_kmer_index": (C.c_uint32, [C.c_char_p, C.c_uint64, _P(Params)]),
+            "or_table_count": (C.c_uint64, [C.c_char_p, C.c_uint32, C.c_uint32, _P(Params)]),
+            "or_build_table": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, _P(Params), u32p, u32p, C.c_uint64, u64p]),
+            "or_chunk_seeds": (C.c_uint64, [C.c_char_p, C.c_uint32, C.c_uint32, _P(Params), u64p, C.c_uint64]),
+            "or_seed_and_filter": (C.c_int, [_P(Params), u8p, C.c_uint32, u8p, C.c_uint32, u32p, u32p, u64p,
+                                             C.c_uint64, C.c_int, C.c_int, C.c_uint32, C.c_uint32, segpp, u64p,
+                                             _P(Stats)]),
+            "or_free": (None, [C.c_void_p]),
+            "or_extend_hit": (None, [_P(Params), u8p, C.c_uint32, u8p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     _P(HitResult)]),
+            "or_pipeline": (C.c_int, [_P(Params), _P(PipelineCfg), C.c_char_p, C.c_uint32, C.c_char_p, C.c_uint32,
+                                      u32p, u32p, segpp, u64p, segpp, u64p, _P(Stats)]),
+            "or_rm_intervals": (C.c_uint64, [_P(SEGSTRUCT := C.c_uint8), C.c_uint64, C.c_uint32, C.c_uint32, u32p,
+                                             u32p, C.c_uint64, u8p]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def ref_ntcoding() -> C.CDLL | None:
+    """The reference's own common/ntcoding.cpp (built by `make -C oracle ref`), or None."""
+    if not os.path.exists(REF_LIB_PATH):
+        return None
+    L = C.CDLL(REF_LIB_PATH)
+    L.ref_generate_shape_pos.restype = C.c_int
+    L.ref_generate_shape_pos.argtypes = [C.c_char_p]
+    L.ref_is_transition_at_pos.restype = C.c_int
+    L.ref_is_transition_at_pos.argtypes = [C.c_int]
+    L.ref_get_kmer_index_at_pos.restype = C.c_uint32
+    L.ref_get_kmer_index_at_pos.argtypes = [C.c_char_p, C.c_size_t, C.c_uint32]
+    L.ref_revcomp.restype = None
+    L.ref_revcomp.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t, C.c_size_t, C.c_size_t]
+    return L
+
+
+def params(xdrop=910, hspthresh=3000, noentropy=False, shape="12of19", transition=False, ambiguous="",
+           max_hits=1 << 40, rm_exclude_diag=False) -> Params:
+    p = Params()
+    L = lib()
+    if L.or_build_sub_mat(xdrop, ambiguous.encode(), p.sub_mat) != 0:
+        raise ValueError("bad ambiguous")
+    if L.or_parse_shape(shape.encode(), C.byref(p)) < 0:
+        raise ValueError("bad shape")
+    p.xdrop, p.hspthresh, p.noentropy = xdrop, hspthresh, int(noentropy)
+    p.transition, p.max_hits, p.rm_exclude_diag = int(transition), max_hits, int(rm_exclude_diag)
+    return p
+
+
+def encode(text: bytes) -> np.ndarray:
+    out = np.empty(len(text), dtype=np.uint8)
+    lib().or_encode(text, len(text), out.ctypes.data_as(_P(C.c_uint8)))
+    return out
+
+
+def encode_rc(text: bytes) -> np.ndarray:
+    out = np.empty(len(text), dtype=np.uint8)
+    lib().or_encode_rc(text, len(text), out.ctypes.data_as(_P(C.c_uint8)))
+    return out
+
+
+def rc_codes(codes: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(codes, dtype=np.uint8)
+    out = np.empty_like(c)
+    lib().or_rc_codes(c.ctypes.data_as(_P(C.c_uint8)), len(c), out.ctypes.data_as(_P(C.c_uint8)))
+    return out
+
+
+def revcomp_text(text: bytes) -> bytes:
+    dst = C.create_string_buffer(len(text))
+    n = lib().or_revcomp_text(dst, text, len(text))
+    return dst.raw[:n]
+
+
+def sub_mat(xdrop=910, ambiguous="") -> np.ndarray:
+    m = (C.c_int32 * 64)()
+    if lib().or_build_sub_mat(xdrop, ambiguous.encode(), m) != 0:
+        raise ValueError("bad ambiguous")
+    return np.array(list(m), dtype=np.int32)
+
+
+def build_table(text: bytes, p: Params, step: int = 1):
+    L = lib()
+    n = L.or_table_count(text, len(text), step, C.byref(p))
+    idx = np.zeros(1 << (2 * p.kmer_size), dtype=np.uint32)
+    pos = np.zeros(max(n, 1), dtype=np.uint32)
+    ni = C.c_uint64()
+    r = L.or_build_table(text, len(text), step, C.byref(p), idx.ctypes.data_as(_P(C.c_uint32)),
+                         pos.ctypes.data_as(_P(C.c_uint32)), len(pos), C.byref(ni))
+    assert r == 0
+    return idx, pos[: ni.value]
+
+
+def chunk_seeds(text: bytes, j0: int, j1: int, p: Params) -> np.ndarray:
+    L = lib()
+    n = L.or_chunk_seeds(text, j0, j1, C.byref(p), None, 0)
+    out = np.empty(max(n, 1), dtype=np.uint64)
+    L.or_chunk_seeds(text, j0, j1, C.byref(p), out.ctypes.data_as(_P(C.c_uint64)), n)
+    return out[:n]
+
+
+def _segs(ptr, n):
+    try:
+        if n == 0:
+            return np.zeros(0, dtype=SEGMENT_DTYPE)
+        buf = C.cast(ptr, _P(C.c_uint8 * (16 * n))).contents
+        return np.frombuffer(bytes(buf), dtype=SEGMENT_DTYPE).copy()
+    finally:
+        lib().or_free(ptr)
+
+
+def seed_and_filter(p: Params, ref_codes: np.ndarray, query_codes: np.ndarray, index: np.ndarray, pos: np.ndarray,
+                    seeds: np.ndarray, rev: bool, mode: int = 0, rm_ref_start: int = 0, rm_ref_end: int = 0):
+    """Returns (segments with header, stats dict); raises on an oracle error code."""
+    L = lib()
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    ptr, n, st = _P(C.c_uint8)(), C.c_uint64(), Stats()
+    r = L.or_seed_and_filter(C.byref(p), ref_codes.ctypes.data_as(_P(C.c_uint8)), len(ref_codes),
+                             query_codes.ctypes.data_as(_P(C.c_uint8)), len(query_codes),
+                             index.ctypes.data_as(_P(C.c_uint32)), pos.ctypes.data_as(_P(C.c_uint32)),
+                             s.ctypes.data_as(_P(C.c_uint64)), len(s), int(rev), mode, rm_ref_start, rm_ref_end,
+                             C.byref(ptr), C.byref(n), C.byref(st))
+    if r != 0:
+        raise RuntimeError(f"oracle seed_and_filter error {r}")
+    return _segs(ptr, n.value), {k: getattr(st, k) for k, _ in Stats._fields_ if k != "pad"}
+
+
+def extend_hit(p: Params, ref_codes, query_codes, ref_loc: int, query_loc: int) -> dict:
+    h = HitResult()
+    lib().or_extend_hit(C.byref(p), ref_codes.ctypes.data_as(_P(C.c_uint8)), len(ref_codes),
+                        query_codes.ctypes.data_as(_P(C.c_uint8)), len(query_codes), ref_loc, query_loc, C.byref(h))
+    return {k: getattr(h, k) for k, _ in HitResult._fields_ if k != "pad"}
+
+
+def pipeline(p: Params, ref_text: bytes, query_text: bytes, index, pos, strand=3, nthreads=1,
+             interval_size=10_000_000, chunk_size=250_000, interval_overlap=0, max_chunks=0):
+    """Seeder pipeline over one query block (src/seeder.cpp:47-121) -> (fw, rc, stats)."""
+    L = lib()
+    cfg = PipelineCfg(interval_size, interval_overlap, chunk_size, strand, nthreads, max_chunks)
+    fw, fl, rc, rl, st = _P(C.c_uint8)(), C.c_uint64(), _P(C.c_uint8)(), C.c_uint64(), Stats()
+    r = L.or_pipeline(C.byref(p), C.byref(cfg), ref_text, len(ref_text), query_text, len(query_text),
+                      index.ctypes.data_as(_P(C.c_uint32)), pos.ctypes.data_as(_P(C.c_uint32)), C.byref(fw),
+                      C.byref(fl), C.byref(rc), C.byref(rl), C.byref(st))
+    if r != 0:
+        raise RuntimeError(f"oracle pipeline error {r}")
+    return _segs(fw, fl.value), _segs(rc, rl.value), {k: getattr(st, k) for k, _ in Stats._fields_ if k != "pad"}
+
+
+def rm_intervals(hsps: np.ndarray, block_len: int, M: int):
+    """repeat_masker_src/seeder.cpp:151-186 coverage runs -> (starts, lens)."""
+    L = lib()
+    h = np.ascontiguousarray(hsps, dtype=SEGMENT_DTYPE)
+    cnt = np.zeros(block_len, dtype=np.uint8)
+    n = L.or_rm_intervals(h.ctypes.data_as(_P(C.c_uint8)), len(h), block_len, M, None, None, 0,
+                          cnt.ctypes.data_as(_P(C.c_uint8)))
+    st = np.zeros(max(n, 1), dtype=np.uint32)
+    ln = np.zeros(max(n, 1), dtype=np.uint32)
+    L.or_rm_intervals(h.ctypes.data_as(_P(C.c_uint8)), len(h), block_len, M, st.ctypes.data_as(_P(C.c_uint32)),
+                      ln.ctypes.data_as(_P(C.c_uint32)), n, cnt.ctypes.data_as(_P(C.c_uint8)))
+    return st[:n], ln[:n]

@@ -1,0 +1,305 @@
+"""segalign_b200 — B200-native seed-filter path of SegAlign behind its C ABI.
+
+The compute path is the CUDA library ``libsegalign_b200.so`` (kernels for
+sm_100a + host C++).  This module is a thin ctypes binding that mirrors the
+reference's ``seed_filter_interface`` call sequence (src/main.cpp:290-291,
+606-674; src/seeder.cpp:78,113):
+
+    sf = SeedFilter()
+    sf.initialize_interface(-1)                       # InitializeInterface
+    sf.generate_shape_pos("12of19")                  # GenerateShapePos
+    sf.initialize_processor(transition, 250000, 19, sub_mat, 910, 3000, False)
+    sf.send_ref_write_request(target_text)           # SendRefWriteRequest
+    sf.generate_seed_pos_table(target_text, 1, 19, 12)   # GenerateSeedPosTable
+    sf.send_query_write_request(query_text, 0)       # SendQueryWriteRequest
+    hsps = sf.seed_and_filter(seeds, rev, 0)         # SeedAndFilter
+    ...
+
+There is no CPU fallback: importing works without a GPU, but every call that
+computes needs the CUDA library and a device, and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsegalign_b200.so")
+
+SEGMENT_DTYPE = np.dtype([("ref_start", "<u4"), ("query_start", "<u4"), ("len", "<u4"), ("score", "<i4")])
+
+SA_OK = 0
+ERRORS = {
+    -1: "SA_ERR_ARG", -2: "SA_ERR_STATE", -3: "SA_ERR_CUDA", -4: "SA_ERR_NOMEM", -5: "SA_ERR_MAX_SEEDS",
+    -6: "SA_ERR_BAD_SEED", -7: "SA_ERR_MAX_HITS", -8: "SA_ERR_CAPACITY", -9: "SA_ERR_NO_DEVICE",
+    -10: "SA_ERR_TOO_MANY_GPUS",
+}
+
+# Every entry point of include/segalign_b200.h and include/segalign_b200_host.h.
+EXPORTS = [
+    "sa_initialize_interface", "sa_send_ref_write_request", "sa_clear_ref", "sa_generate_shape_pos",
+    "sa_generate_seed_pos_table", "sa_send_seed_pos_table", "sa_get_seed_pos_table", "sa_initialize_processor",
+    "sa_send_query_write_request", "sa_seed_and_filter", "sa_clear_query", "sa_shutdown_processor",
+    "sa_rm_send_query_write_request", "sa_rm_seed_and_filter", "sa_rm_clear_query", "sa_free_segments",
+    "sa_set_max_hits", "sa_set_rm_exclude_diagonal", "sa_last_call_stats", "sa_last_error", "sa_set_tuning",
+    "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
+]
+
+
+class SegAlignError(RuntimeError):
+    def __init__(self, code: int, fn: str, msg: str):
+        super().__init__(f"{fn} -> {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class CallStats(C.Structure):
+    _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("hits_extended", C.c_uint64),
+                ("seeds_with_hits", C.c_uint64), ("survivors", C.c_uint64), ("num_hsps", C.c_uint64),
+                ("long_hits", C.c_uint64), ("tiles", C.c_uint64), ("num_iter", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class SeederCfg(C.Structure):
+    _fields_ = [("interval_size", C.c_uint32), ("interval_overlap", C.c_uint32), ("chunk_size", C.c_uint32),
+                ("strand", C.c_int32), ("num_threads", C.c_int32), ("buffer", C.c_uint32),
+                ("max_chunks", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class SeederStats(C.Structure):
+    _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
+                ("num_calls", C.c_uint64), ("seconds", C.c_double)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+_P = C.POINTER
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m segalign_b200._build` "
+                               "(there is no CPU fallback)")
+        lib = C.CDLL(path)
+        u64p, u32p, i32p = _P(C.c_uint64), _P(C.c_uint32), _P(C.c_int32)
+        segpp = _P(_P(C.c_uint8))
+        sig = {
+            "sa_initialize_interface": (C.c_int, [C.c_int]),
+            "sa_send_ref_write_request": (C.c_int, [C.c_char_p, C.c_size_t, C.c_uint32]),
+            "sa_clear_ref": (C.c_int, []),
+            "sa_generate_shape_pos": (C.c_int, [C.c_char_p]),
+            "sa_generate_seed_pos_table": (C.c_int, [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_int, C.c_int]),
+            "sa_send_seed_pos_table": (C.c_int, [u32p, C.c_uint32, u32p, C.c_uint32]),
+            "sa_get_seed_pos_table": (C.c_int, [u32p, C.c_uint64, u32p, C.c_uint64, u64p, u64p]),
+            "sa_initialize_processor": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, i32p, C.c_int, C.c_int, C.c_int]),
+            "sa_send_query_write_request": (C.c_int, [C.c_char_p, C.c_size_t, C.c_uint32, C.c_uint32]),
+            "sa_seed_and_filter": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, segpp, u64p]),
+            "sa_clear_query": (C.c_int, [C.c_uint32]),
+            "sa_shutdown_processor": (C.c_int, []),
+            "sa_rm_send_query_write_request": (C.c_int, []),
+            "sa_rm_seed_and_filter": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32, segpp, u64p]),
+            "sa_rm_clear_query": (C.c_int, []),
+            "sa_free_segments": (None, [_P(C.c_uint8)]),
+            "sa_set_max_hits": (C.c_int, [C.c_uint64]),
+            "sa_set_rm_exclude_diagonal": (C.c_int, [C.c_int]),
+            "sa_last_call_stats": (C.c_int, [_P(CallStats)]),
+            "sa_last_error": (C.c_char_p, []),
+            "sa_set_tuning": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+            "sa_host_set_shape": (C.c_int, [C.c_char_p, C.c_int]),
+            "sa_host_chunk_seeds": (C.c_uint64, [C.c_char_p, C.c_uint32, C.c_uint32, u64p, C.c_uint64]),
+            "sa_host_revcomp": (C.c_uint64, [C.c_char_p, C.c_char_p, C.c_uint64]),
+            "sa_build_sub_mat": (C.c_int, [C.c_int, C.c_char_p, i32p]),
+            "sa_seeder_run": (C.c_int, [_P(SeederCfg), C.c_char_p, C.c_uint32, segpp, u64p, segpp, u64p,
+                                        _P(SeederStats)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+        return lib
+
+
+def _u64p(a: np.ndarray):
+    return a.ctypes.data_as(_P(C.c_uint64))
+
+
+def _u32p(a: np.ndarray):
+    return a.ctypes.data_as(_P(C.c_uint32))
+
+
+def _bytes(text) -> bytes:
+    if isinstance(text, np.ndarray):
+        return text.tobytes()
+    if isinstance(text, str):
+        return text.encode("ascii")
+    return bytes(text)
+
+
+def build_sub_mat(xdrop: int = 910, ambiguous: str = "") -> np.ndarray:
+    """Scoring table of src/main.cpp:180-261 (C++ host code)."""
+    lib = load_library()
+    m = np.zeros(64, dtype=np.int32)
+    r = lib.sa_build_sub_mat(xdrop, ambiguous.encode(), m.ctypes.data_as(_P(C.c_int32)))
+    if r != SA_OK:
+        raise SegAlignError(r, "sa_build_sub_mat", "bad ambiguous string")
+    return m
+
+
+def host_seeds(text: bytes, j0: int, j1: int, shape: str = "12of19", transition: bool = False) -> np.ndarray:
+    """Seed words of query positions [j0, j1) (src/seeder.cpp:57-74), computed by the C++ host seeder."""
+    lib = load_library()
+    lib.sa_host_set_shape(shape.encode(), int(transition))
+    n = lib.sa_host_chunk_seeds(text, j0, j1, None, 0)
+    out = np.empty(max(n, 1), dtype=np.uint64)
+    lib.sa_host_chunk_seeds(text, j0, j1, _u64p(out), n)
+    return out[:n]
+
+
+def host_revcomp(text: bytes) -> bytes:
+    lib = load_library()
+    dst = C.create_string_buffer(len(text))
+    n = lib.sa_host_revcomp(dst, text, len(text))
+    return dst.raw[:n]
+
+
+def _take_segments(lib, ptr, n) -> np.ndarray:
+    try:
+        if n == 0:
+            return np.zeros(0, dtype=SEGMENT_DTYPE)
+        buf = C.cast(ptr, _P(C.c_uint8 * (16 * n))).contents
+        return np.frombuffer(bytes(buf), dtype=SEGMENT_DTYPE).copy()
+    finally:
+        lib.sa_free_segments(ptr)
+
+
+class SeedFilter:
+    """Mirror of the reference seed_filter_interface over the C ABI."""
+
+    def __init__(self):
+        self.lib = load_library()
+
+    def _chk(self, r: int, fn: str) -> int:
+        if r < 0:
+            raise SegAlignError(r, fn, (self.lib.sa_last_error() or b"").decode())
+        return r
+
+    # ---- common/seed_filter_interface.cu ----
+    def initialize_interface(self, num_gpu: int = -1) -> int:
+        return self._chk(self.lib.sa_initialize_interface(num_gpu), "InitializeInterface")
+
+    def send_ref_write_request(self, seq, start_addr: int = 0, length: int | None = None) -> None:
+        self._ref = _bytes(seq)
+        n = len(self._ref) - start_addr if length is None else length
+        self._chk(self.lib.sa_send_ref_write_request(self._ref, start_addr, n), "SendRefWriteRequest")
+        self._ref_args = (start_addr, n)
+
+    def clear_ref(self) -> None:
+        self._chk(self.lib.sa_clear_ref(), "ClearRef")
+
+    # ---- seeds and table ----
+    def generate_shape_pos(self, shape: str = "12of19") -> int:
+        return self._chk(self.lib.sa_generate_shape_pos(shape.encode()), "GenerateShapePos")
+
+    def generate_seed_pos_table(self, ref=None, step: int = 1, shape_size: int = 19, kmer_size: int = 12,
+                                start_addr: int | None = None, length: int | None = None) -> None:
+        if ref is None:
+            ref = self._ref
+            s, n = self._ref_args
+        else:
+            ref = _bytes(ref)
+            if ref == getattr(self, "_ref", None):
+                ref = self._ref  # same host buffer -> build from the resident target
+            s = 0 if start_addr is None else start_addr
+            n = len(ref) - s if length is None else length
+        self._chk(self.lib.sa_generate_seed_pos_table(ref, s, n, step, shape_size, kmer_size), "GenerateSeedPosTable")
+
+    def send_seed_pos_table(self, index_table: np.ndarray, pos_table: np.ndarray) -> None:
+        it = np.ascontiguousarray(index_table, dtype=np.uint32)
+        pt = np.ascontiguousarray(pos_table, dtype=np.uint32)
+        self._chk(self.lib.sa_send_seed_pos_table(_u32p(it), len(it), _u32p(pt), len(pt)), "SendSeedPosTable")
+
+    def get_seed_pos_table(self):
+        nb, ni = C.c_uint64(), C.c_uint64()
+        self._chk(self.lib.sa_get_seed_pos_table(None, 0, None, 0, C.byref(nb), C.byref(ni)), "GetSeedPosTable")
+        it = np.empty(nb.value, dtype=np.uint32)
+        pt = np.empty(max(ni.value, 1), dtype=np.uint32)
+        self._chk(self.lib.sa_get_seed_pos_table(_u32p(it), nb.value, _u32p(pt), ni.value, None, None),
+                  "GetSeedPosTable")
+        return it, pt[: ni.value]
+
+    # ---- src/seed_filter.cu ----
+    def initialize_processor(self, transition: bool, wga_chunk: int, seed_size: int, sub_mat, xdrop: int,
+                             hspthresh: int, noentropy: bool) -> None:
+        m = np.ascontiguousarray(sub_mat, dtype=np.int32)
+        self._chk(self.lib.sa_initialize_processor(int(transition), wga_chunk, seed_size,
+                                                   m.ctypes.data_as(_P(C.c_int32)), xdrop, hspthresh,
+                                                   int(noentropy)), "InitializeProcessor")
+
+    def send_query_write_request(self, query, buffer: int = 0, start_addr: int = 0, length: int | None = None):
+        q = _bytes(query)
+        n = len(q) - start_addr if length is None else length
+        self._chk(self.lib.sa_send_query_write_request(q, start_addr, n, buffer), "SendQueryWriteRequest")
+
+    def seed_and_filter(self, seeds: np.ndarray, rev: bool, buffer: int = 0) -> np.ndarray:
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        ptr, n = _P(C.c_uint8)(), C.c_uint64()
+        self._chk(self.lib.sa_seed_and_filter(_u64p(s), len(s), int(rev), buffer, C.byref(ptr), C.byref(n)),
+                  "SeedAndFilter")
+        return _take_segments(self.lib, ptr, n.value)
+
+    def clear_query(self, buffer: int = 0) -> None:
+        self._chk(self.lib.sa_clear_query(buffer), "ClearQuery")
+
+    def shutdown_processor(self) -> None:
+        self._chk(self.lib.sa_shutdown_processor(), "ShutdownProcessor")
+
+    # ---- repeat_masker_src/seed_filter.cu ----
+    def rm_send_query_write_request(self) -> None:
+        self._chk(self.lib.sa_rm_send_query_write_request(), "SendQueryWriteRequest(rm)")
+
+    def rm_seed_and_filter(self, seeds: np.ndarray, rev: bool, ref_start: int, ref_end: int) -> np.ndarray:
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        ptr, n = _P(C.c_uint8)(), C.c_uint64()
+        self._chk(self.lib.sa_rm_seed_and_filter(_u64p(s), len(s), int(rev), ref_start, ref_end, C.byref(ptr),
+                                                 C.byref(n)), "SeedAndFilter(rm)")
+        return _take_segments(self.lib, ptr, n.value)
+
+    def rm_clear_query(self) -> None:
+        self._chk(self.lib.sa_rm_clear_query(), "ClearQuery(rm)")
+
+    # ---- configuration / diagnostics ----
+    def set_max_hits(self, n: int) -> None:
+        self._chk(self.lib.sa_set_max_hits(n), "set_max_hits")
+
+    def set_rm_exclude_diagonal(self, on: bool) -> None:
+        self._chk(self.lib.sa_set_rm_exclude_diagonal(int(on)), "set_rm_exclude_diagonal")
+
+    def set_tuning(self, lane_cap=-1, ext_block=-1, ext_ctas_per_sm=-1, tile_hits=-1) -> None:
+        self._chk(self.lib.sa_set_tuning(lane_cap, ext_block, ext_ctas_per_sm, tile_hits), "set_tuning")
+
+    def last_call_stats(self) -> dict:
+        st = CallStats()
+        self.lib.sa_last_call_stats(C.byref(st))
+        return {k: getattr(st, k) for k, _ in CallStats._fields_ if k != "pad"}
+
+    def seeder_run(self, query, buffer: int = 0, strand: int = 3, num_threads: int = 4,
+                   interval_size: int = 10_000_000, chunk_size: int = 250_000, interval_overlap: int = 0,
+                   max_chunks: int = 0, shape: str = "12of19", transition: bool = False):
+        """Seeder pipeline over one query block (src/seeder.cpp:12-127) in C++ host threads."""
+        q = _bytes(query)
+        self.lib.sa_host_set_shape(shape.encode(), int(transition))
+        cfg = SeederCfg(interval_size, interval_overlap, chunk_size, strand, num_threads, buffer, max_chunks, 0)
+        fw, fl, rc, rl = _P(C.c_uint8)(), C.c_uint64(), _P(C.c_uint8)(), C.c_uint64()
+        st = SeederStats()
+        self._chk(self.lib.sa_seeder_run(C.byref(cfg), q, len(q), C.byref(fw), C.byref(fl), C.byref(rc),
+                                         C.byref(rl), C.byref(st)), "seeder_run")
+        f = _take_segments(self.lib, fw, fl.value)
+        r = _take_segments(self.lib, rc, rl.value)
+        return f, r, {k: getattr(st, k) for k, _ in SeederStats._fields_}

@@ -1,0 +1,852 @@
+// sa_api.cu — C ABI of the B200 seed-filter path: device registry, resident
+// target / table / query buffers, the slot pool and the per-call pipeline.
+//
+// Reference interfaces (file:line) are cited at each entry point and in
+// include/segalign_b200.h.  Differences from the reference: status codes in
+// place of exit(); a pool of slots (stream + workspace) per GPU in place of
+// one lock per GPU; host pointers in place of the query_DRAM global.
+#include <algorithm>
+#include <condition_variable>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/segalign_b200.h"
+#include "sa_launch.h"
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+static thread_local std::string t_err;
+static thread_local sa_call_stats t_stats;
+
+void sa_set_error(int, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_err = buf;
+}
+
+int sa_cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    sa_set_error(SA_ERR_CUDA, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    return e == cudaErrorMemoryAllocation ? SA_ERR_NOMEM : SA_ERR_CUDA;
+}
+
+#define SA_TRY(expr)                   \
+    do {                               \
+        int _r = (expr);               \
+        if (_r != SA_OK) return _r;    \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// State
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kMaxBuffers = 8;
+
+struct Packed {
+    uint32_t* base = nullptr;  // allocation (with padding)
+    uint32_t* data = nullptr;  // word 0
+    uint64_t len = 0;
+    void release() {
+        if (base) cudaFree(base);
+        base = data = nullptr;
+        len = 0;
+    }
+};
+
+struct Slot;
+
+struct DevState {
+    int dev = 0;
+    int num_sms = 148;
+    uint64_t total_mem = 0;
+    Packed ref, ref_rc;
+    uint32_t* index = nullptr;
+    uint64_t nbuckets = 0;
+    uint32_t* pos = nullptr;
+    uint64_t num_index = 0;
+    Packed qf[kMaxBuffers], qr[kMaxBuffers];
+    std::vector<Slot*> slots;
+};
+
+struct Slot {
+    int dev_idx = 0;
+    cudaStream_t stream = nullptr;
+    SaWork w{};
+    void* arena = nullptr;  // one device allocation carved into the workspace
+    SaCounters* h_ctr = nullptr;
+    SaCallDesc* h_desc = nullptr;
+    SaUnit* h_units = nullptr;
+    uint32_t* h_scope_flags = nullptr;
+    uint32_t* h_scope_count = nullptr;
+    SaRec* h_out = nullptr;
+    uint64_t h_out_cap = 0;
+};
+
+struct Global {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Slot*> free_slots;
+    std::vector<DevState> devs;
+    bool interface_ready = false;
+    bool processor_ready = false;
+    // shape (common/ntcoding.cpp globals)
+    SaParams params{};
+    bool shape_set = false;
+    // processor configuration
+    uint32_t wga_chunk = 250000;
+    uint64_t max_seeds = 0;
+    uint64_t max_hits_override = 0;
+    uint64_t max_hits_default = 0;
+    int rm_exclude_diag = 0;
+    SaTuning tuning{64, 256, 4, 256, 296, 1024};
+    // last target upload (to reuse it for the table build)
+    const char* last_ref_ptr = nullptr;
+    size_t last_ref_start = 0;
+    uint32_t last_ref_len = 0;
+    uint32_t ref_len = 0;
+    uint64_t surv_cap = 0;
+    uint64_t long_cap = 0;
+};
+
+Global& G() {
+    static Global g;
+    return g;
+}
+
+uint64_t env_u64(const char* name, uint64_t dflt) {
+    const char* v = getenv(name);
+    if (!v || !*v) return dflt;
+    return strtoull(v, nullptr, 10);
+}
+
+// Default 12of19 shape (src/main.cpp:153-156).
+void set_shape_positions(SaParams& p, const std::string& shape) {
+    int k = 0;
+    for (size_t i = 0; i < shape.size(); ++i)
+        if (shape[i] == '1' || shape[i] == 'T') p.shape_pos[k++] = (int)i;
+    p.kmer_size = k;
+    p.seed_size = (int)shape.size();
+}
+
+int alloc_packed(Packed& pk, uint64_t len) {
+    pk.release();
+    uint64_t nw = (len + 7) / 8 + 2 * SA_PADW;
+    SA_CUDA_OK(cudaMalloc(&pk.base, nw * sizeof(uint32_t)));
+    pk.data = pk.base + SA_PADW;
+    pk.len = len;
+    return SA_OK;
+}
+
+// Uploads text[0, len) and packs it into pk (and its reverse complement into rc if given).
+int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed* rc) {
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    SA_TRY(alloc_packed(pk, len));
+    if (rc) SA_TRY(alloc_packed(*rc, len));
+    uint64_t nw = (len + 7) / 8 + 2 * SA_PADW;
+    sa_launch_pad_fill(pk.base, nw, 0);
+    if (rc) sa_launch_pad_fill(rc->base, nw, 0);
+    char* d_text = nullptr;
+    const uint64_t chunk = 1ull << 28;  // 256 MiB text per round
+    SA_CUDA_OK(cudaMalloc(&d_text, std::min<uint64_t>(len ? len : 1, chunk) + 16));
+    for (uint64_t off = 0; off < len; off += chunk) {
+        uint64_t n = std::min(chunk, len - off);
+        cudaError_t e = cudaMemcpy(d_text, text + off, n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(d_text);
+            return sa_cuda_fail(e, "cudaMemcpy(text)", __FILE__, __LINE__);
+        }
+        // chunk is a multiple of 8 bases, so word boundaries line up
+        sa_launch_pack_text(d_text, n, pk.data + off / 8, 0);
+    }
+    if (rc) sa_launch_rc_packed(pk.data, len, rc->data, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(d_text);
+    if (e != cudaSuccess) return sa_cuda_fail(e, "pack", __FILE__, __LINE__);
+    return SA_OK;
+}
+
+void free_slot(Slot* s) {
+    if (!s) return;
+    cudaSetDevice(s->dev_idx >= 0 ? G().devs[s->dev_idx].dev : 0);
+    if (s->arena) cudaFree(s->arena);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->h_ctr) cudaFreeHost(s->h_ctr);
+    if (s->h_desc) cudaFreeHost(s->h_desc);
+    if (s->h_units) cudaFreeHost(s->h_units);
+    if (s->h_scope_flags) cudaFreeHost(s->h_scope_flags);
+    if (s->h_scope_count) cudaFreeHost(s->h_scope_count);
+    if (s->h_out) cudaFreeHost(s->h_out);
+    delete s;
+}
+
+// Carves one slot workspace out of a single device allocation.
+int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_cap, Slot** out) {
+    DevState& d = G().devs[dev_idx];
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    Slot* s = new Slot();
+    s->dev_idx = dev_idx;
+    struct Part {
+        void** ptr;
+        uint64_t bytes;
+    };
+    SaWork& w = s->w;
+    w.seed_cap = seed_cap;
+    w.surv_cap = surv_cap;
+    w.long_cap = long_cap;
+    std::vector<Part> parts = {
+        {(void**)&w.seeds, 8 * seed_cap},
+        {(void**)&w.s_lo, 4 * seed_cap},
+        {(void**)&w.s_cnt, 4 * seed_cap},
+        {(void**)&w.s_P, 8 * seed_cap},
+        {(void**)&w.cs.E, 8 * (seed_cap + 1)},
+        {(void**)&w.cs.lo, 4 * (seed_cap + 1)},
+        {(void**)&w.cs.qpos, 4 * (seed_cap + 1)},
+        {(void**)&w.cs.scope, 4 * (seed_cap + 1)},
+        {(void**)&w.cs.unit, 4 * (seed_cap + 1)},
+        {(void**)&w.cta_a, 8 * SA_MAX_CTAS},
+        {(void**)&w.cta_b, 8 * SA_MAX_CTAS},
+        {(void**)&w.limits, 8 * SA_MAX_ITERS},
+        {(void**)&w.long_q, sizeof(SaLongHit) * long_cap},
+        {(void**)&w.rec[0], sizeof(SaRec) * surv_cap},
+        {(void**)&w.rec[1], sizeof(SaRec) * surv_cap},
+        {(void**)&w.scope[0], 4 * surv_cap},
+        {(void**)&w.scope[1], 4 * surv_cap},
+        {(void**)&w.out, sizeof(SaRec) * surv_cap},
+        {(void**)&w.out_scope, 4 * surv_cap},
+        {(void**)&w.scope_count, 4 * SA_MAX_SCOPES},
+        {(void**)&w.scope_flags, 4 * SA_MAX_SCOPES},
+        {(void**)&w.sort_hist, 4 * 256 * SA_SORT_MAX_DIGITS},
+        {(void**)&w.sort_cta_hist, 4 * 256 * (uint64_t)SA_MAX_CTAS + 4 * 64},
+        {(void**)&w.sort_in_buf, 4 * (SA_SORT_MAX_DIGITS + 2)},
+        {(void**)&w.ctr, sizeof(SaCounters)},
+        {(void**)&w.desc, sizeof(SaCallDesc)},
+        {(void**)&w.units, sizeof(SaUnit) * 64},
+    };
+    w.flags = nullptr;
+    w.bunits = nullptr;
+    uint64_t total = 0;
+    for (auto& p : parts) total += (p.bytes + 255) & ~255ull;
+    cudaError_t e = cudaMalloc(&s->arena, total);
+    if (e != cudaSuccess) {
+        delete s;
+        return sa_cuda_fail(e, "cudaMalloc(slot workspace)", __FILE__, __LINE__);
+    }
+    char* at = (char*)s->arena;
+    for (auto& p : parts) {
+        *p.ptr = at;
+        at += (p.bytes + 255) & ~255ull;
+    }
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&s->h_ctr, sizeof(SaCounters)) != cudaSuccess ||
+        cudaMallocHost(&s->h_desc, sizeof(SaCallDesc)) != cudaSuccess ||
+        cudaMallocHost(&s->h_units, sizeof(SaUnit) * 64) != cudaSuccess ||
+        cudaMallocHost(&s->h_scope_flags, 4 * SA_MAX_ITERS) != cudaSuccess ||
+        cudaMallocHost(&s->h_scope_count, 4 * SA_MAX_ITERS) != cudaSuccess) {
+        free_slot(s);
+        sa_set_error(SA_ERR_NOMEM, "pinned host allocation failed");
+        return SA_ERR_NOMEM;
+    }
+    *out = s;
+    return SA_OK;
+}
+
+Slot* acquire_slot() {
+    Global& g = G();
+    std::unique_lock<std::mutex> lk(g.mu);
+    g.cv.wait(lk, [&] { return !g.free_slots.empty(); });
+    Slot* s = g.free_slots.front();
+    g.free_slots.pop_front();
+    return s;
+}
+
+void release_slot(Slot* s) {
+    Global& g = G();
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        g.free_slots.push_back(s);
+    }
+    g.cv.notify_one();
+}
+
+int map_device_error(unsigned long long e) {
+    switch (e) {
+        case 0: return SA_OK;
+        case 1: sa_set_error(SA_ERR_BAD_SEED, "seed key outside the 4^K seed table"); return SA_ERR_BAD_SEED;
+        case 2: sa_set_error(SA_ERR_MAX_HITS, "a single seed has at least MAX_HITS hits"); return SA_ERR_MAX_HITS;
+        case 3: sa_set_error(SA_ERR_MAX_HITS, "more than %d MAX_HITS iterations", SA_MAX_ITERS); return SA_ERR_MAX_HITS;
+        case 4: sa_set_error(SA_ERR_CAPACITY, "survivor workspace exceeded (raise SA_SURV_CAP)"); return SA_ERR_CAPACITY;
+        case 5: sa_set_error(SA_ERR_BAD_SEED, "hit coordinates past the end of the target or query"); return SA_ERR_BAD_SEED;
+        default: sa_set_error(SA_ERR_CUDA, "device error %llu", e); return SA_ERR_CUDA;
+    }
+}
+
+uint64_t max_hits_now() {
+    Global& g = G();
+    return g.max_hits_override ? g.max_hits_override : g.max_hits_default;
+}
+
+// One SeedAndFilter call on a slot: seeds -> hits -> X-drop -> dedup -> host.
+// mode 0 = plain, 1 = repeat masker.
+int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& q, int mode, uint32_t rm_lo,
+             uint32_t rm_hi, sa_segment** out, uint64_t* out_len) {
+    Global& g = G();
+    DevState& d = g.devs[s->dev_idx];
+    SaWork& w = s->w;
+    cudaStream_t st = s->stream;
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
+    // descriptor, unit, scope flags
+    SaCallDesc* hd = s->h_desc;
+    hd->num_seeds = n;
+    hd->max_hits = max_hits_now();
+    hd->num_units = 1;
+    hd->num_scopes_max = SA_MAX_ITERS;
+    hd->rm_exclude_diag = (uint32_t)g.rm_exclude_diag;
+    SaUnit* u = s->h_units;
+    u[0].q_packed = q.data;
+    u[0].q_len = (uint32_t)q.len;
+    u[0].rm_lo = rm_lo;
+    u[0].rm_hi = rm_hi;
+    u[0].flags = mode == 1 ? (1u | (rev ? 2u : 0u)) : 0u;
+    for (int i = 0; i < SA_MAX_ITERS; ++i)
+        s->h_scope_flags[i] = (rev ? 1u : 0u) | ((mode == 1 && g.rm_exclude_diag) ? 2u : 0u);
+    SA_CUDA_OK(cudaMemcpyAsync(w.seeds, seeds, 8ull * n, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.desc, hd, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.units, u, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
+    sa_launch_lookup_seeds(w, d.index, (uint32_t)d.nbuckets, g.params, Gr, st);
+    SaExtendArgs xa;
+    xa.ref = d.ref.data;
+    xa.ref_len = (uint32_t)d.ref.len;
+    xa.pos_table = d.pos;
+    xa.seed_size = (uint32_t)g.params.seed_size;
+    xa.xdrop = g.params.xdrop;
+    xa.hspthresh = g.params.hspthresh;
+    xa.noentropy = g.params.noentropy;
+    sa_launch_extend(w, xa, g.params, g.tuning, d.num_sms, st);
+    sa_launch_dedup(w, mode, Gr, st);
+    SA_CUDA_OK(cudaGetLastError());
+    SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
+    SA_CUDA_OK(cudaStreamSynchronize(st));
+    SaCounters c = *s->h_ctr;
+    std::memset(&t_stats, 0, sizeof t_stats);
+    t_stats.num_seeds = n;
+    t_stats.num_hits = c.num_hits;
+    t_stats.hits_extended = c.extended;
+    t_stats.seeds_with_hits = c.nnz;
+    t_stats.survivors = c.surv_count;
+    t_stats.num_hsps = c.uniq_count;
+    t_stats.long_hits = c.long_count;
+    t_stats.tiles = c.base_steps;
+    t_stats.num_iter = (uint32_t)c.num_iter;
+    if (c.error) return map_device_error(c.error);
+    const uint64_t nh = c.uniq_count;
+    if (nh + 1 > s->h_out_cap) {
+        if (s->h_out) cudaFreeHost(s->h_out);
+        s->h_out = nullptr;
+        uint64_t cap = std::max<uint64_t>(nh + 1, 1 << 16);
+        cap = std::max(cap, s->h_out_cap * 2);
+        SA_CUDA_OK(cudaMallocHost(&s->h_out, cap * sizeof(SaRec)));
+        s->h_out_cap = cap;
+    }
+    if (nh) SA_CUDA_OK(cudaMemcpyAsync(s->h_out + 1, w.out, nh * sizeof(SaRec), cudaMemcpyDeviceToHost, st));
+    SA_CUDA_OK(cudaStreamSynchronize(st));
+    // header (src/seed_filter.cu:756-759): len = total anchors, score = num_hits
+    s->h_out[0].ref_start = 0;
+    s->h_out[0].query_start = 0;
+    s->h_out[0].len = (uint32_t)nh;
+    s->h_out[0].score = (int32_t)(uint32_t)c.num_hits;
+    sa_segment* res = (sa_segment*)malloc((nh + 1) * sizeof(sa_segment));
+    if (!res) {
+        sa_set_error(SA_ERR_NOMEM, "host allocation of %llu records failed", (unsigned long long)(nh + 1));
+        return SA_ERR_NOMEM;
+    }
+    std::memcpy(res, s->h_out, (nh + 1) * sizeof(sa_segment));
+    *out = res;
+    *out_len = nh + 1;
+    return SA_OK;
+}
+
+int check_ready(bool need_query) {
+    Global& g = G();
+    if (!g.interface_ready) {
+        sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
+        return SA_ERR_STATE;
+    }
+    if (!g.processor_ready) {
+        sa_set_error(SA_ERR_STATE, "sa_initialize_processor() has not been called");
+        return SA_ERR_STATE;
+    }
+    for (auto& d : g.devs) {
+        if (!d.ref.data || !d.index || !d.pos) {
+            sa_set_error(SA_ERR_STATE, "no resident target and seed table");
+            return SA_ERR_STATE;
+        }
+    }
+    (void)need_query;
+    return SA_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* sa_last_error(void) { return t_err.c_str(); }
+
+int sa_last_call_stats(sa_call_stats* s) {
+    if (!s) return SA_ERR_ARG;
+    *s = t_stats;
+    return SA_OK;
+}
+
+// common/seed_filter_interface.cu:49-80
+int sa_initialize_interface(int num_gpu) {
+    Global& g = G();
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        sa_set_error(SA_ERR_NO_DEVICE, "no GPU device found");
+        return SA_ERR_NO_DEVICE;
+    }
+    int use = num_gpu == -1 ? n : num_gpu;
+    if (use < 1) {
+        sa_set_error(SA_ERR_ARG, "num_gpu must be -1 or >= 1");
+        return SA_ERR_ARG;
+    }
+    if (use > n) {
+        sa_set_error(SA_ERR_TOO_MANY_GPUS, "requested %d GPUs, %d available", use, n);
+        return SA_ERR_TOO_MANY_GPUS;
+    }
+    if (g.interface_ready) sa_shutdown_processor();
+    int cur = 0;
+    cudaGetDevice(&cur);
+    g.devs.assign(use, DevState());
+    for (int i = 0; i < use; ++i) {
+        // with one GPU in use, keep the caller's current device
+        g.devs[i].dev = use == 1 ? cur : i;
+        cudaDeviceProp prop;
+        SA_CUDA_OK(cudaGetDeviceProperties(&prop, g.devs[i].dev));
+        g.devs[i].num_sms = prop.multiProcessorCount;
+        g.devs[i].total_mem = prop.totalGlobalMem;
+    }
+    if (!g.shape_set) {
+        set_shape_positions(g.params, "TTT0T00TT00T0T0TTTT");
+        g.shape_set = true;
+    }
+    g.interface_ready = true;
+    return use;
+}
+
+// common/ntcoding.cpp:21-37 + src/main.cpp:152-171
+int sa_generate_shape_pos(const char* shape) {
+    if (!shape) return SA_ERR_ARG;
+    std::string name = shape, pat;
+    if (name == "12of19") pat = "TTT0T00TT00T0T0TTTT";
+    else if (name == "14of22") pat = "TTT0T0TT00TT00T0T0TTTT";
+    else {
+        pat = name;
+        for (auto& c : pat) c = (c == '1' || c == 'T') ? 'T' : '0';
+    }
+    int k = 0;
+    for (char c : pat) k += c == 'T';
+    if (k > 15 || k <= 3 || pat.size() > 32) {
+        sa_set_error(SA_ERR_ARG, "shape must have 4..15 sampled positions and span <= 32 (got K=%d, span=%zu)", k,
+                     pat.size());
+        return SA_ERR_ARG;
+    }
+    Global& g = G();
+    set_shape_positions(g.params, pat);
+    g.shape_set = true;
+    return k;
+}
+
+// common/seed_filter_interface.cu:82-101
+int sa_send_ref_write_request(const char* seq, size_t start_addr, uint32_t len) {
+    Global& g = G();
+    if (!g.interface_ready) {
+        sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
+        return SA_ERR_STATE;
+    }
+    if (!seq) return SA_ERR_ARG;
+    for (auto& d : g.devs) SA_TRY(upload_pack(d, seq + start_addr, len, d.ref, nullptr));
+    g.last_ref_ptr = seq;
+    g.last_ref_start = start_addr;
+    g.last_ref_len = len;
+    g.ref_len = len;
+    return SA_OK;
+}
+
+// common/seed_filter_interface.cu:103-113
+int sa_clear_ref(void) {
+    Global& g = G();
+    for (auto& d : g.devs) {
+        cudaSetDevice(d.dev);
+        d.ref.release();
+        d.ref_rc.release();
+        if (d.index) cudaFree(d.index);
+        if (d.pos) cudaFree(d.pos);
+        d.index = d.pos = nullptr;
+        d.nbuckets = d.num_index = 0;
+    }
+    g.last_ref_ptr = nullptr;
+    return SA_OK;
+}
+
+static int build_table_on(DevState& d, const Packed& ref, uint32_t step) {
+    Global& g = G();
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    const SaParams& p = g.params;
+    // common/seed_pos_table.cu:58-64: offset, start, num_steps
+    uint32_t offset = (uint32_t)(p.seed_size + 1) % step;
+    uint32_t start = step - offset;
+    int64_t span = (int64_t)ref.len - p.seed_size + offset;
+    uint64_t num_steps = span > 0 ? (uint64_t)span / step : 0;
+    uint64_t nb = 1ull << (2 * p.kmer_size);
+    uint64_t cap = num_steps ? num_steps : 1;
+    uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr;
+    unsigned long long* scratch = nullptr;
+    unsigned int* hist = nullptr;
+    auto cleanup = [&]() {
+        if (keys) cudaFree(keys);
+        if (vals) cudaFree(vals);
+        if (keys2) cudaFree(keys2);
+        if (vals2) cudaFree(vals2);
+        if (scratch) cudaFree(scratch);
+        if (hist) cudaFree(hist);
+    };
+    cudaError_t e = cudaSuccess;
+    if ((e = cudaMalloc(&keys, 4 * cap)) != cudaSuccess || (e = cudaMalloc(&vals, 4 * cap)) != cudaSuccess ||
+        (e = cudaMalloc(&keys2, 4 * cap)) != cudaSuccess || (e = cudaMalloc(&vals2, 4 * cap)) != cudaSuccess ||
+        (e = cudaMalloc(&scratch, 8 * (2 * SA_MAX_CTAS + 4))) != cudaSuccess ||
+        (e = cudaMalloc(&hist, 4 * (256 * (uint64_t)SA_MAX_CTAS + 64))) != cudaSuccess) {
+        cleanup();
+        return sa_cuda_fail(e, "cudaMalloc(table build)", __FILE__, __LINE__);
+    }
+    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
+    unsigned long long* cta_a = scratch;
+    unsigned long long* cta_b = scratch + SA_MAX_CTAS;
+    unsigned long long* d_total = scratch + 2 * SA_MAX_CTAS;
+    cudaMemset(d_total, 0, 8);
+    sa_launch_table_keys(ref.data, start, num_steps, step, p, keys, vals, cta_a, cta_b, d_total, Gr, 0);
+    int in_tmp = 0;
+    sa_launch_sort_kv(keys, vals, keys2, vals2, d_total, 2 * p.kmer_size, hist, Gr, 0, &in_tmp);
+    unsigned long long n_valid = 0;
+    e = cudaMemcpy(&n_valid, d_total, 8, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cleanup();
+        return sa_cuda_fail(e, "table build", __FILE__, __LINE__);
+    }
+    if (d.index) cudaFree(d.index);
+    if (d.pos) cudaFree(d.pos);
+    d.index = d.pos = nullptr;
+    if ((e = cudaMalloc(&d.index, 4 * nb)) != cudaSuccess) {
+        cleanup();
+        return sa_cuda_fail(e, "cudaMalloc(index table)", __FILE__, __LINE__);
+    }
+    uint32_t* sk = in_tmp ? keys2 : keys;
+    uint32_t* sv = in_tmp ? vals2 : vals;
+    sa_launch_table_index(sk, d_total, d.index, nb, 0);
+    // keep the sorted positions as the position table; free the rest
+    d.pos = sv;
+    if (sv == vals) vals = nullptr;
+    else vals2 = nullptr;
+    e = cudaDeviceSynchronize();
+    cleanup();
+    if (e != cudaSuccess) return sa_cuda_fail(e, "table build", __FILE__, __LINE__);
+    d.nbuckets = nb;
+    d.num_index = n_valid;
+    return SA_OK;
+}
+
+// common/seed_pos_table.cu:49-109
+int sa_generate_seed_pos_table(const char* ref_str, size_t start_addr, uint32_t ref_length, uint32_t step,
+                               int shape_size, int kmer_size) {
+    Global& g = G();
+    if (!g.interface_ready) {
+        sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
+        return SA_ERR_STATE;
+    }
+    if (step == 0 || shape_size != g.params.seed_size || kmer_size != g.params.kmer_size) {
+        sa_set_error(SA_ERR_ARG, "step must be >= 1 and shape_size/kmer_size must match the shape (%d/%d)",
+                     g.params.seed_size, g.params.kmer_size);
+        return SA_ERR_ARG;
+    }
+    const bool resident = ref_str == g.last_ref_ptr && start_addr == g.last_ref_start &&
+                          ref_length == g.last_ref_len && g.last_ref_ptr;
+    for (auto& d : g.devs) {
+        if (resident && d.ref.data) {
+            SA_TRY(build_table_on(d, d.ref, step));
+        } else {
+            if (!ref_str) return SA_ERR_ARG;
+            Packed tmp;
+            SA_TRY(upload_pack(d, ref_str + start_addr, ref_length, tmp, nullptr));
+            int r = build_table_on(d, tmp, step);
+            tmp.release();
+            if (r != SA_OK) return r;
+        }
+    }
+    return SA_OK;
+}
+
+// common/seed_pos_table.cu:33-47
+int sa_send_seed_pos_table(const uint32_t* index_table, uint32_t index_table_size, const uint32_t* pos_table,
+                           uint32_t num_index) {
+    Global& g = G();
+    if (!g.interface_ready) return SA_ERR_STATE;
+    if (!index_table || (num_index && !pos_table)) return SA_ERR_ARG;
+    if (index_table_size != (1ull << (2 * g.params.kmer_size)) || index_table[index_table_size - 1] != num_index) {
+        sa_set_error(SA_ERR_ARG, "index table must have 4^K = %llu entries ending at num_index",
+                     1ull << (2 * g.params.kmer_size));
+        return SA_ERR_ARG;
+    }
+    for (uint32_t i = 0; i < num_index; ++i)
+        if ((uint64_t)pos_table[i] + (uint64_t)g.params.seed_size > g.ref_len) {
+            sa_set_error(SA_ERR_ARG, "position %u of the table lies past the target end", pos_table[i]);
+            return SA_ERR_ARG;
+        }
+    for (auto& d : g.devs) {
+        SA_CUDA_OK(cudaSetDevice(d.dev));
+        if (d.index) cudaFree(d.index);
+        if (d.pos) cudaFree(d.pos);
+        d.index = d.pos = nullptr;
+        SA_CUDA_OK(cudaMalloc(&d.index, 4ull * index_table_size));
+        SA_CUDA_OK(cudaMemcpy(d.index, index_table, 4ull * index_table_size, cudaMemcpyHostToDevice));
+        SA_CUDA_OK(cudaMalloc(&d.pos, 4ull * (num_index ? num_index : 1)));
+        if (num_index) SA_CUDA_OK(cudaMemcpy(d.pos, pos_table, 4ull * num_index, cudaMemcpyHostToDevice));
+        d.nbuckets = index_table_size;
+        d.num_index = num_index;
+    }
+    return SA_OK;
+}
+
+int sa_get_seed_pos_table(uint32_t* index_table, uint64_t index_cap, uint32_t* pos_table, uint64_t pos_cap,
+                          uint64_t* index_table_size, uint64_t* num_index) {
+    Global& g = G();
+    if (g.devs.empty() || !g.devs[0].index) return SA_ERR_STATE;
+    DevState& d = g.devs[0];
+    if (index_table_size) *index_table_size = d.nbuckets;
+    if (num_index) *num_index = d.num_index;
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    if (index_table && index_cap >= d.nbuckets)
+        SA_CUDA_OK(cudaMemcpy(index_table, d.index, 4 * d.nbuckets, cudaMemcpyDeviceToHost));
+    if (pos_table && pos_cap >= d.num_index && d.num_index)
+        SA_CUDA_OK(cudaMemcpy(pos_table, d.pos, 4 * d.num_index, cudaMemcpyDeviceToHost));
+    return SA_OK;
+}
+
+// src/seed_filter.cu:780-847
+int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_size, const int* sub_mat, int xdrop,
+                            int hspthresh, int noentropy) {
+    Global& g = G();
+    if (!g.interface_ready) {
+        sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
+        return SA_ERR_STATE;
+    }
+    if (!sub_mat || wga_chunk == 0 || (int)seed_size != g.params.seed_size) {
+        sa_set_error(SA_ERR_ARG, "sub_mat required, wga_chunk > 0, seed_size must equal the shape span (%d)",
+                     g.params.seed_size);
+        return SA_ERR_ARG;
+    }
+    // release old slots
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        for (auto* s : g.free_slots) free_slot(s);
+        g.free_slots.clear();
+        for (auto& d : g.devs) d.slots.clear();
+    }
+    for (int i = 0; i < 64; ++i) g.params.sub_mat[i] = sub_mat[i];
+    g.params.xdrop = xdrop;
+    g.params.hspthresh = hspthresh;
+    g.params.noentropy = noentropy ? 1 : 0;
+    g.params.transition = transition ? 1 : 0;
+    g.wga_chunk = wga_chunk;
+    g.max_seeds = transition ? 13ull * wga_chunk : wga_chunk;  // :786-789
+    // MAX_HITS = MAX_HITS_PER_GB * (float)(totalGlobalMem / 1 GiB) (:784, :791)
+    float gb = (float)(g.devs[0].total_mem / 1073741824.0f);
+    g.max_hits_default = (uint64_t)(int)(4194304 * gb);
+    g.surv_cap = env_u64("SA_SURV_CAP", 1ull << 25);
+    g.long_cap = env_u64("SA_LONG_CAP", 1ull << 24);
+    const int per_gpu = (int)env_u64("SA_SLOTS_PER_GPU", 2);
+    for (size_t di = 0; di < g.devs.size(); ++di) {
+        for (int k = 0; k < per_gpu; ++k) {
+            Slot* s = nullptr;
+            SA_TRY(make_slot((int)di, g.max_seeds, g.surv_cap, g.long_cap, &s));
+            std::lock_guard<std::mutex> lk(g.mu);
+            g.devs[di].slots.push_back(s);
+            g.free_slots.push_back(s);
+        }
+    }
+    g.processor_ready = true;
+    return SA_OK;
+}
+
+// src/seed_filter.cu:849-869
+int sa_send_query_write_request(const char* query_buffer, size_t start_addr, uint32_t len, uint32_t buffer) {
+    Global& g = G();
+    if (!g.interface_ready) return SA_ERR_STATE;
+    if (!query_buffer || buffer >= (uint32_t)kMaxBuffers) {
+        sa_set_error(SA_ERR_ARG, "query buffer pointer required and buffer < %d", kMaxBuffers);
+        return SA_ERR_ARG;
+    }
+    for (auto& d : g.devs) SA_TRY(upload_pack(d, query_buffer + start_addr, len, d.qf[buffer], &d.qr[buffer]));
+    return SA_OK;
+}
+
+// src/seed_filter.cu:654-778
+int sa_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t buffer, sa_segment** out,
+                       uint64_t* out_len) {
+    SA_TRY(check_ready(true));
+    Global& g = G();
+    if (!out || !out_len || (num_seeds && !seeds) || buffer >= (uint32_t)kMaxBuffers) return SA_ERR_ARG;
+    if (num_seeds > g.max_seeds) {
+        sa_set_error(SA_ERR_MAX_SEEDS, "%u seeds exceed MAX_SEEDS = %llu", num_seeds,
+                     (unsigned long long)g.max_seeds);
+        return SA_ERR_MAX_SEEDS;
+    }
+    Slot* s = acquire_slot();
+    DevState& d = g.devs[s->dev_idx];
+    const Packed& q = rev ? d.qr[buffer] : d.qf[buffer];
+    int r;
+    if (!q.data) {
+        sa_set_error(SA_ERR_STATE, "query buffer %u is not resident", buffer);
+        r = SA_ERR_STATE;
+    } else {
+        r = run_call(s, seeds, num_seeds, rev, q, 0, 0, 0, out, out_len);
+    }
+    release_slot(s);
+    return r;
+}
+
+// src/seed_filter.cu:871-880
+int sa_clear_query(uint32_t buffer) {
+    Global& g = G();
+    if (buffer >= (uint32_t)kMaxBuffers) return SA_ERR_ARG;
+    for (auto& d : g.devs) {
+        cudaSetDevice(d.dev);
+        d.qf[buffer].release();
+        d.qr[buffer].release();
+    }
+    return SA_OK;
+}
+
+// repeat_masker_src/seed_filter.cu:925-935
+int sa_rm_send_query_write_request(void) {
+    Global& g = G();
+    for (auto& d : g.devs) {
+        if (!d.ref.data) {
+            sa_set_error(SA_ERR_STATE, "no resident target");
+            return SA_ERR_STATE;
+        }
+        SA_CUDA_OK(cudaSetDevice(d.dev));
+        SA_TRY(alloc_packed(d.ref_rc, d.ref.len));
+        sa_launch_pad_fill(d.ref_rc.base, (d.ref.len + 7) / 8 + 2 * SA_PADW, 0);
+        sa_launch_rc_packed(d.ref.data, d.ref.len, d.ref_rc.data, 0);
+        SA_CUDA_OK(cudaDeviceSynchronize());
+    }
+    return SA_OK;
+}
+
+// repeat_masker_src/seed_filter.cu:723-855
+int sa_rm_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t ref_start, uint32_t ref_end,
+                          sa_segment** out, uint64_t* out_len) {
+    SA_TRY(check_ready(false));
+    Global& g = G();
+    if (!out || !out_len || (num_seeds && !seeds)) return SA_ERR_ARG;
+    if (num_seeds > g.max_seeds) {
+        sa_set_error(SA_ERR_MAX_SEEDS, "%u seeds exceed MAX_SEEDS", num_seeds);
+        return SA_ERR_MAX_SEEDS;
+    }
+    Slot* s = acquire_slot();
+    DevState& d = g.devs[s->dev_idx];
+    const Packed& q = rev ? d.ref_rc : d.ref;
+    int r;
+    if (!q.data) {
+        sa_set_error(SA_ERR_STATE, "sa_rm_send_query_write_request() has not been called");
+        r = SA_ERR_STATE;
+    } else {
+        r = run_call(s, seeds, num_seeds, rev, q, 1, ref_start, ref_end, out, out_len);
+    }
+    release_slot(s);
+    return r;
+}
+
+// repeat_masker_src/seed_filter.cu:937-946
+int sa_rm_clear_query(void) {
+    Global& g = G();
+    for (auto& d : g.devs) {
+        cudaSetDevice(d.dev);
+        d.ref_rc.release();
+    }
+    return SA_OK;
+}
+
+// src/seed_filter.cu:882-890 (without cudaDeviceReset: only this library's buffers are freed)
+int sa_shutdown_processor(void) {
+    Global& g = G();
+    {
+        std::lock_guard<std::mutex> lk(g.mu);
+        for (auto& d : g.devs)
+            for (auto* s : d.slots) free_slot(s);
+        g.free_slots.clear();
+        for (auto& d : g.devs) d.slots.clear();
+    }
+    for (auto& d : g.devs) {
+        cudaSetDevice(d.dev);
+        for (int b = 0; b < kMaxBuffers; ++b) {
+            d.qf[b].release();
+            d.qr[b].release();
+        }
+    }
+    sa_clear_ref();
+    g.processor_ready = false;
+    return SA_OK;
+}
+
+void sa_free_segments(sa_segment* p) { free(p); }
+
+int sa_set_max_hits(uint64_t max_hits) {
+    G().max_hits_override = max_hits;
+    return SA_OK;
+}
+
+int sa_set_rm_exclude_diagonal(int on) {
+    G().rm_exclude_diag = on ? 1 : 0;
+    return SA_OK;
+}
+
+int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits) {
+    SaTuning& t = G().tuning;
+    if (lane_cap >= 0) {
+        if (lane_cap % 8 || lane_cap < 8) return SA_ERR_ARG;
+        t.lane_cap = lane_cap;
+    }
+    if (ext_block >= 0) {
+        if (ext_block % 32 || ext_block > 1024 || ext_block < 64) return SA_ERR_ARG;
+        t.ext_block = ext_block;
+    }
+    if (ext_ctas_per_sm >= 0) {
+        if (ext_ctas_per_sm < 1 || ext_ctas_per_sm > 16) return SA_ERR_ARG;
+        t.ext_ctas_per_sm = ext_ctas_per_sm;
+    }
+    if (tile_hits >= 0) {
+        if (tile_hits < 32) return SA_ERR_ARG;
+        t.tile_hits = tile_hits;
+    }
+    return SA_OK;
+}
+
+}  // extern "C"

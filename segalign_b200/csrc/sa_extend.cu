@@ -1,0 +1,555 @@
+// sa_extend.cu — ungapped X-drop extension of every seed hit, HSP keep/score
+// (entropy adjustment) and survivor compaction.
+//
+// Reference: find_hsps (src/seed_filter.cu:204-624; repeat-masker variant
+// repeat_masker_src/seed_filter.cu:249-688) and compress_output (:626-652;
+// rm :690-721).  The reference runs one warp per hit over 32-base tiles with
+// four shuffle scans per tile.  Its result does not depend on the tile width.
+// For each direction it is defined per position:
+//   S(o) = running score, M(o) = max(0, max S up to o),
+//   stop at the first o with M(o) - S(o) > xdrop or at the sequence edge,
+//   best = max over o < stop, pos = first o reaching best (right: -1 if
+//   best == 0; left: 0).
+// This file computes the same quantities in two phases:
+//   phase A (sa_k_extend_lane): one hit per lane.  A warp keeps its 32 lanes
+//     busy by handing out the next hits of its tile, in order, to lanes that
+//     finish ("refill").  Hits are expanded on the fly from the compacted seed
+//     list.  The short random-hit extensions that dominate the hit count
+//     finish here in one or two 8-base steps.
+//   phase B (sa_k_extend_warp): hits whose extension passes `lane_cap` bases in
+//     one direction move to a queue and are redone by one warp per hit,
+//     256 bases per step.  Each lane scans 8 bases; warp scans carry the
+//     running sum and maximum.
+// Survivors are appended with warp-aggregated atomics, together with their
+// dedup scope.
+#include <climits>
+
+#include "sa_launch.h"
+#include "sa_radix.cuh"
+
+#define SA_FULL 0xffffffffu
+
+struct SaExtK {
+    const uint32_t* ref;
+    uint32_t ref_len;
+    const uint32_t* pos_table;
+    SaSeedList cs;
+    const SaUnit* units;
+    SaCounters* ctr;
+    SaLongHit* long_q;
+    uint64_t long_cap;
+    SaRec* surv;
+    uint32_t* surv_scope;
+    uint64_t surv_cap;
+    uint32_t seed_size;
+    int32_t xdrop, hspthresh, noentropy;
+    uint32_t lane_cap;
+    uint32_t tile_hits;
+};
+
+// Reverse the order of the 8 nibbles of a word.
+__device__ __forceinline__ uint32_t sa_rev_nibbles(uint32_t x) {
+    x = __byte_perm(x, 0, 0x0123);
+    return ((x >> 4) & 0x0f0f0f0fu) | ((x & 0x0f0f0f0fu) << 4);
+}
+
+// Largest compacted seed c in [0, nnz) with E[c] <= h (E strictly increasing,
+// E[0] == 0 <= h).  Warp-cooperative 32-ary search; all lanes get the result.
+__device__ __forceinline__ uint64_t sa_warp_find_seed(const uint64_t* __restrict__ E, uint64_t nnz, uint64_t h) {
+    const int lane = threadIdx.x & 31;
+    uint64_t lo = 0, hi = nnz;
+    while (hi - lo > 32) {
+        uint64_t step = (hi - lo + 31) / 32;
+        uint64_t probe = lo + (uint64_t)lane * step;
+        bool ok = probe < hi && E[probe] <= h;
+        uint32_t m = __ballot_sync(SA_FULL, ok);
+        uint64_t k = 31 - __clz(m);
+        uint64_t nlo = lo + k * step;
+        hi = (nlo + step < hi) ? nlo + step : hi;
+        lo = nlo;
+    }
+    uint64_t probe = lo + lane;
+    bool ok = probe < hi && E[probe] <= h;
+    uint32_t m = __ballot_sync(SA_FULL, ok);
+    return lo + (31 - __clz(m));
+}
+
+// Entropy factor and keep/score of one HSP (src/seed_filter.cu:580-621).
+// c[] are the match counts per base over the HSP, already summed.
+__device__ __forceinline__ void sa_keep_score(int total, int ext, const int* cnt, bool entropy_branch,
+                                              int hspthresh, int* keep, int* score) {
+    double E = 1.0;  // entropy[warp_id] = 1.0f
+    if (entropy_branch) {
+        short c0 = (short)cnt[0], c1 = (short)cnt[1], c2 = (short)cnt[2], c3 = (short)cnt[3];
+        if ((int)c0 + (int)c1 + (int)c2 + (int)c3 >= 20) {
+            double n = (double)(ext + 1);
+            double e = 0.0;
+            short cs[4] = {c0, c1, c2, c3};
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                double q = (double)cs[b] / n;
+                double lg = (cs[b] != 0) ? log((double)cs[b] / n) : 0.0;
+                e = fma(q, lg, e);
+            }
+            E = -e / (double)logf(4.0f);
+        }
+    }
+    *keep = (int)(((double)(float)total) * E) >= hspthresh;
+    *score = E > 0 ? (int)((double)total * E) : 0;
+}
+
+__device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
+    return !a.noentropy && total >= a.hspthresh && total <= 3 * a.hspthresh;
+}
+
+// ---------------------------------------------------------------------------
+// Phase A: one hit per lane with in-order warp refill.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256, 4)
+sa_k_extend_lane(SaExtK a, SaParams P) {
+    __shared__ int sub[64];
+    if (threadIdx.x < 64) sub[threadIdx.x] = P.sub_mat[threadIdx.x];
+    __syncthreads();
+    if (a.ctr->error) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = sa_lanemask_lt();
+    const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
+    const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
+    const int xdrop = a.xdrop;
+
+    uint64_t tile_next = 0, tile_end = 0, cur = 0;
+    bool exhausted = (H == 0);
+
+    bool has = false, nocap = false;
+    uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0, uflags = 0, qlen = 0;
+    const uint32_t* qp = a.ref;
+    int dir = 0;
+    uint32_t o = 0, avail = 0;
+    int S = 0, best = 0, bpos = -1, Rbest = 0, Rpos = -1;
+    uint32_t tiles = 0;
+    unsigned long long tiles_acc = 0, ext_acc = 0;
+
+    while (true) {
+        // ---- refill lanes without a hit, in hit order ----
+        uint32_t need = __ballot_sync(SA_FULL, !has);
+        while (need && !exhausted) {
+            if (tile_next >= tile_end) {
+                unsigned long long t0 = 0;
+                if (lane == 0) t0 = atomicAdd(&a.ctr->hit_cursor, (unsigned long long)a.tile_hits);
+                t0 = __shfl_sync(SA_FULL, t0, 0);
+                if (t0 >= H) {
+                    exhausted = true;
+                    break;
+                }
+                tile_next = t0;
+                tile_end = (t0 + a.tile_hits < H) ? t0 + a.tile_hits : H;
+                cur = sa_warp_find_seed(a.cs.E, nnz, t0);
+            }
+            const uint64_t left_in_tile = tile_end - tile_next;
+            const uint32_t m = min((uint32_t)__popc(need), (uint32_t)(left_in_tile < 32 ? left_in_tile : 32));
+            const uint32_t rank = __popc(need & lt);
+            const bool take = !has && rank < m;
+            const uint64_t h = tile_next + rank;
+            // The m hits span at most m consecutive compacted seeds from `cur`.
+            const uint64_t Ew = (cur + lane < nnz) ? a.cs.E[cur + lane] : ~0ull;
+            int k = 0;
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1) {
+                uint64_t v = __shfl_sync(SA_FULL, Ew, k + s);
+                if (v <= h) k += s;
+            }
+            const uint64_t Ek = __shfl_sync(SA_FULL, Ew, k);
+            const uint32_t lm = __ballot_sync(SA_FULL, Ew <= tile_next + m - 1);
+            const uint64_t newcur = cur + (31 - __clz(lm));
+            if (take) {
+                const uint64_t c = cur + k;
+                const uint32_t t = a.cs.lo[c] + (uint32_t)(h - Ek);
+                rl = __ldg(a.pos_table + t) + seed_size;   // find_hits :192
+                ql = a.cs.qpos[c] + seed_size;            // find_hits :176
+                scope = a.cs.scope[c];
+                unit_id = a.cs.unit[c];
+                const SaUnit U = a.units[unit_id];
+                qp = U.q_packed;
+                qlen = U.q_len;
+                uflags = U.flags;
+                // rm: hits outside [ref_start, ref_end] are never extended
+                // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
+                bool skip = (uflags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+                // Coordinates past either sequence end (a caller-supplied
+                // table or seed beyond the sequences) are rejected, not read.
+                if (rl > ref_len || ql > qlen) {
+                    atomicCAS(&a.ctr->error, 0ull, 5ull);
+                    skip = true;
+                }
+                if (!skip) {
+                    has = true;
+                    nocap = false;
+                    dir = 0;
+                    o = 0;
+                    S = 0;
+                    best = 0;
+                    bpos = -1;
+                    tiles = 0;
+                    avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
+                    ++ext_acc;
+                }
+            }
+            tile_next += m;
+            cur = newcur;
+            need = __ballot_sync(SA_FULL, !has);
+        }
+        if (!__any_sync(SA_FULL, has)) break;
+
+        // ---- one 8-base step per busy lane ----
+        bool finished = false, to_long = false;
+        int keep = 0, score = 0, Lpos = 0;
+        if (has) {
+            uint32_t rw, qw;
+            if (dir == 0) {
+                rw = sa_load8(a.ref, (int64_t)rl + o);
+                qw = sa_load8(qp, (int64_t)ql + o);
+            } else {
+                rw = sa_rev_nibbles(sa_load8(a.ref, (int64_t)rl - o - 8));
+                qw = sa_rev_nibbles(sa_load8(qp, (int64_t)ql - o - 8));
+            }
+            bool alive = true;
+            uint32_t stop = 0;
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                const uint32_t off = o + kk;  // 0-based index along this direction
+                const int sc = sub[(((rw >> (4 * kk)) & 7u) << 3) | ((qw >> (4 * kk)) & 7u)];
+                if (alive) {
+                    if (off >= avail) {
+                        alive = false;
+                        stop = off;
+                    } else {
+                        S += sc;
+                        if (S > best) {
+                            best = S;
+                            bpos = (int)off + dir;  // left offsets are 1-based
+                        }
+                        if (best - S > xdrop) {
+                            alive = false;
+                            stop = off;
+                        }
+                    }
+                }
+            }
+            if (!alive) {
+                tiles += (stop >> 5) + 1;
+                if (dir == 0) {
+                    Rbest = best;
+                    Rpos = bpos;
+                    dir = 1;
+                    o = 0;
+                    S = 0;
+                    best = 0;
+                    bpos = 0;
+                    avail = min(rl, ql);
+                } else {
+                    finished = true;
+                }
+            } else {
+                o += 8;
+                if (o >= a.lane_cap && !nocap) to_long = true;
+            }
+            if (finished) {
+                Lpos = bpos;
+                const int total = Rbest + best;
+                const int ext = Rpos + Lpos;
+                int cnt[4] = {0, 0, 0, 0};
+                const bool eb = sa_entropy_branch(a, total);
+                if (eb) {
+                    const int64_t r0 = (int64_t)rl - Lpos, q0 = (int64_t)ql - Lpos, nb = (int64_t)ext + 1;
+                    for (int64_t i = 0; i < nb; i += 8) {
+                        uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
+                        sa_count_matches8(sa_load8(a.ref, r0 + i), sa_load8(qp, q0 + i), nm, cnt);
+                    }
+                }
+                sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
+                tiles_acc += tiles;
+                has = false;
+            }
+        }
+
+        // ---- long queue pushes (warp-aggregated) ----
+        {
+            const uint32_t lm = __ballot_sync(SA_FULL, to_long);
+            if (lm) {
+                const int leader = __ffs(lm) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(&a.ctr->long_count, (unsigned long long)__popc(lm));
+                base = __shfl_sync(SA_FULL, base, leader);
+                if (to_long) {
+                    const unsigned long long idx = base + __popc(lm & lt);
+                    if (idx < a.long_cap) {
+                        SaLongHit e;
+                        e.ref_loc = rl;
+                        e.query_loc = ql;
+                        e.unit = unit_id;
+                        e.scope = scope;
+                        a.long_q[idx] = e;
+                        has = false;
+                    } else {
+                        nocap = true;  // queue full: finish this hit in the lane
+                        atomicAdd(&a.ctr->long_overflow, 1ull);
+                    }
+                }
+            }
+        }
+        // ---- survivor appends (warp-aggregated) ----
+        {
+            const bool emit = finished && keep;
+            const uint32_t em = __ballot_sync(SA_FULL, emit);
+            if (em) {
+                const int leader = __ffs(em) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(em));
+                base = __shfl_sync(SA_FULL, base, leader);
+                if (emit) {
+                    const unsigned long long idx = base + __popc(em & lt);
+                    if (idx < a.surv_cap) {
+                        SaRec r;
+                        r.ref_start = rl - (uint32_t)Lpos;  // :606-608
+                        r.query_start = ql - (uint32_t)Lpos;
+                        r.len = (uint32_t)(Rpos + Lpos);
+                        r.score = score;
+                        if (uflags & 2u) r.query_start = ref_len - 1 - (r.query_start + r.len);  // rm :704-707
+                        a.surv[idx] = r;
+                        a.surv_scope[idx] = scope;
+                    } else {
+                        atomicAdd(&a.ctr->surv_overflow, 1ull);
+                    }
+                }
+            }
+        }
+    }
+    // flush statistics
+    unsigned long long t = tiles_acc, e = ext_acc;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        t += __shfl_xor_sync(SA_FULL, t, s);
+        e += __shfl_xor_sync(SA_FULL, e, s);
+    }
+    if (lane == 0) {
+        atomicAdd(&a.ctr->base_steps, t);
+        atomicAdd(&a.ctr->extended, e);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phase B: one warp per long hit, 256 bases per step.
+// ---------------------------------------------------------------------------
+struct SaDirResult {
+    int best;
+    int pos;
+    uint32_t tiles;
+};
+
+__device__ __forceinline__ int sa_warp_incl_max(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(SA_FULL, v, o);
+        if (lane >= o) v = max(v, t);
+    }
+    return v;
+}
+
+// (value, index) arg-max over the warp: larger value wins, ties go to the smaller index.
+__device__ __forceinline__ void sa_warp_argmax(int& v, uint32_t& idx) {
+    long long key = ((long long)v << 32) | (long long)(uint32_t)(~idx);
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        long long o = __shfl_xor_sync(SA_FULL, key, s);
+        key = o > key ? o : key;
+    }
+    v = (int)(key >> 32);
+    idx = ~(uint32_t)(key & 0xffffffffll);
+}
+
+__device__ SaDirResult sa_warp_xdrop(const int* sub, const uint32_t* __restrict__ ref, const uint32_t* __restrict__ qp,
+                                     uint32_t rl, uint32_t ql, uint32_t avail, int dir, int xdrop) {
+    const int lane = threadIdx.x & 31;
+    int S_prev = 0, best = 0, bpos = dir ? 0 : -1;
+    uint32_t o = 0;
+    SaDirResult res;
+    while (true) {
+        const uint32_t loff = o + 8u * lane;
+        const int cnt_in = (avail > loff) ? (int)min(avail - loff, 8u) : 0;
+        uint32_t rw = 0, qw = 0;
+        if (cnt_in > 0) {
+            if (dir == 0) {
+                rw = sa_load8(ref, (int64_t)rl + loff);
+                qw = sa_load8(qp, (int64_t)ql + loff);
+            } else {
+                rw = sa_rev_nibbles(sa_load8(ref, (int64_t)rl - loff - 8));
+                qw = sa_rev_nibbles(sa_load8(qp, (int64_t)ql - loff - 8));
+            }
+        }
+        int ps[8];
+        int p = 0, lmax = INT_MIN, lmax_k = 0, lmin = INT_MAX;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            int s = (kk < cnt_in) ? sub[(((rw >> (4 * kk)) & 7u) << 3) | ((qw >> (4 * kk)) & 7u)] : 0;
+            p += s;
+            ps[kk] = p;
+            if (kk < cnt_in) {
+                if (p > lmax) {
+                    lmax = p;
+                    lmax_k = kk;
+                }
+                lmin = min(lmin, p);
+            }
+        }
+        const int incl = sa_warp_incl_sum(p);
+        const int pre = incl - p;
+        const int step_total = __shfl_sync(SA_FULL, incl, 31);
+        const int base = S_prev + pre;
+        const int amax = cnt_in > 0 ? base + lmax : INT_MIN;
+        const int im = sa_warp_incl_max(amax);
+        int excl = __shfl_up_sync(SA_FULL, im, 1);
+        if (lane == 0) excl = INT_MIN;
+        const int Mbefore = max(best, excl);
+        int stop_k = -1, bmax = INT_MIN, bmax_k = 0;
+        const bool possible = (cnt_in < 8) || (max(Mbefore, amax) - (base + lmin) > xdrop);
+        if (possible) {
+            int M = Mbefore;
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                if (stop_k < 0) {
+                    if (kk >= cnt_in) {
+                        stop_k = kk;
+                    } else {
+                        const int Sv = base + ps[kk];
+                        M = max(M, Sv);
+                        if (M - Sv > xdrop) stop_k = kk;
+                        else if (Sv > bmax) {
+                            bmax = Sv;
+                            bmax_k = kk;
+                        }
+                    }
+                }
+            }
+        }
+        const uint32_t sm = __ballot_sync(SA_FULL, stop_k >= 0);
+        int cv;
+        uint32_t ci;
+        if (sm) {
+            const int f = __ffs(sm) - 1;
+            if (lane < f) {
+                cv = amax;
+                ci = loff + lmax_k;
+            } else if (lane == f) {
+                cv = bmax;
+                ci = loff + bmax_k;
+            } else {
+                cv = INT_MIN;
+                ci = 0xffffffffu;
+            }
+            sa_warp_argmax(cv, ci);
+            if (cv > best) {
+                best = cv;
+                bpos = (int)ci + dir;
+            }
+            const uint32_t stop_idx = __shfl_sync(SA_FULL, loff + (uint32_t)stop_k, f);
+            res.tiles = (stop_idx >> 5) + 1;
+            break;
+        }
+        cv = amax;
+        ci = loff + lmax_k;
+        sa_warp_argmax(cv, ci);
+        if (cv > best) {
+            best = cv;
+            bpos = (int)ci + dir;
+        }
+        S_prev += step_total;
+        o += 256;
+    }
+    res.best = best;
+    res.pos = bpos;
+    return res;
+}
+
+__global__ void __launch_bounds__(256)
+sa_k_extend_warp(SaExtK a, SaParams P) {
+    __shared__ int sub[64];
+    if (threadIdx.x < 64) sub[threadIdx.x] = P.sub_mat[threadIdx.x];
+    __syncthreads();
+    if (a.ctr->error) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long nlong = min(a.ctr->long_count, (unsigned long long)a.long_cap);
+    unsigned long long tiles_acc = 0;
+    while (true) {
+        unsigned long long idx = 0;
+        if (lane == 0) idx = atomicAdd(&a.ctr->long_cursor, 1ull);
+        idx = __shfl_sync(SA_FULL, idx, 0);
+        if (idx >= nlong) break;
+        const SaLongHit L = a.long_q[idx];
+        const SaUnit U = a.units[L.unit];
+        const uint32_t rl = L.ref_loc, ql = L.query_loc;
+        const uint32_t avail_r = (rl < a.ref_len && ql < U.q_len) ? min(a.ref_len - rl, U.q_len - ql) : 0u;
+        const SaDirResult R = sa_warp_xdrop(sub, a.ref, U.q_packed, rl, ql, avail_r, 0, a.xdrop);
+        const SaDirResult Lr = sa_warp_xdrop(sub, a.ref, U.q_packed, rl, ql, min(rl, ql), 1, a.xdrop);
+        tiles_acc += R.tiles + Lr.tiles;
+        const int total = R.best + Lr.best;
+        const int ext = R.pos + Lr.pos;
+        int cnt[4] = {0, 0, 0, 0};
+        const bool eb = sa_entropy_branch(a, total);
+        if (eb) {
+            const int64_t r0 = (int64_t)rl - Lr.pos, q0 = (int64_t)ql - Lr.pos, nb = (int64_t)ext + 1;
+            for (int64_t i = 8 * lane; i < nb; i += 256) {
+                uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
+                sa_count_matches8(sa_load8(a.ref, r0 + i), sa_load8(U.q_packed, q0 + i), nm, cnt);
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int s = 16; s >= 1; s >>= 1) cnt[b] += __shfl_xor_sync(SA_FULL, cnt[b], s);
+        }
+        if (lane == 0) {
+            int keep, score;
+            sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
+            if (keep) {
+                const unsigned long long o = atomicAdd(&a.ctr->surv_count, 1ull);
+                if (o < a.surv_cap) {
+                    SaRec r;
+                    r.ref_start = rl - (uint32_t)Lr.pos;
+                    r.query_start = ql - (uint32_t)Lr.pos;
+                    r.len = (uint32_t)ext;
+                    r.score = score;
+                    if (U.flags & 2u) r.query_start = a.ref_len - 1 - (r.query_start + r.len);
+                    a.surv[o] = r;
+                    a.surv_scope[o] = L.scope;
+                } else {
+                    atomicAdd(&a.ctr->surv_overflow, 1ull);
+                }
+            }
+        }
+    }
+    if (lane == 0) atomicAdd(&a.ctr->base_steps, tiles_acc);
+}
+
+void sa_launch_extend(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
+                      cudaStream_t st) {
+    SaExtK a;
+    a.ref = x.ref;
+    a.ref_len = x.ref_len;
+    a.pos_table = x.pos_table;
+    a.cs = w.cs;
+    a.units = w.units;
+    a.ctr = w.ctr;
+    a.long_q = w.long_q;
+    a.long_cap = w.long_cap;
+    a.surv = w.rec[0];
+    a.surv_scope = w.scope[0];
+    a.surv_cap = w.surv_cap;
+    a.seed_size = x.seed_size;
+    a.xdrop = x.xdrop;
+    a.hspthresh = x.hspthresh;
+    a.noentropy = x.noentropy;
+    a.lane_cap = (uint32_t)t.lane_cap;
+    a.tile_hits = (uint32_t)t.tile_hits;
+    sa_k_extend_lane<<<num_sms * t.ext_ctas_per_sm, t.ext_block, 0, st>>>(a, p);
+    sa_k_extend_warp<<<num_sms * 4, t.long_block, 0, st>>>(a, p);
+}

@@ -1,0 +1,253 @@
+// sa_host.cpp — host side of the seed-filter path, in C++ as in the
+// reference: query seeding (src/seeder.cpp), the scoring table
+// (src/main.cpp:180-261), host reverse complement (common/ntcoding.cpp:63-105)
+// and the seeder pipeline that cuts a query block into intervals and chunks
+// and calls sa_seed_and_filter() from several host threads, in the way the
+// reference's TBB flow graph does (src/main.cpp:546-566, src/seeder.cpp:12-127).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/segalign_b200.h"
+#include "../../include/segalign_b200_host.h"
+
+namespace {
+
+struct HostShape {
+    int seed_size = 19;
+    int kmer_size = 12;
+    int pos[32] = {0, 1, 2, 4, 7, 8, 11, 13, 15, 16, 17, 18};
+    int transition = 0;
+};
+HostShape g_shape;
+
+inline int nt_valid(char ch, uint32_t* v) {
+    switch (ch) {
+        case 'A': *v = 0; return 1;
+        case 'C': *v = 1; return 1;
+        case 'G': *v = 2; return 1;
+        case 'T': *v = 3; return 1;
+        default: return 0;  // lowercase, N, '&', IUPAC: invalid (common/ntcoding.cpp:10-19)
+    }
+}
+
+// common/ntcoding.cpp:43-61
+inline uint32_t kmer_at(const char* s, uint64_t p) {
+    uint32_t nt[32];
+    for (int i = 0; i < g_shape.seed_size; ++i)
+        if (!nt_valid(s[p + i], &nt[i])) return 1u << 31;
+    uint32_t k = 0;
+    for (int i = 0; i < g_shape.kmer_size; ++i) k = (k << 2) + nt[g_shape.pos[i]];
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sa_host_set_shape(const char* shape, int transition) {
+    std::string name = shape ? shape : "12of19", pat;
+    if (name == "12of19") pat = "TTT0T00TT00T0T0TTTT";
+    else if (name == "14of22") pat = "TTT0T0TT00TT00T0T0TTTT";
+    else {
+        pat = name;
+        for (auto& c : pat) c = (c == '1' || c == 'T') ? 'T' : '0';
+    }
+    int k = 0;
+    for (size_t i = 0; i < pat.size() && k < 32; ++i)
+        if (pat[i] == 'T') g_shape.pos[k++] = (int)i;
+    if (k > 15 || k <= 3 || pat.size() > 32) return SA_ERR_ARG;
+    g_shape.kmer_size = k;
+    g_shape.seed_size = (int)pat.size();
+    g_shape.transition = transition ? 1 : 0;
+    return k;
+}
+
+// src/seeder.cpp:57-74: for j in [j0, j1): word (key << 32) + j, followed by
+// the transition variants key ^ (2 << 2t), t = 0..K-1, when transitions are on.
+uint64_t sa_host_chunk_seeds(const char* text, uint32_t j0, uint32_t j1, uint64_t* out, uint64_t cap) {
+    uint64_t n = 0;
+    for (uint32_t j = j0; j < j1; ++j) {
+        uint32_t k = kmer_at(text, j);
+        if (k == (1u << 31)) continue;
+        if (n < cap) out[n] = ((uint64_t)k << 32) + j;
+        ++n;
+        if (g_shape.transition)
+            for (int t = 0; t < g_shape.kmer_size; ++t) {
+                if (n < cap) out[n] = ((uint64_t)(k ^ (2u << (2 * t))) << 32) + j;
+                ++n;
+            }
+    }
+    return n;
+}
+
+// common/ntcoding.cpp:63-105; characters other than ACGTacgtnN& are skipped.
+uint64_t sa_host_revcomp(char* dst, const char* src, uint64_t len) {
+    uint64_t r = 0;
+    for (uint64_t i = len; i > 0; --i) {
+        char c = src[i - 1], o;
+        switch (c) {
+            case 'a': o = 't'; break;
+            case 'A': o = 'T'; break;
+            case 'c': o = 'g'; break;
+            case 'C': o = 'G'; break;
+            case 'g': o = 'c'; break;
+            case 'G': o = 'C'; break;
+            case 't': o = 'a'; break;
+            case 'T': o = 'A'; break;
+            case 'n': o = 'n'; break;
+            case 'N': o = 'N'; break;
+            case '&': o = '&'; break;
+            default: continue;
+        }
+        dst[r++] = o;
+    }
+    return r;
+}
+
+// src/main.cpp:180-261 (no --scoring file): HOXD70 plus the lowercase, N,
+// other-IUPAC and separator rows.  ambiguous: NULL/"" , "n", "iupac", or
+// "<field>,<reward>,<penalty>".
+int sa_build_sub_mat(int xdrop, const char* ambiguous, int* m) {
+    int reward = -100, penalty = -100;
+    const int fill = -100, bad = -1000;
+    std::string amb = ambiguous ? ambiguous : "";
+    std::vector<std::string> f;
+    size_t s = 0;
+    while (true) {
+        size_t k = amb.find(',', s);
+        f.push_back(amb.substr(s, k == std::string::npos ? std::string::npos : k - s));
+        if (k == std::string::npos) break;
+        s = k + 1;
+    }
+    const std::string field = f[0];
+    if (f.size() == 3) {
+        char* e1 = nullptr;
+        char* e2 = nullptr;
+        long r = strtol(f[1].c_str(), &e1, 10), p = strtol(f[2].c_str(), &e2, 10);
+        if (f[1].empty() || f[2].empty() || *e1 || *e2) return SA_ERR_ARG;
+        reward = (int)r;
+        penalty = -(int)p;
+    } else if (amb == "n" || amb == "iupac") {
+        reward = 0;
+        penalty = 0;
+    }
+    static const int hoxd70[4][4] = {{91, -114, -31, -123}, {-114, 100, -125, -31}, {-31, -125, 100, -114}, {-123, -31, -114, 91}};
+    for (int i = 0; i < 64; ++i) m[i] = 0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) m[i * 8 + j] = hoxd70[i][j];
+    for (int i = 0; i < 4; ++i) m[i * 8 + 4] = m[4 * 8 + i] = bad;
+    m[4 * 8 + 4] = bad;
+    const bool nmode = field == "n" || field == "iupac";
+    for (int i = 0; i < 5; ++i) m[i * 8 + 5] = m[5 * 8 + i] = nmode ? penalty : bad;
+    m[5 * 8 + 5] = nmode ? reward : bad;
+    if (field == "iupac") {
+        for (int i = 0; i < 6; ++i) m[i * 8 + 6] = m[6 * 8 + i] = penalty;
+        m[6 * 8 + 6] = reward;
+    } else {
+        for (int i = 0; i < 4; ++i) m[i * 8 + 6] = m[6 * 8 + i] = fill;
+        for (int i = 4; i < 6; ++i) m[i * 8 + 6] = m[6 * 8 + i] = bad;
+        m[6 * 8 + 6] = fill;
+    }
+    for (int i = 0; i < 7; ++i) m[i * 8 + 7] = m[7 * 8 + i] = -10 * xdrop;
+    m[7 * 8 + 7] = -10 * xdrop;
+    return SA_OK;
+}
+
+// Seeder pipeline over one query block (src/main.cpp:373-386 intervals,
+// :707 q_len = Lq - seed_size; src/seeder.cpp:47-121 chunks and strands).
+// Calls run on cfg->num_threads host threads; results are concatenated per
+// strand in interval/chunk order.
+int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_len, sa_segment** fw,
+                  uint64_t* fw_len, sa_segment** rc, uint64_t* rc_len, sa_seeder_stats* stats) {
+    if (!cfg || !query || !fw || !fw_len || !rc || !rc_len || cfg->chunk_size == 0 || cfg->interval_size == 0)
+        return SA_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    if (query_len < (uint32_t)g_shape.seed_size) return SA_ERR_ARG;
+    std::vector<char> rctext(query_len);
+    if (cfg->strand & 2) {
+        if (sa_host_revcomp(rctext.data(), query, query_len) != query_len) return SA_ERR_ARG;
+    }
+    const uint32_t qlen_s = query_len - (uint32_t)g_shape.seed_size;
+    struct Call {
+        int strand;
+        uint32_t j0, j1;
+    };
+    std::vector<Call> calls;
+    for (uint64_t cur = 0; cur < qlen_s; cur += cfg->interval_size) {
+        uint32_t s = (uint32_t)cur;
+        uint32_t e = (uint32_t)std::min<uint64_t>(qlen_s, cur + cfg->interval_size + cfg->interval_overlap);
+        if (cfg->strand & 1)
+            for (uint64_t i = s; i < e; i += cfg->chunk_size)
+                calls.push_back({0, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg->chunk_size, e)});
+        if (cfg->strand & 2) {
+            uint32_t rs = qlen_s - e, re = qlen_s - s;
+            for (uint64_t i = rs; i < re; i += cfg->chunk_size)
+                calls.push_back({1, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg->chunk_size, re)});
+        }
+    }
+    if (cfg->max_chunks && calls.size() > cfg->max_chunks) calls.resize(cfg->max_chunks);
+    std::vector<std::vector<sa_segment>> res(calls.size());
+    std::atomic<uint64_t> next{0}, nseeds{0}, nhits{0}, nhsps{0};
+    std::atomic<int> err{0};
+    auto worker = [&]() {
+        std::vector<uint64_t> seeds;
+        while (!err) {
+            uint64_t c = next.fetch_add(1);
+            if (c >= calls.size()) break;
+            const Call& cl = calls[c];
+            const char* txt = cl.strand ? rctext.data() : query;
+            uint64_t need = sa_host_chunk_seeds(txt, cl.j0, cl.j1, nullptr, 0);
+            if (need == 0) continue;  // src/seeder.cpp:190
+            seeds.resize(need);
+            sa_host_chunk_seeds(txt, cl.j0, cl.j1, seeds.data(), need);
+            sa_segment* out = nullptr;
+            uint64_t ol = 0;
+            int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, cfg->buffer, &out, &ol);
+            if (r != SA_OK) {
+                err = r;
+                break;
+            }
+            sa_call_stats cs;
+            sa_last_call_stats(&cs);
+            nseeds += need;
+            nhits += cs.num_hits;
+            nhsps += ol - 1;
+            res[c].assign(out + 1, out + ol);
+            sa_free_segments(out);
+        }
+    };
+    int nt = std::max(1, cfg->num_threads);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) th.emplace_back(worker);
+    for (auto& t : th) t.join();
+    if (err) return err;
+    uint64_t nf = 0, nr = 0;
+    for (size_t c = 0; c < calls.size(); ++c) (calls[c].strand ? nr : nf) += res[c].size();
+    *fw = (sa_segment*)malloc(sizeof(sa_segment) * (nf ? nf : 1));
+    *rc = (sa_segment*)malloc(sizeof(sa_segment) * (nr ? nr : 1));
+    if (!*fw || !*rc) return SA_ERR_NOMEM;
+    uint64_t a = 0, b = 0;
+    for (size_t c = 0; c < calls.size(); ++c) {
+        sa_segment* dst = calls[c].strand ? *rc + b : *fw + a;
+        if (!res[c].empty()) std::memcpy(dst, res[c].data(), res[c].size() * sizeof(sa_segment));
+        (calls[c].strand ? b : a) += res[c].size();
+    }
+    *fw_len = nf;
+    *rc_len = nr;
+    if (stats) {
+        stats->num_seeds = nseeds;
+        stats->num_hits = nhits;
+        stats->num_hsps = nhsps;
+        stats->num_calls = calls.size();
+        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return SA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// sa_internal.cuh — shared types and device helpers of the B200 seed-filter path.
+//
+// Sequence layout in HBM: one 4-bit code per base, 8 bases per uint32 word
+// ("nibble-packed"), base i in bits [4*(i&7), 4*(i&7)+4) of word i>>3.  Codes
+// are the reference's (common/parameters.h:4-11): A0 C1 G2 T3 L4 N5 X6 E7.
+// Every packed array carries SA_PADW words of padding on both sides (filled
+// with E codes) so that 8-base windows next to either end can be loaded
+// without bounds checks; scoring itself never reads past the sequence.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SA_PADW 8  // padding words on each side of a packed sequence
+#define SA_NUC 8
+#define SA_WARP 32
+#define SA_INVALID_KEY 0xffffffffu
+
+// Filter parameters (src/seed_filter.cu:20-27; InitializeProcessor :780-796).
+struct SaParams {
+    int32_t sub_mat[64];   // row = target code, column = query code
+    int32_t xdrop;
+    int32_t hspthresh;
+    int32_t noentropy;
+    int32_t seed_size;     // shape span (19 for 12of19)
+    int32_t kmer_size;     // K
+    int32_t transition;
+    int32_t shape_pos[32];
+};
+
+// A query (or target-as-query) view used by one extension unit.
+struct SaSeqView {
+    const uint32_t* packed;  // points at word 0 (padding precedes it)
+    uint32_t len;
+};
+
+// Per compacted seed (seed with >= 1 hit), struct-of-arrays in the workspace.
+//   E[c]     exclusive prefix of hits (uint64), E[nnz] = total hits
+//   lo[c]    first bucket entry in the position table
+//   qpos[c]  query position j (seed word low 32 bits)
+//   scope[c] dedup scope (MAX_HITS iteration, or unit/iteration in batches)
+//   unit[c]  extension unit (query view, strand, rm window)
+struct SaSeedList {
+    uint64_t* E;
+    uint32_t* lo;
+    uint32_t* qpos;
+    uint32_t* scope;
+    uint32_t* unit;
+};
+
+// Extension unit: what a hit needs besides its two coordinates.
+struct SaUnit {
+    const uint32_t* q_packed;
+    uint32_t q_len;
+    uint32_t rm_lo, rm_hi;   // rm window on ref_loc, inclusive
+    uint32_t flags;          // bit0 = rm mode, bit1 = rev (rm coordinate flip)
+};
+
+// Survivor record (segmentPair, src/graph.h:25-30) + dedup scope.
+struct SaRec {
+    uint32_t ref_start;
+    uint32_t query_start;
+    uint32_t len;
+    int32_t score;
+};
+
+// Long-extension queue entry (hits whose X-drop ran past the lane-per-hit cap).
+struct SaLongHit {
+    uint32_t ref_loc;
+    uint32_t query_loc;
+    uint32_t unit;
+    uint32_t scope;
+};
+
+// Device-side counters of one call.
+struct SaCounters {
+    unsigned long long num_hits;       // total hits (ungapped extensions)
+    unsigned long long nnz;            // seeds with >= 1 hit
+    unsigned long long hit_cursor;     // extension work counter
+    unsigned long long long_count;     // hits in the long queue
+    unsigned long long long_cursor;
+    unsigned long long surv_count;     // survivors appended
+    unsigned long long extended;       // hits actually extended (rm window)
+    unsigned long long base_steps;     // bases scored
+    unsigned long long long_overflow;  // long-queue pushes refused (handled in place)
+    unsigned long long surv_overflow;  // survivor appends refused -> error
+    unsigned long long uniq_count;     // records after dedup
+    unsigned long long num_iter;       // MAX_HITS iterations
+    unsigned long long error;          // nonzero = device-side error code
+    unsigned long long pad[3];
+};
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t sa_lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// 8 consecutive codes starting at base position p (may be negative down to
+// -8*SA_PADW): nibble k of the result is the code of base p+k.
+__device__ __forceinline__ uint32_t sa_load8(const uint32_t* __restrict__ packed, int64_t p) {
+    int64_t w = p >> 3;  // floor division (arithmetic shift)
+    uint32_t sh = (uint32_t)(p & 7) * 4u;
+    uint32_t lo = __ldg(packed + w);
+    uint32_t hi = __ldg(packed + w + 1);
+    return __funnelshift_r(lo, hi, sh);
+}
+
+__device__ __forceinline__ uint32_t sa_code_at(const uint32_t* __restrict__ packed, int64_t p) {
+    return (__ldg(packed + (p >> 3)) >> ((uint32_t)(p & 7) * 4u)) & 0xfu;
+}
+
+// Per-base match counts (R == Q == b, b in 0..3) over 8 packed bases, only for
+// the nibbles selected by `nmask` (one bit per nibble, bit k = base k).
+__device__ __forceinline__ void sa_count_matches8(uint32_t rw, uint32_t qw, uint32_t nmask,
+                                                  int* c) {
+    uint32_t eq = ~(rw ^ qw);
+    eq = eq & (eq >> 1) & (eq >> 2) & (eq >> 3) & 0x11111111u;  // nibble equal -> bit 0 set
+    uint32_t sel = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sel |= ((nmask >> k) & 1u) << (4 * k);
+    eq &= sel;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        uint32_t t = ~(rw ^ (0x11111111u * (uint32_t)b));
+        t = t & (t >> 1) & (t >> 2) & (t >> 3) & 0x11111111u;
+        c[b] += __popc(eq & t);
+    }
+}
+
+#define SA_CUDA_OK(expr)                                   \
+    do {                                                   \
+        cudaError_t _e = (expr);                           \
+        if (_e != cudaSuccess) return sa_cuda_fail(_e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+int sa_cuda_fail(cudaError_t e, const char* what, const char* file, int line);

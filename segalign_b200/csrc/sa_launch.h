@@ -1,0 +1,120 @@
+// sa_launch.h — host-side launchers of the device kernels (internal).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sa_internal.cuh"
+
+// Per-call device descriptor, read by every kernel of one call so that the
+// whole chain can be launched without host-side sizes.
+struct SaCallDesc {
+    uint64_t num_seeds;     // seed words (plain) or seed slots (batched)
+    uint64_t max_hits;      // MAX_HITS (dedup iteration size)
+    uint32_t num_units;
+    uint32_t num_scopes_max;
+    uint32_t rm_exclude_diag;
+    uint32_t pad;
+};
+
+// Batched unit: a query window [start, end) of one packed query, seeded on the device.
+struct SaBatchUnit {
+    uint64_t slot_begin;    // first seed slot of the unit in the flattened slot space
+    uint32_t q_start, q_end;// seed positions j in [q_start, q_end)
+    uint32_t keys_index;    // which key array (query buffer x strand)
+    uint32_t unit;          // index into the SaUnit table
+};
+
+// Workspace of one slot (one in-flight call).  Sizes are capacities.
+struct SaWork {
+    // seeds
+    uint64_t* seeds;        // [seed_cap]
+    uint32_t* s_lo;         // [seed_cap] bucket start per seed
+    uint32_t* s_cnt;        // [seed_cap] bucket size per seed
+    uint64_t* s_P;          // [seed_cap] inclusive hit prefix per seed
+    SaSeedList cs;          // compacted seeds [seed_cap + 1]
+    uint64_t seed_cap;
+    // per-CTA partials (range-partitioned kernels)
+    unsigned long long* cta_a;  // [SA_MAX_CTAS]
+    unsigned long long* cta_b;  // [SA_MAX_CTAS]
+    // MAX_HITS iteration limits (seed indices) [SA_MAX_ITERS]
+    uint64_t* limits;
+    // long queue
+    SaLongHit* long_q;
+    uint64_t long_cap;
+    // survivors (ping-pong) and dedup output
+    SaRec* rec[2];
+    uint32_t* scope[2];
+    uint32_t* flags;        // [surv_cap]
+    uint64_t surv_cap;
+    SaRec* out;             // [surv_cap] deduplicated records (device)
+    uint32_t* out_scope;
+    uint32_t* scope_count;  // [SA_MAX_SCOPES]
+    uint32_t* scope_flags;  // [SA_MAX_SCOPES] bit0 = rev (rm diagonal exclusion)
+    // sort state
+    unsigned int* sort_hist;      // [SA_SORT_MAX_DIGITS * 256] global histograms
+    unsigned int* sort_cta_hist;  // [256 * SA_MAX_CTAS]
+    int* sort_in_buf;             // [SA_SORT_MAX_DIGITS + 1] input buffer per pass, final at [D]
+    // counters + descriptor
+    SaCounters* ctr;
+    SaCallDesc* desc;
+    // units
+    SaUnit* units;          // [SA_MAX_UNITS]
+    SaBatchUnit* bunits;    // [SA_MAX_UNITS]
+};
+
+#define SA_MAX_CTAS 1024
+#define SA_MAX_ITERS 256
+#define SA_MAX_SCOPES 65536
+#define SA_MAX_UNITS 65536
+#define SA_SORT_MAX_DIGITS 20
+
+struct SaTuning {
+    int lane_cap;        // bases per direction handled lane-per-hit before a hit moves to the long queue
+    int ext_block;       // threads per CTA of the lane-per-hit kernel
+    int ext_ctas_per_sm;
+    int long_block;      // threads per CTA of the warp-per-hit kernel
+    int range_ctas;      // CTAs of the range-partitioned kernels
+    int tile_hits;       // hits per warp tile
+};
+
+// ---- sa_pack.cu ----
+void sa_launch_pack_text(const char* d_text, uint64_t len, uint32_t* packed, cudaStream_t st);
+void sa_launch_rc_packed(const uint32_t* in, uint64_t len, uint32_t* out, cudaStream_t st);
+void sa_launch_pad_fill(uint32_t* packed_base, uint64_t nwords_with_pad, cudaStream_t st);
+// Table build: keys of target positions, ordered compaction of valid ones.
+void sa_launch_table_keys(const uint32_t* ref, uint32_t start, uint64_t num_steps, uint32_t step,
+                          const SaParams& p, uint32_t* keys, uint32_t* vals,
+                          unsigned long long* cta_a, unsigned long long* cta_b,
+                          unsigned long long* d_total, int G, cudaStream_t st);
+void sa_launch_table_index(const uint32_t* sorted_keys, const unsigned long long* d_n,
+                           uint32_t* index, uint64_t nbuckets, cudaStream_t st);
+// Plain (key, value) radix sort by the low `bits` bits of the key.
+void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint32_t* vals_tmp,
+                       const unsigned long long* d_n, int bits, unsigned int* cta_hist,
+                       int G, cudaStream_t st, int* result_in_tmp);
+
+// ---- sa_lookup.cu ----
+void sa_launch_lookup_seeds(SaWork& w, const uint32_t* index, uint32_t nbuckets,
+                            const SaParams& p, int G, cudaStream_t st);
+void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets,
+                            const uint32_t* const* keys_arrays, uint32_t n_bunits,
+                            const SaParams& p, int G, cudaStream_t st);
+
+// ---- sa_extend.cu ----
+struct SaExtendArgs {
+    const uint32_t* ref;
+    uint32_t ref_len;
+    const uint32_t* pos_table;
+    uint32_t seed_size;
+    int32_t xdrop, hspthresh, noentropy;
+};
+void sa_launch_extend(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
+                      int num_sms, cudaStream_t st);
+
+// ---- sa_sort.cu ----
+// mode 0 = plain dedup; 1 = rm (adds diagonal sort/unique and final sort).
+void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t st);
+
+// Hand-off of a failed CUDA call to the API layer's error state.
+void sa_set_error(int code, const char* fmt, ...);

@@ -1,0 +1,282 @@
+// sa_sort.cu — per-scope ordering and deduplication of surviving HSPs.
+//
+// Reference (per SeedAndFilter call and MAX_HITS iteration):
+//   plain: thrust::stable_sort(hspComp) + unique_copy(hspEqual)
+//          src/seed_filter.cu:47-80, 728-732
+//   rm:    then stable_sort(hspDiagComp) + unique_copy(hspDiagEqual) +
+//          stable_sort(hspFinalComp)   repeat_masker_src/seed_filter.cu:45-107, 797-811
+// unique_copy on the CUDA backend keeps element i iff i == 0 or
+// !pred(x[i-1], x[i]) with x[i-1] the input predecessor (CUB FlagHeads), which
+// matters for the non-transitive hspDiagEqual.
+//
+// Keys.  Records of one scope come from one (query, target) pair, so the HSP
+// score is a function of (ref_start, query_start, len): total is the sum of
+// substitution scores over the segment and the entropy factor depends only on
+// the segment's base counts.  hspComp therefore orders a scope totally by
+// (query_start asc, len desc, ref_start asc); equal keys are equal records.
+// The rm sorts are stable on their input, so hspDiagComp needs (diag, ref_start,
+// score desc) [query_start follows from diag and ref_start] and hspFinalComp
+// needs (query_start, score desc, ref_start desc); ties keep the earlier order
+// exactly as thrust's stable sort does.  The scope is the most significant key.
+#include "sa_launch.h"
+#include "sa_radix.cuh"
+
+#define SA_DERR_SURV_OVERFLOW 4
+
+enum : uint8_t { F_RS = 0, F_QS = 1, F_LEN = 2, F_SCORE = 3, F_SCOPE = 4, F_DIAG = 5 };
+
+struct SaSortSpec {
+    int npass;
+    uint8_t field[SA_SORT_MAX_DIGITS];
+    uint8_t byte[SA_SORT_MAX_DIGITS];
+    uint8_t inv[SA_SORT_MAX_DIGITS];
+};
+
+struct SaRecOps {
+    struct Ctx {
+        SaRec* rec[2];
+        uint32_t* scope[2];
+        SaSortSpec spec;
+    };
+    static __device__ __forceinline__ uint32_t field_value(const SaRec& r, uint32_t scope, int f) {
+        switch (f) {
+            case F_RS: return r.ref_start;
+            case F_QS: return r.query_start;
+            case F_LEN: return r.len;
+            case F_SCORE: return (uint32_t)r.score ^ 0x80000000u;  // signed ascending
+            case F_SCOPE: return scope;
+            default: return r.ref_start - r.query_start;      // uint32 diagonal
+        }
+    }
+    static __device__ __forceinline__ uint32_t digit(const Ctx& c, int buf, uint64_t i, int pass) {
+        const SaRec r = c.rec[buf][i];
+        uint32_t v = field_value(r, c.scope[buf][i], c.spec.field[pass]);
+        if (c.spec.inv[pass]) v = ~v;
+        return (v >> (8 * c.spec.byte[pass])) & 0xffu;
+    }
+    static __device__ __forceinline__ void move(const Ctx& c, int buf, uint64_t i, uint32_t dst) {
+        c.rec[buf ^ 1][dst] = c.rec[buf][i];
+        c.scope[buf ^ 1][dst] = c.scope[buf][i];
+    }
+};
+
+// Histograms of every digit of the spec in one read (pre-pass).
+__global__ void __launch_bounds__(256)
+sa_k_sort_hist_all(SaRecOps::Ctx c, const unsigned long long* d_n, const int* st, unsigned int* ghist) {
+    __shared__ unsigned int h[SA_SORT_MAX_DIGITS][256];
+    const int np = c.spec.npass, t = threadIdx.x;
+    for (int p = 0; p < np; ++p) h[p][t] = 0;
+    __syncthreads();
+    const int buf = st[0];
+    uint64_t a, b;
+    sa_cta_range(*d_n, a, b);
+    for (uint64_t i = a + t; i < b; i += 256) {
+        const SaRec r = c.rec[buf][i];
+        const uint32_t sc = c.scope[buf][i];
+        for (int p = 0; p < np; ++p) {
+            uint32_t v = SaRecOps::field_value(r, sc, c.spec.field[p]);
+            if (c.spec.inv[p]) v = ~v;
+            atomicAdd(&h[p][(v >> (8 * c.spec.byte[p])) & 0xffu], 1u);
+        }
+    }
+    __syncthreads();
+    for (int p = 0; p < np; ++p)
+        if (h[p][t]) atomicAdd(&ghist[p * 256 + t], h[p][t]);
+}
+
+// Pass plan: a pass whose digit is the same for all items is skipped.
+// in_buf[p] = input buffer of pass p (-1 = skip); in_buf[np] = final buffer.
+__global__ void sa_k_sort_plan(const unsigned int* ghist, int np, const unsigned long long* d_n, int* st) {
+    __shared__ int skip[SA_SORT_MAX_DIGITS];
+    const int t = threadIdx.x;
+    const unsigned long long n = *d_n;
+    if (t < np) skip[t] = (n <= 1);
+    __syncthreads();
+    for (int p = 0; p < np; ++p)
+        if (ghist[p * 256 + t] == n) skip[p] = 1;
+    __syncthreads();
+    if (t == 0) {
+        int cur = st[0];
+        for (int p = 0; p < np; ++p) {
+            st[1 + p] = skip[p] ? -1 : cur;
+            if (!skip[p]) cur ^= 1;
+        }
+        st[1 + np] = cur;
+    }
+}
+
+static void sa_radix_sort_recs(SaWork& w, const SaSortSpec& spec, const unsigned long long* d_n, int* st, int G,
+                               cudaStream_t s) {
+    SaRecOps::Ctx c;
+    c.rec[0] = w.rec[0];
+    c.rec[1] = w.rec[1];
+    c.scope[0] = w.scope[0];
+    c.scope[1] = w.scope[1];
+    c.spec = spec;
+    cudaMemsetAsync(w.sort_hist, 0, sizeof(unsigned int) * 256 * SA_SORT_MAX_DIGITS, s);
+    sa_k_sort_hist_all<<<G, 256, 0, s>>>(c, d_n, st, w.sort_hist);
+    sa_k_sort_plan<<<1, 256, 0, s>>>(w.sort_hist, spec.npass, d_n, st);
+    SaRadixCtl ctl{d_n, st + 1};
+    for (int p = 0; p < spec.npass; ++p) {
+        sa_k_radix_up<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
+        sa_k_radix_scan<<<1, 1024, 0, s>>>(w.sort_cta_hist, G, st + 1, p);
+        sa_k_radix_down<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Predecessor-adjacent unique + ordered compaction
+// ---------------------------------------------------------------------------
+struct SaUniqArgs {
+    SaRec* rec[2];
+    uint32_t* scope[2];
+    const uint32_t* scope_flags;
+    SaRec* out_rec;             // null: write to the other ping-pong buffer
+    uint32_t* out_scope;
+    uint32_t* scope_count;      // null: no per-scope counts
+    int mode;                   // 0 = hspEqual, 1 = hspDiagEqual + diagonal exclusion, 2 = keep all (copy)
+};
+
+__device__ __forceinline__ bool sa_rec_equal(const SaRec& x, const SaRec& y) {
+    return x.ref_start == y.ref_start && x.query_start == y.query_start && x.len == y.len && x.score == y.score;
+}
+
+// hspDiagEqual (repeat_masker_src/seed_filter.cu:45-50).
+__device__ __forceinline__ bool sa_rec_diag_equal(const SaRec& x, const SaRec& y) {
+    if ((uint32_t)(x.ref_start - x.query_start) != (uint32_t)(y.ref_start - y.query_start)) return false;
+    const bool xin = x.ref_start >= y.ref_start && (uint32_t)(x.ref_start + x.len) <= (uint32_t)(y.ref_start + y.len);
+    const bool yin = y.ref_start >= x.ref_start && (uint32_t)(y.ref_start + y.len) <= (uint32_t)(x.ref_start + x.len);
+    return xin || yin;
+}
+
+__device__ __forceinline__ bool sa_uniq_keep(const SaUniqArgs& u, int buf, uint64_t i) {
+    const SaRec r = u.rec[buf][i];
+    const uint32_t sc = u.scope[buf][i];
+    bool keep = true;
+    if (u.mode != 2 && i > 0) {
+        const SaRec pr = u.rec[buf][i - 1];
+        const uint32_t ps = u.scope[buf][i - 1];
+        if (ps == sc) keep = u.mode == 0 ? !sa_rec_equal(pr, r) : !sa_rec_diag_equal(pr, r);
+    }
+    // Main-diagonal exclusion for the repeat-masker self alignment: scope
+    // flags bit1 = exclusion requested, bit0 = minus strand (never excluded).
+    if (u.mode == 1 && (u.scope_flags[sc] & 3u) == 2u && r.ref_start == r.query_start) keep = false;
+    return keep;
+}
+
+__global__ void __launch_bounds__(256)
+sa_k_uniq_count(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, unsigned long long* cta_a) {
+    const int buf = *src_buf;
+    uint64_t a, b;
+    sa_cta_range(*d_n, a, b);
+    unsigned long long c = 0;
+    for (uint64_t i = a + threadIdx.x; i < b; i += 256) c += sa_uniq_keep(u, buf, i);
+    __shared__ unsigned long long ws[9];
+    unsigned long long tot;
+    sa_block_excl_sum<unsigned long long, 256>(c, ws, &tot);
+    if (threadIdx.x == 0) cta_a[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(256)
+sa_k_uniq_emit(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, const unsigned long long* cta_a) {
+    const int buf = *src_buf;
+    uint64_t a, b;
+    sa_cta_range(*d_n, a, b);
+    unsigned long long base = cta_a[blockIdx.x];
+    SaRec* dr = u.out_rec ? u.out_rec : u.rec[buf ^ 1];
+    uint32_t* ds = u.out_scope ? u.out_scope : u.scope[buf ^ 1];
+    __shared__ unsigned long long ws[9];
+    for (uint64_t r0 = a; r0 < b; r0 += 256) {
+        const uint64_t i = r0 + threadIdx.x;
+        const bool k = i < b && sa_uniq_keep(u, buf, i);
+        unsigned long long tot;
+        const unsigned long long e = sa_block_excl_sum<unsigned long long, 256>((unsigned long long)k, ws, &tot);
+        if (k) {
+            const uint32_t sc = u.scope[buf][i];
+            dr[base + e] = u.rec[buf][i];
+            ds[base + e] = sc;
+            if (u.scope_count) atomicAdd(&u.scope_count[sc], 1u);
+        }
+        base += tot;
+    }
+}
+
+// st[0] <- 1 - final buffer of the last sort (the buffer the unique step wrote).
+__global__ void sa_k_flip_cur(int* st, int np) { st[0] = st[1 + np] ^ 1; }
+
+__global__ void sa_k_dedup_prep(SaCounters* ctr, uint64_t cap, unsigned long long* n0, int* st) {
+    unsigned long long n = ctr->surv_count;
+    if (ctr->surv_overflow) atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_SURV_OVERFLOW);
+    *n0 = n < cap ? n : cap;
+    st[0] = 0;
+}
+
+__global__ void sa_k_copy_u64(unsigned long long* dst, const unsigned long long* src) { *dst = *src; }
+
+static void sa_uniq(SaWork& w, SaUniqArgs u, const unsigned long long* d_n, const int* src_buf,
+                    unsigned long long* d_out_n, int G, cudaStream_t s) {
+    sa_k_uniq_count<<<G, 256, 0, s>>>(u, d_n, src_buf, w.cta_a);
+    sa_k_scan_partials<<<1, 1024, 0, s>>>(w.cta_a, w.cta_b, G, d_out_n, nullptr);
+    sa_k_uniq_emit<<<G, 256, 0, s>>>(u, d_n, src_buf, w.cta_a);
+}
+
+static SaSortSpec spec_of(std::initializer_list<std::pair<uint8_t, uint8_t>> fields_lsd_first) {
+    // each entry: (field, inverted); expanded to 4 byte digits, least significant first
+    SaSortSpec sp{};
+    int n = 0;
+    for (auto& f : fields_lsd_first)
+        for (int byte = 0; byte < 4; ++byte) {
+            sp.field[n] = f.first;
+            sp.byte[n] = (uint8_t)byte;
+            sp.inv[n] = f.second;
+            ++n;
+        }
+    sp.npass = n;
+    return sp;
+}
+
+void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t s) {
+    // Device-side counts live in the spare counter slots.
+    unsigned long long* n0 = &w.ctr->pad[0];
+    unsigned long long* n1 = &w.ctr->pad[1];
+    unsigned long long* n2 = &w.ctr->pad[2];
+    int* st = w.sort_in_buf;
+    sa_k_dedup_prep<<<1, 1, 0, s>>>(w.ctr, w.surv_cap, n0, st);
+    cudaMemsetAsync(w.scope_count, 0, sizeof(uint32_t) * SA_MAX_SCOPES, s);
+
+    // hspComp order: (scope, query_start asc, len desc, ref_start asc).
+    const SaSortSpec plain = spec_of({{F_RS, 0}, {F_LEN, 1}, {F_QS, 0}, {F_SCOPE, 0}});
+    sa_radix_sort_recs(w, plain, n0, st, G, s);
+    SaUniqArgs u{};
+    u.rec[0] = w.rec[0];
+    u.rec[1] = w.rec[1];
+    u.scope[0] = w.scope[0];
+    u.scope[1] = w.scope[1];
+    u.scope_flags = w.scope_flags;
+    if (mode == 0) {
+        u.mode = 0;
+        u.out_rec = w.out;
+        u.out_scope = w.out_scope;
+        u.scope_count = w.scope_count;
+        sa_uniq(w, u, n0, st + 1 + plain.npass, &w.ctr->uniq_count, G, s);
+        return;
+    }
+    // rm: unique(hspEqual) into the other buffer
+    u.mode = 0;
+    sa_uniq(w, u, n0, st + 1 + plain.npass, n1, G, s);
+    sa_k_flip_cur<<<1, 1, 0, s>>>(st, plain.npass);
+    // hspDiagComp: (scope, diag asc, ref_start asc, score desc), stable
+    const SaSortSpec diag = spec_of({{F_SCORE, 1}, {F_RS, 0}, {F_DIAG, 0}, {F_SCOPE, 0}});
+    sa_radix_sort_recs(w, diag, n1, st, G, s);
+    u.mode = 1;
+    sa_uniq(w, u, n1, st + 1 + diag.npass, n2, G, s);
+    sa_k_flip_cur<<<1, 1, 0, s>>>(st, diag.npass);
+    // hspFinalComp: (scope, query_start asc, score desc, ref_start desc), stable
+    const SaSortSpec fin = spec_of({{F_RS, 1}, {F_SCORE, 1}, {F_QS, 0}, {F_SCOPE, 0}});
+    sa_radix_sort_recs(w, fin, n2, st, G, s);
+    u.mode = 2;
+    u.out_rec = w.out;
+    u.out_scope = w.out_scope;
+    u.scope_count = w.scope_count;
+    sa_uniq(w, u, n2, st + 1 + fin.npass, &w.ctr->uniq_count, G, s);
+}

@@ -1,0 +1,161 @@
+"""GPU parity: the sm_100a path through the C ABI against the CPU oracle.
+
+Workload: the 1 Mbp x 1 Mbp plain-method configuration (seeded synthetic
+stand-in), 12of19, HOXD70, xdrop 910, hspthresh 3000, entropy on, both
+strands, 250 kbp WGA chunks.  Integer fields must match bit for bit.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from segalign_b200 import SeedFilter, host_seeds, host_revcomp, build_sub_mat
+from tests.helpers import compare_segments, small_workload, random_text
+
+pytestmark = pytest.mark.gpu
+
+CHUNK = 250_000
+
+
+@pytest.fixture(scope="module")
+def setup(built):
+    w = small_workload()
+    p = oracle.params()
+    idx, pos = oracle.build_table(w.target, p)
+    sf = SeedFilter()
+    sf.initialize_interface(1)
+    sf.generate_shape_pos("12of19")
+    sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(w.target)
+    sf.generate_seed_pos_table(None, 1, 19, 12)
+    sf.send_query_write_request(w.query, 0)
+    return dict(w=w, p=p, idx=idx, pos=pos, sf=sf, R=oracle.encode(w.target), Q=oracle.encode(w.query),
+                QR=oracle.encode_rc(w.query), rctext=host_revcomp(w.query))
+
+
+def test_device_table_matches_oracle(setup):
+    it, pt = setup["sf"].get_seed_pos_table()
+    assert np.array_equal(it, setup["idx"])
+    assert np.array_equal(pt, setup["pos"])
+
+
+@pytest.mark.parametrize("rev", [False, True])
+def test_seed_and_filter_per_chunk(setup, rev):
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    text = setup["rctext"] if rev else w.query
+    qcodes = setup["QR"] if rev else setup["Q"]
+    L = len(w.query) - 19
+    total_hits = 0
+    for j0 in range(0, L, CHUNK):
+        j1 = min(j0 + CHUNK, L)
+        seeds = host_seeds(text, j0, j1)
+        assert np.array_equal(seeds, oracle.chunk_seeds(text, j0, j1, p))
+        got = sf.seed_and_filter(seeds, rev, 0)
+        want, st = oracle.seed_and_filter(p, setup["R"], qcodes, setup["idx"], setup["pos"], seeds, rev)
+        compare_segments(got, want, f"chunk {j0} rev={rev}")
+        cs = sf.last_call_stats()
+        assert cs["num_hits"] == st["num_hits"]
+        assert cs["tiles"] == st["tiles_right"] + st["tiles_left"]
+        total_hits += st["num_hits"]
+    assert total_hits > 100_000
+
+
+def test_seeder_pipeline_matches_oracle(setup):
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    fw, rc, st = sf.seeder_run(w.query, buffer=0, strand=3, num_threads=4)
+    ofw, orc, ost = oracle.pipeline(p, w.target, w.query, setup["idx"], setup["pos"], nthreads=4)
+    compare_segments(fw, ofw, "plus strand")
+    compare_segments(rc, orc, "minus strand")
+    assert st["num_hits"] == ost["num_hits"]
+    assert len(fw) + len(rc) > 200
+
+
+@pytest.mark.parametrize("max_hits", [3000, 20000])
+def test_max_hits_iterations(setup, max_hits):
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    p2 = oracle.params(max_hits=max_hits)
+    sf.set_max_hits(max_hits)
+    try:
+        seeds = host_seeds(w.query, 0, CHUNK)
+        got = sf.seed_and_filter(seeds, False, 0)
+        want, st = oracle.seed_and_filter(p2, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+        assert st["num_iter"] > 1
+        assert sf.last_call_stats()["num_iter"] == st["num_iter"]
+        compare_segments(got, want, f"MAX_HITS={max_hits}")
+    finally:
+        sf.set_max_hits(0)
+
+
+@pytest.mark.parametrize("lane_cap", [8, 32, 512])
+def test_tuning_does_not_change_results(setup, lane_cap):
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    seeds = host_seeds(w.query, 250_000, 500_000)
+    want, _ = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    sf.set_tuning(lane_cap=lane_cap, tile_hits=64 if lane_cap == 8 else 1024)
+    try:
+        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap}")
+    finally:
+        sf.set_tuning(lane_cap=64, tile_hits=1024)
+
+
+def test_host_table_upload(setup):
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    sf.send_seed_pos_table(setup["idx"], setup["pos"])
+    seeds = host_seeds(w.query, 0, CHUNK)
+    want, _ = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    compare_segments(sf.seed_and_filter(seeds, False, 0), want, "host table")
+    sf.generate_seed_pos_table(None, 1, 19, 12)
+
+
+def test_transitions_small(built):
+    rng = np.random.default_rng(7)
+    T = random_text(rng, 200_000, lower=0.01)
+    Q = bytearray(random_text(rng, 200_000))
+    Q[50_000:60_000] = T[100_000:110_000]
+    Q = bytes(Q)
+    p = oracle.params(transition=True)
+    idx, pos = oracle.build_table(T, p)
+    sf = SeedFilter()
+    sf.initialize_interface(1)
+    sf.generate_shape_pos("12of19")
+    sf.initialize_processor(True, 50_000, 19, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(T)
+    sf.generate_seed_pos_table(None, 1, 19, 12)
+    sf.send_query_write_request(Q, 1)
+    R, QC = oracle.encode(T), oracle.encode(Q)
+    for j0 in range(0, len(Q) - 19, 50_000):
+        seeds = host_seeds(Q, j0, min(j0 + 50_000, len(Q) - 19), transition=True)
+        assert np.array_equal(seeds, oracle.chunk_seeds(Q, j0, min(j0 + 50_000, len(Q) - 19), p))
+        got = sf.seed_and_filter(seeds, False, 1)
+        want, _ = oracle.seed_and_filter(p, R, QC, idx, pos, seeds, False)
+        compare_segments(got, want, f"transition chunk {j0}")
+
+
+@pytest.mark.parametrize("exclude", [False, True])
+def test_repeat_masker_self_alignment(built, exclude):
+    w = small_workload(scale=0.5, seed=9)
+    T = w.target
+    p = oracle.params(rm_exclude_diag=exclude)
+    idx, pos = oracle.build_table(T, p)
+    sf = SeedFilter()
+    sf.initialize_interface(1)
+    sf.generate_shape_pos("12of19")
+    sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(T)
+    sf.generate_seed_pos_table(None, 1, 19, 12)
+    sf.rm_send_query_write_request()
+    sf.set_rm_exclude_diagonal(exclude)
+    try:
+        R = oracle.encode(T)
+        RC = oracle.rc_codes(R)
+        rctext = host_revcomp(T)
+        L = len(T)
+        ref_start, ref_end = 50_000, 400_000
+        for rev in (False, True):
+            text = rctext if rev else T
+            seeds = host_seeds(text, 100_000, 300_000)
+            got = sf.rm_seed_and_filter(seeds, rev, ref_start, ref_end)
+            want, st = oracle.seed_and_filter(p, R, RC if rev else R, idx, pos, seeds, rev, 1, ref_start, ref_end)
+            assert st["hits_extended"] < st["num_hits"]
+            compare_segments(got, want, f"rm rev={rev} exclude={exclude}")
+    finally:
+        sf.set_rm_exclude_diagonal(False)
