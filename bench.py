@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 seed-filter path: ungapped extensions/s (and HSPs/s).
+
+Workload (named by its sizes): genome scale, a synthetic 100 Mbp target in 6
+chromosomes against a 108 Mbp query, GC 36%, ~60% of the query built from
+target blocks of 1-50 kbp at 15-35% divergence (5% inverted), 12% repeats,
+8% soft-masking.  12of19 seed, no transitions, HOXD70, xdrop 910, hspthresh
+3000, entropy on, both strands; query intervals of 10 Mbp with 50 kbp
+overlap cut into 250 kbp SeedAndFilter units.
+
+One step = one pass of the hot path over the whole query (both strands):
+  value  batched form, target table + query resident in HBM, seeds generated
+         on the GPU, HSPs left in HBM; device time from CUDA events on the
+         library's stream;
+  e2e    the reference-facing C ABI: the C++ seeder builds each unit's seed
+         words on the host and calls sa_seed_and_filter(), which copies them to
+         the GPU and copies the HSP list back (host wall time);
+  e2e_batched  host query text -> GPU -> batched call -> HSP lists on the host.
+Ranks (torchrun) are weak-scaled: each rank runs its own genome pair of the
+same shape; value = all ranks' extensions / the slowest rank's time.
+
+--impl reference times the reference semantics on the host cores (the CPU
+port in oracle/, the reference's own kernels being GPU-only), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+INTERVAL, OVERLAP, CHUNK, SEED_SIZE = 10_000_000, 50_000, 250_000, 19
+METRIC, UNIT = "ungapped extensions/s", "extensions/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = named sizes)")
+    ap.add_argument("--cpu-chunks", type=int, default=64, help="units in the bounded CPU sample")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def seeder_calls(query_len: int):
+    """SeedAndFilter calls in seeder order: per interval (src/main.cpp:373-386, plus a 50 kbp
+    overlap), its plus-strand chunks then its minus-strand chunks (src/seeder.cpp:47-121)."""
+    L = query_len - SEED_SIZE
+    calls = []
+    for s in range(0, L, INTERVAL):
+        e = min(L, s + INTERVAL + OVERLAP)
+        for i in range(s, e, CHUNK):
+            calls.append((0, 0, i, min(i + CHUNK, e)))
+        rs, re = L - e, L - s
+        for i in range(rs, re, CHUNK):
+            calls.append((0, 1, i, min(i + CHUNK, re)))
+    return calls
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (reference semantics on the host cores)
+# ---------------------------------------------------------------------------
+_TABLES = {}
+
+
+def cpu_sample(w, max_chunks: int, threads: int):
+    import oracle
+
+    p = oracle.params()
+    t = time.perf_counter()
+    key = id(w)
+    if key not in _TABLES:
+        _TABLES[key] = oracle.build_table(w.target, p)
+    idx, pos = _TABLES[key]
+    table_s = time.perf_counter() - t
+    t = time.perf_counter()
+    fw, rc, st = oracle.pipeline(p, w.target, w.query, idx, pos, strand=3, nthreads=threads, interval_size=INTERVAL,
+                                 chunk_size=CHUNK, interval_overlap=OVERLAP, max_chunks=max_chunks)
+    dt = time.perf_counter() - t
+    return dict(seconds=dt, hits=st["num_hits"], hsps=st["num_hsps"], table_s=table_s, fw=fw, rc=rc, stats=st)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from segalign_b200 import synth
+
+    w = synth.make(2, seed=102, scale=args.scale)
+    threads = os.cpu_count() or 1
+    vals = []
+    last = None
+    for k in range(args.warmup + args.steps):
+        r = cpu_sample(w, args.cpu_chunks, threads)
+        if k >= args.warmup:
+            vals.append(r["hits"] / r["seconds"])
+        last = r
+    v = float(statistics.median(vals)) if vals else 0.0
+    sample = (f"first {args.cpu_chunks} SeedAndFilter units (250 kbp, seeder order: interval 0 plus strand, then "
+              f"minus) of the genome-scale workload; {last['hits']} extensions per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * last["seconds"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "genome scale 100 Mbp (6 chr) x 108 Mbp, 12of19, xdrop 910, hspthresh 3000, both "
+                               "strands, 250 kbp units", "sample_units": args.cpu_chunks},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "hsps_per_s": last["hsps"] / last["seconds"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    from segalign_b200 import SeedFilter, build_sub_mat, synth
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allreduce(x: float, op: str) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        return float(t.item())
+
+    # weak scaling: each rank its own genome pair of the same shape
+    w = synth.make(2, seed=102 + 1000 * rank, scale=args.scale)
+    sf = SeedFilter()
+    sf.initialize_interface(1)
+    sf.generate_shape_pos("12of19")
+    os.environ.setdefault("SA_SLOTS_PER_GPU", "4")
+    sf.initialize_processor(False, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(w.target)
+    t = time.perf_counter()
+    sf.generate_seed_pos_table(None, 1, SEED_SIZE, 12)
+    torch.cuda.synchronize()
+    table_ms = 1000 * (time.perf_counter() - t)
+    sf.send_query_write_request(w.query, 0)
+    calls = seeder_calls(len(w.query))
+    plus = [c for c in calls if c[1] == 0]
+    minus = [c for c in calls if c[1] == 1]
+    units = plus + minus
+    unit_of = {c: i for i, c in enumerate(units)}
+    sf.set_timing(True)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # ---- value: batched, device resident ----
+    for _ in range(args.warmup):
+        sf.seed_and_filter_batch(units, keep_on_device=True)
+    barrier()
+    l0 = sf.kernel_launches()
+    dev_ms, hits, hsps, lane_ms, warp_ms, surv, tiles, nnz, longs = [], 0, 0, [], [], 0, 0, 0, 0
+    with ClockSampler(gpu_index(local)) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            sf.seed_and_filter_batch(units, keep_on_device=True)
+            st = sf.last_call_stats()
+            dev_ms.append(st["ms_total"])
+            lane_ms.append(st["ms_extend_lane"])
+            warp_ms.append(st["ms_extend_warp"])
+            hits, hsps, surv, tiles, nnz, longs = (st["num_hits"], st["num_hsps"], st["survivors"], st["tiles"],
+                                                   st["seeds_with_hits"], st["long_hits"])
+        barrier()
+        wall_s = time.perf_counter() - t0
+    launches = sf.kernel_launches() - l0
+    ms_step = sum(dev_ms) / len(dev_ms)
+    ms_step_max = allreduce(ms_step, "max")
+    hits_all = allreduce(float(hits), "sum")
+    hsps_all = allreduce(float(hsps), "sum")
+    value = hits_all / (ms_step_max / 1000.0)
+
+    # roofline of the dominant kernel (lane-per-hit X-drop): algorithmic bytes
+    # = 24 B per hit-bearing seed (E, lo, j, scope, unit) + 4 B per hit (pos)
+    # + 24 B per 32-base tile scanned (2 sequences x 32 bases x 3 bits)
+    # + 16 B per surviving HSP record
+    lane_ms_avg = sum(lane_ms) / len(lane_ms)
+    st_tiles = tiles
+    alg_bytes = 24.0 * nnz + 4.0 * hits + 24.0 * st_tiles + 16.0 * surv
+    peak, peak_src = peaks()
+    achieved = alg_bytes / (lane_ms_avg / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "sa_k_extend_lane", "peak_source": peak_src,
+                "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "genome scale: 100 Mbp target (6 chr) x 108 Mbp query, GC 36%, 12of19, HOXD70, "
+                               "xdrop 910, hspthresh 3000, entropy, both strands, 10 Mbp intervals + 50 kbp overlap, "
+                               "250 kbp units", "path": "batched, device-resident", "units": len(units),
+                   "target_bp": len(w.target), "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)",
+                   "scale": args.scale},
+        "hsps_per_s": hsps_all / (ms_step_max / 1000.0),
+        "extensions_per_step": hits_all, "hsps_per_step": hsps_all,
+        "phase_ms": {"extend_lane": lane_ms_avg, "extend_warp": sum(warp_ms) / len(warp_ms),
+                     "wall_per_step": 1000 * wall_s / args.steps},
+        "table_build_ms": table_ms,
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "counts": {"survivors": surv, "long_hits": longs, "tiles": st_tiles, "seeds_with_hits": nnz},
+    }
+
+    # ---- e2e: reference-facing C ABI (host seeds in, host HSP lists out) ----
+    if not args.no_e2e:
+        k_e2e = args.e2e_steps or max(1, min(args.steps, 3))
+        sf.set_timing(False)
+        sf.seeder_run(w.query, buffer=0, strand=3, num_threads=8, interval_size=INTERVAL, chunk_size=CHUNK,
+                      interval_overlap=OVERLAP)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            fw, rc, sst = sf.seeder_run(w.query, buffer=0, strand=3, num_threads=8, interval_size=INTERVAL,
+                                        chunk_size=CHUNK, interval_overlap=OVERLAP)
+        barrier()
+        e2e_s = (time.perf_counter() - t0) / k_e2e
+        e2e_s_max = allreduce(e2e_s, "max")
+        e2e_hits = allreduce(float(sst["num_hits"]), "sum")
+        # per call: seed words + call descriptor (32 B) + unit (32 B) + scope flags (1 KiB) up;
+        # counters (128 B) + header and HSP records (16 B each) down
+        h2d = sst["num_seeds"] * 8 + sst["num_calls"] * (32 + 32 + 1024)
+        d2h = (sst["num_hsps"] + sst["num_calls"]) * 16 + sst["num_calls"] * 128
+        out["e2e"] = {"value": e2e_hits / e2e_s_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                      "d2h_bytes_per_step": int(d2h), "path": "sa_seed_and_filter per 250 kbp unit from 8 host "
+                      "threads (C++ seeder), host wall time", "steps": k_e2e}
+        # batched with host buffers: query text up, HSP lists down
+        sf.set_timing(True)
+        barrier()
+        t0 = time.perf_counter()
+        outs = None
+        for _ in range(k_e2e):
+            sf.send_query_write_request(w.query, 1)
+            outs = sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
+        barrier()
+        eb_s = allreduce((time.perf_counter() - t0) / k_e2e, "max")
+        out["e2e_batched"] = {"value": e2e_hits / eb_s, "unit": UNIT, "h2d_bytes_per_step": len(w.query),
+                              "d2h_bytes_per_step": int(sum(len(o) for o in outs) * 16)}
+        # bit-exact: batched units == plain per-call results (concatenated per strand)
+        bf = np.concatenate([o[1:] for o in outs[: len(plus)]]) if plus else np.zeros(0)
+        br = np.concatenate([o[1:] for o in outs[len(plus):]]) if minus else np.zeros(0)
+        out["bit_exact_batched_vs_plain"] = bool(
+            len(bf) == len(fw) and len(br) == len(rc) and np.array_equal(bf.view(np.uint32), fw.view(np.uint32))
+            and np.array_equal(br.view(np.uint32), rc.view(np.uint32)))
+        out["batched_vs_plain"] = out["value"] / out["e2e"]["value"]
+
+    # ---- CPU baseline on a bounded sample (rank 0, one GPU only) ----
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        r = cpu_sample(w, args.cpu_chunks, threads)
+        cpu_v = r["hits"] / r["seconds"]
+        out["cpu_baseline"] = {"value": cpu_v, "unit": UNIT, "cores": threads, "kind": "port",
+                               "sample": f"first {args.cpu_chunks} 250 kbp units of the same workload "
+                                         f"({r['hits']} extensions, {r['seconds']:.1f} s)"}
+        if not args.no_e2e:
+            # the sampled calls (seeder order), GPU batched units vs CPU port, bit-exact
+            samp = calls[: args.cpu_chunks]
+            gf = [outs[unit_of[c]][1:] for c in samp if c[1] == 0]
+            gr = [outs[unit_of[c]][1:] for c in samp if c[1] == 1]
+            gf = np.concatenate(gf) if gf else np.zeros(0, dtype=r["fw"].dtype)
+            gr = np.concatenate(gr) if gr else np.zeros(0, dtype=r["rc"].dtype)
+            out["bit_exact_vs_cpu_sample"] = bool(
+                len(gf) == len(r["fw"]) and len(gr) == len(r["rc"])
+                and np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32))
+                and np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))
+
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    sf.shutdown_processor()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -134,6 +134,26 @@ int sa_rm_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, ui
 /* ClearQuery(), repeat_masker_src/seed_filter.cu:937-946. */
 int sa_rm_clear_query(void);
 
+/* ---- batched form (no single reference counterpart) ---- */
+
+/* One unit = one SeedAndFilter call of the reference on the seed words the
+ * host seeder builds for query positions [start, end) of `buffer` on strand
+ * `rev` (src/seeder.cpp:47-121): its output equals sa_seed_and_filter() on
+ * those seeds.  Seeds are generated on the GPU from the resident query. */
+typedef struct {
+    uint32_t buffer;
+    int32_t rev;
+    uint32_t start;
+    uint32_t end;
+} sa_unit;
+
+/* Runs n_units units in as few device passes as the workspace allows.
+ * Unit u's records (header + HSPs) are out[offsets[u] .. offsets[u+1]);
+ * offsets must hold n_units + 1 entries.  With out == NULL and out_len ==
+ * NULL the HSPs stay on the device and only sa_last_call_stats() is filled. */
+int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment** out, uint64_t* out_len,
+                             uint64_t* offsets);
+
 /* ---- results, configuration, diagnostics (no reference counterpart) ---- */
 
 void sa_free_segments(sa_segment* segments);
@@ -157,10 +177,19 @@ typedef struct {
     uint64_t tiles;          /* 32-base tiles the reference would scan          */
     uint32_t num_iter;       /* MAX_HITS iterations                            */
     uint32_t pad;
+    /* device time of the call's phases (CUDA events on the call's stream),
+     * filled when sa_set_timing(1) is on */
+    double ms_total, ms_lookup, ms_extend_lane, ms_extend_warp, ms_dedup, ms_copy;
 } sa_call_stats;
 
 /* Statistics of the calling thread's last sa_*seed_and_filter* call. */
 int sa_last_call_stats(sa_call_stats* stats);
+
+/* Per-phase device timing of the following calls (CUDA events); off by default. */
+int sa_set_timing(int on);
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t sa_kernel_launches(void);
 
 /* Message of the calling thread's last error. */
 const char* sa_last_error(void);

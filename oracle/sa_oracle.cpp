@@ -392,13 +392,31 @@ static void table_geometry(uint32_t len, uint32_t step, const or_params* p, uint
     *num_steps = span > 0 ? (uint64_t)(span / step) : 0;
 }
 
-uint64_t or_table_count(const char* text, uint32_t len, uint32_t step, const or_params* p) {
+// Keys of all table positions, computed with std::threads (the reference
+// uses a TBB parallel_for, common/seed_pos_table.cu:69-81).
+static void table_keys(const char* text, uint32_t len, uint32_t step, const or_params* p,
+                       std::vector<uint32_t>& keys, uint32_t* start_out) {
     uint32_t start;
     uint64_t n;
     table_geometry(len, step, p, &start, &n);
+    *start_out = start;
+    keys.resize(n);
+    unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t)
+        th.emplace_back([&, t]() {
+            uint64_t a = n * t / nt, b = n * (t + 1) / nt;
+            for (uint64_t i = a; i < b; ++i) keys[i] = or_kmer_index(text, start + i * step, p);
+        });
+    for (auto& x : th) x.join();
+}
+
+uint64_t or_table_count(const char* text, uint32_t len, uint32_t step, const or_params* p) {
+    std::vector<uint32_t> keys;
+    uint32_t start;
+    table_keys(text, len, step, p, keys, &start);
     uint64_t c = 0;
-    for (uint64_t i = 0; i < n; ++i)
-        if (or_kmer_index(text, start + i * step, p) != INVALID_KMER) ++c;
+    for (uint32_t k : keys) c += k != INVALID_KMER;
     return c;
 }
 
@@ -410,16 +428,13 @@ int or_build_table(const char* text, uint32_t len, uint32_t step, const or_param
                    uint32_t* index_table, uint32_t* pos_table, uint64_t pos_cap,
                    uint64_t* num_index) {
     uint32_t start;
-    uint64_t n;
-    table_geometry(len, step, p, &start, &n);
+    std::vector<uint32_t> keys;
+    table_keys(text, len, step, p, keys, &start);
+    const uint64_t n = keys.size();
     const uint64_t nb = 1ull << (2 * p->kmer_size);
-    std::vector<uint32_t> keys(n);
     std::vector<uint64_t> cnt(nb + 1, 0);
-    for (uint64_t i = 0; i < n; ++i) {
-        uint32_t k = or_kmer_index(text, start + i * step, p);
-        keys[i] = k;
-        if (k != INVALID_KMER) cnt[k + 1]++;
-    }
+    for (uint64_t i = 0; i < n; ++i)
+        if (keys[i] != INVALID_KMER) cnt[keys[i] + 1]++;
     for (uint64_t k = 1; k <= nb; ++k) cnt[k] += cnt[k - 1];
     uint64_t total = cnt[nb];
     *num_index = total;

@@ -46,6 +46,7 @@ EXPORTS = [
     "sa_rm_send_query_write_request", "sa_rm_seed_and_filter", "sa_rm_clear_query", "sa_free_segments",
     "sa_set_max_hits", "sa_set_rm_exclude_diagonal", "sa_last_call_stats", "sa_last_error", "sa_set_tuning",
     "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
+    "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches",
 ]
 
 
@@ -58,13 +59,20 @@ class SegAlignError(RuntimeError):
 class CallStats(C.Structure):
     _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("hits_extended", C.c_uint64),
                 ("seeds_with_hits", C.c_uint64), ("survivors", C.c_uint64), ("num_hsps", C.c_uint64),
-                ("long_hits", C.c_uint64), ("tiles", C.c_uint64), ("num_iter", C.c_uint32), ("pad", C.c_uint32)]
+                ("long_hits", C.c_uint64), ("tiles", C.c_uint64), ("num_iter", C.c_uint32), ("pad", C.c_uint32),
+                ("ms_total", C.c_double), ("ms_lookup", C.c_double), ("ms_extend_lane", C.c_double),
+                ("ms_extend_warp", C.c_double), ("ms_dedup", C.c_double), ("ms_copy", C.c_double)]
 
 
 class SeederCfg(C.Structure):
     _fields_ = [("interval_size", C.c_uint32), ("interval_overlap", C.c_uint32), ("chunk_size", C.c_uint32),
                 ("strand", C.c_int32), ("num_threads", C.c_int32), ("buffer", C.c_uint32),
                 ("max_chunks", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class Unit(C.Structure):
+    """sa_unit: seed positions [start, end) of query buffer `buffer` on strand `rev`."""
+    _fields_ = [("buffer", C.c_uint32), ("rev", C.c_int32), ("start", C.c_uint32), ("end", C.c_uint32)]
 
 
 class SeederStats(C.Structure):
@@ -117,6 +125,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_build_sub_mat": (C.c_int, [C.c_int, C.c_char_p, i32p]),
             "sa_seeder_run": (C.c_int, [_P(SeederCfg), C.c_char_p, C.c_uint32, segpp, u64p, segpp, u64p,
                                         _P(SeederStats)]),
+            "sa_seed_and_filter_batch": (C.c_int, [_P(Unit), C.c_uint32, segpp, u64p, u64p]),
+            "sa_set_timing": (C.c_int, [C.c_int]),
+            "sa_kernel_launches": (C.c_uint64, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -260,6 +271,23 @@ class SeedFilter:
     def shutdown_processor(self) -> None:
         self._chk(self.lib.sa_shutdown_processor(), "ShutdownProcessor")
 
+    def seed_and_filter_batch(self, units, keep_on_device: bool = False):
+        """Batched form: units = [(buffer, rev, start, end), ...].
+
+        Returns one header+HSP array per unit (as seed_and_filter would for the
+        host seeds of that window), or None with keep_on_device=True.
+        """
+        arr = (Unit * max(len(units), 1))(*[Unit(b, int(r), s, e) for (b, r, s, e) in units])
+        if keep_on_device:
+            self._chk(self.lib.sa_seed_and_filter_batch(arr, len(units), None, None, None), "SeedAndFilterBatch")
+            return None
+        ptr, n = _P(C.c_uint8)(), C.c_uint64()
+        offs = np.zeros(len(units) + 1, dtype=np.uint64)
+        self._chk(self.lib.sa_seed_and_filter_batch(arr, len(units), C.byref(ptr), C.byref(n), _u64p(offs)),
+                  "SeedAndFilterBatch")
+        allsegs = _take_segments(self.lib, ptr, n.value)
+        return [allsegs[int(offs[i]):int(offs[i + 1])] for i in range(len(units))]
+
     # ---- repeat_masker_src/seed_filter.cu ----
     def rm_send_query_write_request(self) -> None:
         self._chk(self.lib.sa_rm_send_query_write_request(), "SendQueryWriteRequest(rm)")
@@ -283,6 +311,12 @@ class SeedFilter:
 
     def set_tuning(self, lane_cap=-1, ext_block=-1, ext_ctas_per_sm=-1, tile_hits=-1) -> None:
         self._chk(self.lib.sa_set_tuning(lane_cap, ext_block, ext_ctas_per_sm, tile_hits), "set_tuning")
+
+    def set_timing(self, on: bool) -> None:
+        self.lib.sa_set_timing(int(on))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.sa_kernel_launches())
 
     def last_call_stats(self) -> dict:
         st = CallStats()

@@ -6,6 +6,7 @@
 // place of exit(); a pool of slots (stream + workspace) per GPU in place of
 // one lock per GPU; host pointers in place of the query_DRAM global.
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
@@ -24,6 +25,10 @@
 // ---------------------------------------------------------------------------
 static thread_local std::string t_err;
 static thread_local sa_call_stats t_stats;
+static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<int> g_timing{0};
+
+void sa_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void sa_set_error(int, const char* fmt, ...) {
     char buf[512];
@@ -75,7 +80,9 @@ struct DevState {
     uint32_t* pos = nullptr;
     uint64_t num_index = 0;
     Packed qf[kMaxBuffers], qr[kMaxBuffers];
+    uint32_t* qkeys[kMaxBuffers][2] = {};  // per-position seed keys (batched seeding)
     std::vector<Slot*> slots;
+    Slot* batch = nullptr;                 // workspace of batched calls
 };
 
 struct Slot {
@@ -90,10 +97,38 @@ struct Slot {
     uint32_t* h_scope_count = nullptr;
     SaRec* h_out = nullptr;
     uint64_t h_out_cap = 0;
+    cudaEvent_t ev[6] = {};
+};
+
+// Phase timing with CUDA events on the slot stream (enabled by sa_set_timing).
+struct PhaseTimer {
+    Slot* s;
+    bool on;
+    PhaseTimer(Slot* slot) : s(slot), on(g_timing.load() != 0) {}
+    void mark(int i) {
+        if (on) cudaEventRecord(s->ev[i], s->stream);
+    }
+    // after the stream is synchronized
+    void collect(sa_call_stats& st) {
+        if (!on) return;
+        float a = 0, b = 0, b2 = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, s->ev[0], s->ev[1]);
+        cudaEventElapsedTime(&b, s->ev[1], s->ev[2]);
+        cudaEventElapsedTime(&b2, s->ev[2], s->ev[3]);
+        cudaEventElapsedTime(&c, s->ev[3], s->ev[4]);
+        cudaEventElapsedTime(&d, s->ev[4], s->ev[5]);
+        st.ms_lookup += a;
+        st.ms_extend_lane += b;
+        st.ms_extend_warp += b2;
+        st.ms_dedup += c;
+        st.ms_copy += d;
+        st.ms_total += a + b + b2 + c + d;
+    }
 };
 
 struct Global {
     std::mutex mu;
+    std::mutex batch_mu;  // one batched call at a time
     std::condition_variable cv;
     std::deque<Slot*> free_slots;
     std::vector<DevState> devs;
@@ -116,6 +151,8 @@ struct Global {
     uint32_t ref_len = 0;
     uint64_t surv_cap = 0;
     uint64_t long_cap = 0;
+    uint64_t batch_slot_cap = 0;
+    uint64_t batch_surv_cap = 0;
 };
 
 Global& G() {
@@ -186,11 +223,14 @@ void free_slot(Slot* s) {
     if (s->h_scope_flags) cudaFreeHost(s->h_scope_flags);
     if (s->h_scope_count) cudaFreeHost(s->h_scope_count);
     if (s->h_out) cudaFreeHost(s->h_out);
+    for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
     delete s;
 }
 
 // Carves one slot workspace out of a single device allocation.
-int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_cap, Slot** out) {
+int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_cap, Slot** out,
+              bool batch = false) {
     DevState& d = G().devs[dev_idx];
     SA_CUDA_OK(cudaSetDevice(d.dev));
     Slot* s = new Slot();
@@ -203,11 +243,12 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
     w.seed_cap = seed_cap;
     w.surv_cap = surv_cap;
     w.long_cap = long_cap;
+    const uint64_t nunits = batch ? SA_MAX_UNITS : 64;
     std::vector<Part> parts = {
-        {(void**)&w.seeds, 8 * seed_cap},
+        {(void**)&w.seeds, batch ? 0 : 8 * seed_cap},
         {(void**)&w.s_lo, 4 * seed_cap},
         {(void**)&w.s_cnt, 4 * seed_cap},
-        {(void**)&w.s_P, 8 * seed_cap},
+        {(void**)&w.s_P, batch ? 0 : 8 * seed_cap},
         {(void**)&w.cs.E, 8 * (seed_cap + 1)},
         {(void**)&w.cs.lo, 4 * (seed_cap + 1)},
         {(void**)&w.cs.qpos, 4 * (seed_cap + 1)},
@@ -230,10 +271,15 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
         {(void**)&w.sort_in_buf, 4 * (SA_SORT_MAX_DIGITS + 2)},
         {(void**)&w.ctr, sizeof(SaCounters)},
         {(void**)&w.desc, sizeof(SaCallDesc)},
-        {(void**)&w.units, sizeof(SaUnit) * 64},
+        {(void**)&w.units, sizeof(SaUnit) * nunits},
+        {(void**)&w.bunits, batch ? sizeof(SaBatchUnit) * nunits : 0},
+        {(void**)&w.unit_hit_base, batch ? 8 * nunits : 0},
+        {(void**)&w.unit_hit_end, batch ? 8 * nunits : 0},
+        {(void**)&w.bounds, batch ? 8 * nunits * SA_BATCH_ITERS : 0},
+        {(void**)&w.unit_iters, batch ? 4 * nunits : 0},
+        {(void**)&w.keys_arrays, batch ? 8 * SA_MAX_KEY_ARRAYS : 0},
     };
     w.flags = nullptr;
-    w.bunits = nullptr;
     uint64_t total = 0;
     for (auto& p : parts) total += (p.bytes + 255) & ~255ull;
     cudaError_t e = cudaMalloc(&s->arena, total);
@@ -249,9 +295,12 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&s->h_ctr, sizeof(SaCounters)) != cudaSuccess ||
         cudaMallocHost(&s->h_desc, sizeof(SaCallDesc)) != cudaSuccess ||
-        cudaMallocHost(&s->h_units, sizeof(SaUnit) * 64) != cudaSuccess ||
+        cudaMallocHost(&s->h_units, sizeof(SaUnit) * nunits) != cudaSuccess ||
         cudaMallocHost(&s->h_scope_flags, 4 * SA_MAX_ITERS) != cudaSuccess ||
-        cudaMallocHost(&s->h_scope_count, 4 * SA_MAX_ITERS) != cudaSuccess) {
+        cudaMallocHost(&s->h_scope_count, 4 * SA_MAX_ITERS) != cudaSuccess ||
+        cudaEventCreate(&s->ev[0]) != cudaSuccess || cudaEventCreate(&s->ev[1]) != cudaSuccess ||
+        cudaEventCreate(&s->ev[2]) != cudaSuccess || cudaEventCreate(&s->ev[3]) != cudaSuccess ||
+        cudaEventCreate(&s->ev[4]) != cudaSuccess || cudaEventCreate(&s->ev[5]) != cudaSuccess) {
         free_slot(s);
         sa_set_error(SA_ERR_NOMEM, "pinned host allocation failed");
         return SA_ERR_NOMEM;
@@ -320,12 +369,15 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     u[0].flags = mode == 1 ? (1u | (rev ? 2u : 0u)) : 0u;
     for (int i = 0; i < SA_MAX_ITERS; ++i)
         s->h_scope_flags[i] = (rev ? 1u : 0u) | ((mode == 1 && g.rm_exclude_diag) ? 2u : 0u);
+    PhaseTimer tm(s);
+    tm.mark(0);
     SA_CUDA_OK(cudaMemcpyAsync(w.seeds, seeds, 8ull * n, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.desc, hd, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.units, u, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
     sa_launch_lookup_seeds(w, d.index, (uint32_t)d.nbuckets, g.params, Gr, st);
+    tm.mark(1);
     SaExtendArgs xa;
     xa.ref = d.ref.data;
     xa.ref_len = (uint32_t)d.ref.len;
@@ -334,8 +386,12 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     xa.xdrop = g.params.xdrop;
     xa.hspthresh = g.params.hspthresh;
     xa.noentropy = g.params.noentropy;
-    sa_launch_extend(w, xa, g.params, g.tuning, d.num_sms, st);
-    sa_launch_dedup(w, mode, Gr, st);
+    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(2);
+    sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(3);
+    sa_launch_dedup(w, mode, 0, Gr, st);
+    tm.mark(4);
     SA_CUDA_OK(cudaGetLastError());
     SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
@@ -361,7 +417,9 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
         s->h_out_cap = cap;
     }
     if (nh) SA_CUDA_OK(cudaMemcpyAsync(s->h_out + 1, w.out, nh * sizeof(SaRec), cudaMemcpyDeviceToHost, st));
+    tm.mark(5);
     SA_CUDA_OK(cudaStreamSynchronize(st));
+    tm.collect(t_stats);
     // header (src/seed_filter.cu:756-759): len = total anchors, score = num_hits
     s->h_out[0].ref_start = 0;
     s->h_out[0].query_start = 0;
@@ -395,6 +453,181 @@ int check_ready(bool need_query) {
         }
     }
     (void)need_query;
+    return SA_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched calls: many (query window, strand) units in one launch sequence,
+// seeded on the device from the resident query.  Each unit's output equals
+// what sa_seed_and_filter() returns for the seed words the host seeder would
+// build for that window (src/seeder.cpp:57-74).
+// ---------------------------------------------------------------------------
+int ensure_keys(DevState& d, uint32_t buffer, int rev) {
+    Global& g = G();
+    if (d.qkeys[buffer][rev]) return SA_OK;
+    const Packed& q = rev ? d.qr[buffer] : d.qf[buffer];
+    if (!q.data) {
+        sa_set_error(SA_ERR_STATE, "query buffer %u is not resident", buffer);
+        return SA_ERR_STATE;
+    }
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    SA_CUDA_OK(cudaMalloc(&d.qkeys[buffer][rev], 4 * (q.len ? q.len : 1)));
+    sa_launch_query_keys(q.data, q.len, g.params, d.qkeys[buffer][rev], 0);
+    SA_CUDA_OK(cudaDeviceSynchronize());
+    return SA_OK;
+}
+
+void drop_keys(DevState& d, uint32_t buffer) {
+    for (int r = 0; r < 2; ++r)
+        if (d.qkeys[buffer][r]) {
+            cudaFree(d.qkeys[buffer][r]);
+            d.qkeys[buffer][r] = nullptr;
+        }
+}
+
+struct BatchResult {
+    std::vector<std::vector<SaRec>> recs;  // per unit (body only)
+    std::vector<uint64_t> hits;            // per unit
+    SaCounters tot{};
+    sa_call_stats timing{};
+};
+
+// Runs units [u0, u1) of `units` in one device pass.  Returns SA_ERR_CAPACITY
+// when the survivors do not fit (the caller splits the range).
+int run_batch_group(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uint32_t u1, bool want_out,
+                    BatchResult& res) {
+    Global& g = G();
+    SaWork& w = s->w;
+    cudaStream_t st = s->stream;
+    SA_CUDA_OK(cudaSetDevice(d.dev));
+    const int S = g.params.transition ? 1 + g.params.kmer_size : 1;
+    const uint32_t n = u1 - u0;
+    std::vector<SaBatchUnit> bu(n);
+    std::vector<const uint32_t*> karr(SA_MAX_KEY_ARRAYS, nullptr);
+    SaUnit* hu = s->h_units;
+    uint64_t slots = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const sa_unit& u = units[u0 + i];
+        const int rev = u.rev ? 1 : 0;
+        const Packed& q = rev ? d.qr[u.buffer] : d.qf[u.buffer];
+        bu[i].slot_begin = slots;
+        bu[i].q_start = u.start;
+        bu[i].q_end = u.end;
+        bu[i].keys_index = u.buffer * 2 + rev;
+        bu[i].unit = i;
+        karr[u.buffer * 2 + rev] = d.qkeys[u.buffer][rev];
+        hu[i].q_packed = q.data;
+        hu[i].q_len = (uint32_t)q.len;
+        hu[i].rm_lo = hu[i].rm_hi = 0;
+        hu[i].flags = 0;
+        slots += (uint64_t)(u.end - u.start) * S;
+    }
+    SaCallDesc* hd = s->h_desc;
+    hd->num_seeds = slots;
+    hd->max_hits = max_hits_now();
+    hd->num_units = n;
+    hd->num_scopes_max = n;
+    hd->rm_exclude_diag = 0;
+    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
+    PhaseTimer tm(s);
+    tm.mark(0);
+    SA_CUDA_OK(cudaMemcpyAsync(w.bunits, bu.data(), sizeof(SaBatchUnit) * n, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.units, hu, sizeof(SaUnit) * n, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync((void*)w.keys_arrays, karr.data(), 8 * SA_MAX_KEY_ARRAYS, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.desc, hd, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemsetAsync(w.scope_flags, 0, 4 * n, st));
+    SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
+    sa_launch_lookup_batch(w, d.index, (uint32_t)d.nbuckets, w.keys_arrays, n, g.params, Gr, st);
+    tm.mark(1);
+    SaExtendArgs xa;
+    xa.ref = d.ref.data;
+    xa.ref_len = (uint32_t)d.ref.len;
+    xa.pos_table = d.pos;
+    xa.seed_size = (uint32_t)g.params.seed_size;
+    xa.xdrop = g.params.xdrop;
+    xa.hspthresh = g.params.hspthresh;
+    xa.noentropy = g.params.noentropy;
+    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(2);
+    sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(3);
+    sa_launch_dedup(w, 0, 4, Gr, st);
+    tm.mark(4);
+    SA_CUDA_OK(cudaGetLastError());
+    SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
+    SA_CUDA_OK(cudaStreamSynchronize(st));
+    SaCounters c = *s->h_ctr;
+    if (c.surv_overflow) return SA_ERR_CAPACITY;
+    if (c.error) return map_device_error(c.error);
+    res.tot.num_hits += c.num_hits;
+    res.tot.extended += c.extended;
+    res.tot.nnz += c.nnz;
+    res.tot.surv_count += c.surv_count;
+    res.tot.uniq_count += c.uniq_count;
+    res.tot.long_count += c.long_count;
+    res.tot.base_steps += c.base_steps;
+    std::vector<unsigned long long> hb(n), he(n);
+    std::vector<uint32_t> cnt(n);
+    SA_CUDA_OK(cudaMemcpyAsync(hb.data(), w.unit_hit_base, 8ull * n, cudaMemcpyDeviceToHost, st));
+    SA_CUDA_OK(cudaMemcpyAsync(he.data(), w.unit_hit_end, 8ull * n, cudaMemcpyDeviceToHost, st));
+    SA_CUDA_OK(cudaMemcpyAsync(cnt.data(), w.scope_count, 4ull * n, cudaMemcpyDeviceToHost, st));
+    const uint64_t nh = c.uniq_count;
+    if (want_out && nh + 1 > s->h_out_cap) {
+        SA_CUDA_OK(cudaStreamSynchronize(st));
+        if (s->h_out) cudaFreeHost(s->h_out);
+        s->h_out = nullptr;
+        uint64_t cap = std::max<uint64_t>(nh + 1, std::max<uint64_t>(1 << 16, s->h_out_cap * 2));
+        SA_CUDA_OK(cudaMallocHost(&s->h_out, cap * sizeof(SaRec)));
+        s->h_out_cap = cap;
+    }
+    if (want_out && nh) SA_CUDA_OK(cudaMemcpyAsync(s->h_out, w.out, nh * sizeof(SaRec), cudaMemcpyDeviceToHost, st));
+    tm.mark(5);
+    SA_CUDA_OK(cudaStreamSynchronize(st));
+    tm.collect(res.timing);
+    uint64_t at = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        res.hits[u0 + i] = he[i] - hb[i];
+        if (want_out) res.recs[u0 + i].assign(s->h_out + at, s->h_out + at + cnt[i]);
+        at += cnt[i];
+    }
+    return SA_OK;
+}
+
+int run_batch_range(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uint32_t u1, bool want_out,
+                    BatchResult& res) {
+    Global& g = G();
+    const uint64_t S = g.params.transition ? 1 + g.params.kmer_size : 1;
+    // split by seed-slot capacity and unit count
+    uint32_t a = u0;
+    while (a < u1) {
+        uint32_t b = a;
+        uint64_t slots = 0;
+        while (b < u1 && b - a < SA_MAX_UNITS) {
+            uint64_t add = (uint64_t)(units[b].end - units[b].start) * S;
+            if (b > a && slots + add > s->w.seed_cap) break;
+            if (add > s->w.seed_cap) {
+                sa_set_error(SA_ERR_CAPACITY, "one unit needs %llu seed slots (capacity %llu, SA_BATCH_SLOT_CAP)",
+                             (unsigned long long)add, (unsigned long long)s->w.seed_cap);
+                return SA_ERR_CAPACITY;
+            }
+            slots += add;
+            ++b;
+        }
+        int r = run_batch_group(d, s, units, a, b, want_out, res);
+        if (r == SA_ERR_CAPACITY) {
+            if (b - a == 1) {
+                sa_set_error(SA_ERR_CAPACITY, "survivors of one unit exceed SA_BATCH_SURV_CAP");
+                return r;
+            }
+            uint32_t m = a + (b - a) / 2;
+            SA_TRY(run_batch_range(d, s, units, a, m, want_out, res));
+            SA_TRY(run_batch_range(d, s, units, m, b, want_out, res));
+        } else if (r != SA_OK) {
+            return r;
+        }
+        a = b;
+    }
     return SA_OK;
 }
 
@@ -666,7 +899,12 @@ int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_si
         std::lock_guard<std::mutex> lk(g.mu);
         for (auto* s : g.free_slots) free_slot(s);
         g.free_slots.clear();
-        for (auto& d : g.devs) d.slots.clear();
+        for (auto& d : g.devs) {
+            d.slots.clear();
+            if (d.batch) free_slot(d.batch);
+            d.batch = nullptr;
+            for (int b = 0; b < kMaxBuffers; ++b) drop_keys(d, b);
+        }
     }
     for (int i = 0; i < 64; ++i) g.params.sub_mat[i] = sub_mat[i];
     g.params.xdrop = xdrop;
@@ -680,6 +918,8 @@ int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_si
     g.max_hits_default = (uint64_t)(int)(4194304 * gb);
     g.surv_cap = env_u64("SA_SURV_CAP", 1ull << 25);
     g.long_cap = env_u64("SA_LONG_CAP", 1ull << 24);
+    g.batch_slot_cap = env_u64("SA_BATCH_SLOT_CAP", 1ull << 28);
+    g.batch_surv_cap = env_u64("SA_BATCH_SURV_CAP", 1ull << 29);
     const int per_gpu = (int)env_u64("SA_SLOTS_PER_GPU", 2);
     for (size_t di = 0; di < g.devs.size(); ++di) {
         for (int k = 0; k < per_gpu; ++k) {
@@ -702,7 +942,10 @@ int sa_send_query_write_request(const char* query_buffer, size_t start_addr, uin
         sa_set_error(SA_ERR_ARG, "query buffer pointer required and buffer < %d", kMaxBuffers);
         return SA_ERR_ARG;
     }
-    for (auto& d : g.devs) SA_TRY(upload_pack(d, query_buffer + start_addr, len, d.qf[buffer], &d.qr[buffer]));
+    for (auto& d : g.devs) {
+        drop_keys(d, buffer);
+        SA_TRY(upload_pack(d, query_buffer + start_addr, len, d.qf[buffer], &d.qr[buffer]));
+    }
     return SA_OK;
 }
 
@@ -739,6 +982,7 @@ int sa_clear_query(uint32_t buffer) {
         cudaSetDevice(d.dev);
         d.qf[buffer].release();
         d.qr[buffer].release();
+        drop_keys(d, buffer);
     }
     return SA_OK;
 }
@@ -802,13 +1046,18 @@ int sa_shutdown_processor(void) {
         for (auto& d : g.devs)
             for (auto* s : d.slots) free_slot(s);
         g.free_slots.clear();
-        for (auto& d : g.devs) d.slots.clear();
+        for (auto& d : g.devs) {
+            d.slots.clear();
+            if (d.batch) free_slot(d.batch);
+            d.batch = nullptr;
+        }
     }
     for (auto& d : g.devs) {
         cudaSetDevice(d.dev);
         for (int b = 0; b < kMaxBuffers; ++b) {
             d.qf[b].release();
             d.qr[b].release();
+            drop_keys(d, b);
         }
     }
     sa_clear_ref();
@@ -816,7 +1065,97 @@ int sa_shutdown_processor(void) {
     return SA_OK;
 }
 
+
+// Batched SeedAndFilter (no single reference counterpart; each unit reproduces
+// one src/seed_filter.cu:654-778 call on the seeds of src/seeder.cpp:57-74).
+int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment** out, uint64_t* out_len,
+                             uint64_t* offsets) {
+    SA_TRY(check_ready(true));
+    Global& g = G();
+    if (!units && n_units) return SA_ERR_ARG;
+    if ((out == nullptr) != (out_len == nullptr) || (out && !offsets)) return SA_ERR_ARG;
+    DevState& d = g.devs[0];
+    for (uint32_t i = 0; i < n_units; ++i) {
+        const sa_unit& u = units[i];
+        if (u.buffer >= (uint32_t)kMaxBuffers || u.start > u.end) {
+            sa_set_error(SA_ERR_ARG, "unit %u: buffer < %d and start <= end required", i, kMaxBuffers);
+            return SA_ERR_ARG;
+        }
+        const Packed& q = u.rev ? d.qr[u.buffer] : d.qf[u.buffer];
+        if (!q.data || u.end > q.len) {
+            sa_set_error(SA_ERR_STATE, "unit %u: query buffer %u not resident or window past its end", i, u.buffer);
+            return SA_ERR_STATE;
+        }
+    }
+    std::lock_guard<std::mutex> lk(g.batch_mu);
+    if (!d.batch) {
+        Slot* s = nullptr;
+        SA_TRY(make_slot(0, g.batch_slot_cap, g.batch_surv_cap, g.long_cap, &s, true));
+        d.batch = s;
+    }
+    for (uint32_t i = 0; i < n_units; ++i) SA_TRY(ensure_keys(d, units[i].buffer, units[i].rev ? 1 : 0));
+    // units with an empty window produce a header only
+    std::vector<sa_unit> live;
+    std::vector<uint32_t> live_idx;
+    for (uint32_t i = 0; i < n_units; ++i)
+        if (units[i].end > units[i].start) {
+            live.push_back(units[i]);
+            live_idx.push_back(i);
+        }
+    BatchResult res;
+    res.recs.resize(live.size());
+    res.hits.assign(live.size(), 0);
+    SA_TRY(run_batch_range(d, d.batch, live.data(), 0, (uint32_t)live.size(), out != nullptr, res));
+    std::memset(&t_stats, 0, sizeof t_stats);
+    t_stats.num_hits = res.tot.num_hits;
+    t_stats.hits_extended = res.tot.extended;
+    t_stats.seeds_with_hits = res.tot.nnz;
+    t_stats.survivors = res.tot.surv_count;
+    t_stats.num_hsps = res.tot.uniq_count;
+    t_stats.long_hits = res.tot.long_count;
+    t_stats.tiles = res.tot.base_steps;
+    t_stats.num_iter = 1;
+    t_stats.ms_total = res.timing.ms_total;
+    t_stats.ms_lookup = res.timing.ms_lookup;
+    t_stats.ms_extend_lane = res.timing.ms_extend_lane;
+    t_stats.ms_extend_warp = res.timing.ms_extend_warp;
+    t_stats.ms_dedup = res.timing.ms_dedup;
+    t_stats.ms_copy = res.timing.ms_copy;
+    if (!out) return SA_OK;
+    uint64_t total = n_units;
+    for (auto& r : res.recs) total += r.size();
+    sa_segment* o = (sa_segment*)malloc(sizeof(sa_segment) * (total ? total : 1));
+    if (!o) return SA_ERR_NOMEM;
+    std::vector<int64_t> map(n_units, -1);
+    for (size_t k = 0; k < live_idx.size(); ++k) map[live_idx[k]] = (int64_t)k;
+    uint64_t at = 0;
+    for (uint32_t i = 0; i < n_units; ++i) {
+        offsets[i] = at;
+        const int64_t k = map[i];
+        const uint64_t nb = k >= 0 ? res.recs[k].size() : 0;
+        const uint64_t hits = k >= 0 ? res.hits[k] : 0;
+        o[at].ref_start = 0;
+        o[at].query_start = 0;
+        o[at].len = (uint32_t)nb;
+        o[at].score = (int32_t)(uint32_t)hits;
+        ++at;
+        if (nb) std::memcpy(o + at, res.recs[k].data(), nb * sizeof(sa_segment));
+        at += nb;
+    }
+    offsets[n_units] = at;
+    *out = o;
+    *out_len = at;
+    return SA_OK;
+}
+
 void sa_free_segments(sa_segment* p) { free(p); }
+
+int sa_set_timing(int on) {
+    g_timing = on ? 1 : 0;
+    return SA_OK;
+}
+
+uint64_t sa_kernel_launches(void) { return g_launches.load(); }
 
 int sa_set_max_hits(uint64_t max_hits) {
     G().max_hits_override = max_hits;

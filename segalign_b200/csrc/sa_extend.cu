@@ -530,8 +530,7 @@ sa_k_extend_warp(SaExtK a, SaParams P) {
     if (lane == 0) atomicAdd(&a.ctr->base_steps, tiles_acc);
 }
 
-void sa_launch_extend(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
-                      cudaStream_t st) {
+static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     SaExtK a;
     a.ref = x.ref;
     a.ref_len = x.ref_len;
@@ -550,6 +549,17 @@ void sa_launch_extend(SaWork& w, const SaExtendArgs& x, const SaParams& p, const
     a.noentropy = x.noentropy;
     a.lane_cap = (uint32_t)t.lane_cap;
     a.tile_hits = (uint32_t)t.tile_hits;
-    sa_k_extend_lane<<<num_sms * t.ext_ctas_per_sm, t.ext_block, 0, st>>>(a, p);
-    sa_k_extend_warp<<<num_sms * 4, t.long_block, 0, st>>>(a, p);
+    return a;
+}
+
+void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
+                           cudaStream_t st) {
+    sa_k_extend_lane<<<num_sms * t.ext_ctas_per_sm, t.ext_block, 0, st>>>(sa_ext_args(w, x, t), p);
+    sa_note_launch();
+}
+
+void sa_launch_extend_warp(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
+                           cudaStream_t st) {
+    sa_k_extend_warp<<<num_sms * 4, t.long_block, 0, st>>>(sa_ext_args(w, x, t), p);
+    sa_note_launch();
 }

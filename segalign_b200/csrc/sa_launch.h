@@ -17,6 +17,9 @@ struct SaCallDesc {
     uint32_t pad;
 };
 
+#define SA_BATCH_ITERS 16
+#define SA_MAX_KEY_ARRAYS 16
+
 // Batched unit: a query window [start, end) of one packed query, seeded on the device.
 struct SaBatchUnit {
     uint64_t slot_begin;    // first seed slot of the unit in the flattened slot space
@@ -61,6 +64,12 @@ struct SaWork {
     // units
     SaUnit* units;          // [SA_MAX_UNITS]
     SaBatchUnit* bunits;    // [SA_MAX_UNITS]
+    // batched calls
+    unsigned long long* unit_hit_base;  // [SA_MAX_UNITS]
+    unsigned long long* unit_hit_end;   // [SA_MAX_UNITS]
+    unsigned long long* bounds;         // [SA_MAX_UNITS * SA_BATCH_ITERS]
+    uint32_t* unit_iters;               // [SA_MAX_UNITS]
+    const uint32_t** keys_arrays;       // [SA_MAX_KEY_ARRAYS]
 };
 
 #define SA_MAX_CTAS 1024
@@ -109,12 +118,22 @@ struct SaExtendArgs {
     uint32_t seed_size;
     int32_t xdrop, hspthresh, noentropy;
 };
-void sa_launch_extend(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
-                      int num_sms, cudaStream_t st);
+// Phase A (lane per hit) and phase B (warp per long hit); B must follow A.
+void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
+                           int num_sms, cudaStream_t st);
+void sa_launch_extend_warp(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
+                           int num_sms, cudaStream_t st);
 
 // ---- sa_sort.cu ----
 // mode 0 = plain dedup; 1 = rm (adds diagonal sort/unique and final sort).
-void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t st);
+// scope_shift: records are counted per (scope >> scope_shift) and flags are
+// looked up the same way (0 for single calls, 4 for batches: scope = unit<<4 | iteration).
+void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t st);
+// ---- sa_pack.cu (batched seeding) ----
+void sa_launch_query_keys(const uint32_t* packed, uint64_t len, const SaParams& p, uint32_t* keys, cudaStream_t st);
+
+// Counts kernel launches of this library (reported by sa_kernel_launches()).
+void sa_note_launch();
 
 // Hand-off of a failed CUDA call to the API layer's error state.
 void sa_set_error(int code, const char* fmt, ...);

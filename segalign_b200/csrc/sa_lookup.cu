@@ -126,8 +126,217 @@ __global__ void sa_k_scope(SaSeedList cs, const uint64_t* __restrict__ limits, S
 void sa_launch_lookup_seeds(SaWork& w, const uint32_t* index, uint32_t nbuckets, const SaParams& p, int G,
                             cudaStream_t st) {
     sa_k_lookup_count<<<G, 256, 0, st>>>(w.seeds, w.desc, index, nbuckets, w.s_lo, w.s_cnt, w.cta_a, w.cta_b, w.ctr);
+    sa_note_launch();
     sa_k_scan_partials<<<1, 1024, 0, st>>>(w.cta_a, w.cta_b, G, &w.ctr->num_hits, &w.ctr->nnz);
+    sa_note_launch();
     sa_k_lookup_emit<<<G, 256, 0, st>>>(w.seeds, w.desc, w.s_lo, w.s_cnt, w.s_P, w.cs, w.cta_a, w.cta_b, w.ctr);
+    sa_note_launch();
     sa_k_groups<<<1, 1, 0, st>>>(w.s_P, w.desc, w.limits, w.ctr);
+    sa_note_launch();
     sa_k_scope<<<148 * 4, 256, 0, st>>>(w.cs, w.limits, w.ctr);
+    sa_note_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Batched lookup over "seed slots".  Unit u covers query positions
+// [q_start, q_end) of one strand; each position owns S = 1 (+K with
+// transitions) consecutive slots in the order the host seeder emits seed
+// words (key, then key ^ (2 << 2t), t = 0..K-1).  Positions whose window is
+// not all uppercase ACGT produce no seed in the reference; here their slots
+// simply have no hits, which leaves every hit and its MAX_HITS iteration
+// unchanged (iterations are defined by the hit prefix only).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t sa_find_unit(const SaBatchUnit* __restrict__ bu, uint32_t n, uint64_t slot) {
+    uint32_t lo = 0, hi = n;  // last unit with slot_begin <= slot
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (bu[mid].slot_begin <= slot) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+struct SaSlotInfo {
+    uint32_t unit, j, lo, cnt;
+};
+
+__device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu, uint32_t u, uint64_t s,
+                                              const uint32_t* const* __restrict__ keys_arrays,
+                                              const uint32_t* __restrict__ index, uint32_t nbuckets, int S) {
+    SaSlotInfo r;
+    const SaBatchUnit B = bu[u];
+    const uint64_t off = s - B.slot_begin;
+    r.unit = B.unit;
+    r.j = B.q_start + (uint32_t)(off / S);
+    const uint32_t v = (uint32_t)(off % S);
+    uint32_t key = __ldg(keys_arrays[B.keys_index] + r.j);
+    r.lo = 0;
+    r.cnt = 0;
+    if (key != SA_INVALID_KEY) {
+        if (v) key ^= 2u << (2 * (v - 1));
+        if (key < nbuckets) {
+            uint32_t hi = __ldg(index + key);
+            r.lo = key ? __ldg(index + key - 1) : 0u;
+            r.cnt = hi - r.lo;
+        }
+    }
+    return r;
+}
+
+__global__ void __launch_bounds__(256)
+sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc,
+                   const uint32_t* const* keys_arrays, const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
+                   uint32_t* __restrict__ s_lo, uint32_t* __restrict__ s_cnt, unsigned long long* cta_a,
+                   unsigned long long* cta_b) {
+    uint64_t a, b;
+    sa_cta_range(desc->num_seeds, a, b);
+    const uint32_t nu = desc->num_units;
+    unsigned long long hits = 0, nz = 0;
+    for (uint64_t s = a + threadIdx.x; s < b; s += 256) {
+        const uint32_t u = sa_find_unit(bu, nu, s);
+        const SaSlotInfo si = sa_slot(bu, u, s, keys_arrays, index, nbuckets, S);
+        s_lo[s] = si.lo;
+        s_cnt[s] = si.cnt;
+        hits += si.cnt;
+        nz += si.cnt != 0;
+    }
+    __shared__ unsigned long long ws[9];
+    unsigned long long tot;
+    sa_block_excl_sum<unsigned long long, 256>(hits, ws, &tot);
+    if (threadIdx.x == 0) cta_a[blockIdx.x] = tot;
+    sa_block_excl_sum<unsigned long long, 256>(nz, ws, &tot);
+    if (threadIdx.x == 0) cta_b[blockIdx.x] = tot;
+}
+
+// Compaction of hit-bearing slots; also records each unit's hit range
+// [unit_hit_base, unit_hit_end) in the global hit prefix.
+__global__ void __launch_bounds__(256)
+sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc, int S,
+                  const uint32_t* __restrict__ s_lo, const uint32_t* __restrict__ s_cnt, SaSeedList cs,
+                  const unsigned long long* cta_a, const unsigned long long* cta_b, unsigned long long* unit_hit_base,
+                  unsigned long long* unit_hit_end, SaCounters* ctr) {
+    const uint64_t n = desc->num_seeds;
+    const uint32_t nu = desc->num_units;
+    uint64_t a, b;
+    sa_cta_range(n, a, b);
+    unsigned long long hbase = cta_a[blockIdx.x], cbase = cta_b[blockIdx.x];
+    __shared__ unsigned long long ws[9];
+    for (uint64_t r = a; r < b; r += 256) {
+        const uint64_t s = r + threadIdx.x;
+        const uint32_t cnt = s < b ? s_cnt[s] : 0u;
+        unsigned long long th, tc;
+        const unsigned long long eh = sa_block_excl_sum<unsigned long long, 256>(cnt, ws, &th);
+        const unsigned long long ec = sa_block_excl_sum<unsigned long long, 256>(cnt != 0, ws, &tc);
+        if (s < b) {
+            const uint32_t u = sa_find_unit(bu, nu, s);
+            const SaBatchUnit B = bu[u];
+            const uint64_t end = (u + 1 < nu) ? bu[u + 1].slot_begin : n;
+            if (s == B.slot_begin) unit_hit_base[u] = hbase + eh;
+            if (s + 1 == end) unit_hit_end[u] = hbase + eh + cnt;
+            if (cnt) {
+                const uint64_t c = cbase + ec;
+                cs.E[c] = hbase + eh;
+                cs.lo[c] = s_lo[s];
+                cs.qpos[c] = B.q_start + (uint32_t)((s - B.slot_begin) / S);
+                cs.unit[c] = B.unit;
+                cs.scope[c] = u;  // batch unit index; turned into (unit, iteration) by sa_k_bscope
+            }
+        }
+        hbase += th;
+        cbase += tc;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) cs.E[ctr->nnz] = ctr->num_hits;
+}
+
+// Per unit: MAX_HITS iteration boundaries in hit space (relative to the unit's
+// first hit).  The reference's limit_pos[i] = lower_bound(P, lim) - 1 selects
+// the last seed whose inclusive prefix is < lim; its prefix is the boundary.
+__global__ void sa_k_bgroups(const SaCallDesc* __restrict__ desc, SaSeedList cs,
+                             const unsigned long long* __restrict__ unit_hit_base,
+                             const unsigned long long* __restrict__ unit_hit_end, unsigned long long* bounds,
+                             uint32_t* unit_iters, SaCounters* ctr) {
+    const uint32_t nu = desc->num_units;
+    const uint64_t MH = desc->max_hits, nnz = ctr->nnz;
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < nu; u += gridDim.x * blockDim.x) {
+        const uint64_t base = unit_hit_base[u], H = unit_hit_end[u] - base;
+        uint64_t it = MH ? H / MH + 1 : 1;
+        if (it > SA_BATCH_ITERS) {
+            atomicCAS(&ctr->error, 0ull, 3ull);
+            it = 1;
+        }
+        unit_iters[u] = (uint32_t)it;
+        unsigned long long* B = bounds + (uint64_t)u * SA_BATCH_ITERS;
+        if (it > 1) {
+            // compacted seeds of the unit: c with base <= E[c] < base + H
+            uint64_t lo = 0, hi = nnz;
+            while (lo < hi) {
+                uint64_t m = (lo + hi) >> 1;
+                if (cs.E[m] < base) lo = m + 1;
+                else hi = m;
+            }
+            const uint64_t c0 = lo;
+            hi = nnz;
+            while (lo < hi) {
+                uint64_t m = (lo + hi) >> 1;
+                if (cs.E[m] < base + H) lo = m + 1;
+                else hi = m;
+            }
+            const uint64_t c1 = lo;
+            uint64_t lim = MH, prev_bound = 0;
+            for (uint64_t i = 0; i + 1 < it; ++i) {
+                // last c in [c0, c1) with inclusive prefix E[c+1] - base < lim
+                uint64_t l = c0, h = c1;
+                while (l < h) {
+                    uint64_t m = (l + h) >> 1;
+                    if (cs.E[m + 1] - base < lim) l = m + 1;
+                    else h = m;
+                }
+                uint64_t bnd = (l > c0) ? cs.E[l] - base : 0;  // prefix of the last qualifying seed
+                if (l == c0 || bnd <= prev_bound) {
+                    if (i > 0 || l == c0) atomicCAS(&ctr->error, 0ull, 2ull);
+                }
+                B[i] = bnd;
+                prev_bound = bnd;
+                lim = bnd + MH;
+            }
+        }
+        B[it - 1] = ~0ull;
+    }
+}
+
+// Compacted seed -> scope = (batch unit << 4) | iteration.
+__global__ void sa_k_bscope(SaSeedList cs, const unsigned long long* __restrict__ unit_hit_base,
+                            const unsigned long long* __restrict__ bounds, const uint32_t* __restrict__ unit_iters,
+                            SaCounters* ctr) {
+    const uint64_t nnz = ctr->nnz;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < nnz; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t u = cs.scope[c];
+        const uint32_t it = unit_iters[u];
+        uint32_t g = 0;
+        if (it > 1) {
+            const uint64_t p = cs.E[c + 1] - unit_hit_base[u];
+            const unsigned long long* B = bounds + (uint64_t)u * SA_BATCH_ITERS;
+            while (g + 1 < it && p > B[g]) ++g;
+        }
+        cs.scope[c] = (u << 4) | g;
+    }
+}
+
+void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, const uint32_t* const* keys_arrays,
+                            uint32_t n_bunits, const SaParams& p, int G, cudaStream_t st) {
+    const int S = p.transition ? 1 + p.kmer_size : 1;
+    sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, keys_arrays, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a,
+                                          w.cta_b);
+    sa_note_launch();
+    sa_k_scan_partials<<<1, 1024, 0, st>>>(w.cta_a, w.cta_b, G, &w.ctr->num_hits, &w.ctr->nnz);
+    sa_note_launch();
+    sa_k_blookup_emit<<<G, 256, 0, st>>>(w.bunits, w.desc, S, w.s_lo, w.s_cnt, w.cs, w.cta_a, w.cta_b,
+                                         w.unit_hit_base, w.unit_hit_end, w.ctr);
+    sa_note_launch();
+    const int ub = (int)std::min<uint32_t>((n_bunits + 255) / 256, 1024u);
+    sa_k_bgroups<<<ub > 0 ? ub : 1, 256, 0, st>>>(w.desc, w.cs, w.unit_hit_base, w.unit_hit_end, w.bounds,
+                                                  w.unit_iters, w.ctr);
+    sa_note_launch();
+    sa_k_bscope<<<148 * 4, 256, 0, st>>>(w.cs, w.unit_hit_base, w.bounds, w.unit_iters, w.ctr);
+    sa_note_launch();
 }

@@ -123,6 +123,7 @@ void sa_launch_pack_text(const char* d_text, uint64_t len, uint32_t* packed, cud
     if (!nwords) return;
     int blocks = (int)std::min<uint64_t>((nwords + 255) / 256, 148ull * 16);
     sa_k_pack_text<<<blocks, 256, 0, st>>>((const uint8_t*)d_text, len, packed, nwords);
+    sa_note_launch();
 }
 
 void sa_launch_rc_packed(const uint32_t* in, uint64_t len, uint32_t* out, cudaStream_t st) {
@@ -130,12 +131,14 @@ void sa_launch_rc_packed(const uint32_t* in, uint64_t len, uint32_t* out, cudaSt
     if (!nwords) return;
     int blocks = (int)std::min<uint64_t>((nwords + 255) / 256, 148ull * 16);
     sa_k_rc_packed<<<blocks, 256, 0, st>>>(in, len, out, nwords);
+    sa_note_launch();
 }
 
 void sa_launch_pad_fill(uint32_t* base, uint64_t n, cudaStream_t st) {
     if (!n) return;
     int blocks = (int)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
     sa_k_fill_u32<<<blocks, 256, 0, st>>>(base, n, 0x77777777u);
+    sa_note_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -209,8 +212,11 @@ void sa_launch_table_keys(const uint32_t* ref, uint32_t start, uint64_t num_step
                           const SaParams& p, uint32_t* keys, uint32_t* vals, unsigned long long* cta_a,
                           unsigned long long* cta_b, unsigned long long* d_total, int G, cudaStream_t st) {
     sa_k_table_count<<<G, 256, 0, st>>>(ref, start, num_steps, step, p, cta_a);
+    sa_note_launch();
     sa_k_scan_partials<<<1, 1024, 0, st>>>(cta_a, cta_b, G, d_total, nullptr);
+    sa_note_launch();
     sa_k_table_emit<<<G, 256, 0, st>>>(ref, start, num_steps, step, p, cta_a, keys, vals);
+    sa_note_launch();
 }
 
 // index[k] = number of valid positions with key <= k (the shifted inclusive
@@ -230,6 +236,7 @@ void sa_launch_table_index(const uint32_t* sorted_keys, const unsigned long long
                            uint64_t nbuckets, cudaStream_t st) {
     cudaMemsetAsync(index, 0, nbuckets * sizeof(uint32_t), st);
     sa_k_table_index<<<148 * 8, 256, 0, st>>>(sorted_keys, d_n, index, nbuckets);
+    sa_note_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -260,6 +267,7 @@ void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint3
     // in_buf lives right after the histogram workspace
     int* in_buf = reinterpret_cast<int*>(cta_hist + 256 * (uint64_t)SA_MAX_CTAS);
     sa_k_plan_noskip<<<1, 1, 0, st>>>(in_buf, passes);
+    sa_note_launch();
     SaKvOps::Ctx c;
     c.k[0] = keys;
     c.k[1] = keys_tmp;
@@ -268,8 +276,29 @@ void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint3
     SaRadixCtl ctl{d_n, in_buf};
     for (int p = 0; p < passes; ++p) {
         sa_k_radix_up<SaKvOps><<<G, SA_RADIX_BLOCK, 0, st>>>(c, p, ctl, cta_hist);
+        sa_note_launch();
         sa_k_radix_scan<<<1, 1024, 0, st>>>(cta_hist, G, in_buf, p);
+        sa_note_launch();
         sa_k_radix_down<SaKvOps><<<G, SA_RADIX_BLOCK, 0, st>>>(c, p, ctl, cta_hist);
+        sa_note_launch();
     }
     *result_in_tmp = passes & 1;
+}
+
+// ---------------------------------------------------------------------------
+// Spaced-seed key of every query position (device-side seeding, the work of
+// src/seeder.cpp:57-74 without the host loop): keys[j] = key of the window at
+// j, SA_INVALID_KEY unless all seed_size bases are uppercase ACGT.
+// ---------------------------------------------------------------------------
+__global__ void sa_k_query_keys(const uint32_t* __restrict__ packed, uint64_t len, SaParams P,
+                                uint32_t* __restrict__ keys) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < len; j += (uint64_t)gridDim.x * blockDim.x)
+        keys[j] = sa_key_at(packed, (int64_t)j, P);
+}
+
+void sa_launch_query_keys(const uint32_t* packed, uint64_t len, const SaParams& p, uint32_t* keys, cudaStream_t st) {
+    if (!len) return;
+    int blocks = (int)std::min<uint64_t>((len + 255) / 256, 148ull * 16);
+    sa_k_query_keys<<<blocks, 256, 0, st>>>(packed, len, p, keys);
+    sa_note_launch();
 }

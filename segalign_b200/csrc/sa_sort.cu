@@ -115,12 +115,17 @@ static void sa_radix_sort_recs(SaWork& w, const SaSortSpec& spec, const unsigned
     c.spec = spec;
     cudaMemsetAsync(w.sort_hist, 0, sizeof(unsigned int) * 256 * SA_SORT_MAX_DIGITS, s);
     sa_k_sort_hist_all<<<G, 256, 0, s>>>(c, d_n, st, w.sort_hist);
+    sa_note_launch();
     sa_k_sort_plan<<<1, 256, 0, s>>>(w.sort_hist, spec.npass, d_n, st);
+    sa_note_launch();
     SaRadixCtl ctl{d_n, st + 1};
     for (int p = 0; p < spec.npass; ++p) {
         sa_k_radix_up<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
+        sa_note_launch();
         sa_k_radix_scan<<<1, 1024, 0, s>>>(w.sort_cta_hist, G, st + 1, p);
+        sa_note_launch();
         sa_k_radix_down<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
+        sa_note_launch();
     }
 }
 
@@ -135,6 +140,7 @@ struct SaUniqArgs {
     uint32_t* out_scope;
     uint32_t* scope_count;      // null: no per-scope counts
     int mode;                   // 0 = hspEqual, 1 = hspDiagEqual + diagonal exclusion, 2 = keep all (copy)
+    int scope_shift;            // counts and flags are indexed by scope >> scope_shift
 };
 
 __device__ __forceinline__ bool sa_rec_equal(const SaRec& x, const SaRec& y) {
@@ -160,7 +166,7 @@ __device__ __forceinline__ bool sa_uniq_keep(const SaUniqArgs& u, int buf, uint6
     }
     // Main-diagonal exclusion for the repeat-masker self alignment: scope
     // flags bit1 = exclusion requested, bit0 = minus strand (never excluded).
-    if (u.mode == 1 && (u.scope_flags[sc] & 3u) == 2u && r.ref_start == r.query_start) keep = false;
+    if (u.mode == 1 && (u.scope_flags[sc >> u.scope_shift] & 3u) == 2u && r.ref_start == r.query_start) keep = false;
     return keep;
 }
 
@@ -195,7 +201,7 @@ sa_k_uniq_emit(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, 
             const uint32_t sc = u.scope[buf][i];
             dr[base + e] = u.rec[buf][i];
             ds[base + e] = sc;
-            if (u.scope_count) atomicAdd(&u.scope_count[sc], 1u);
+            if (u.scope_count) atomicAdd(&u.scope_count[sc >> u.scope_shift], 1u);
         }
         base += tot;
     }
@@ -216,8 +222,11 @@ __global__ void sa_k_copy_u64(unsigned long long* dst, const unsigned long long*
 static void sa_uniq(SaWork& w, SaUniqArgs u, const unsigned long long* d_n, const int* src_buf,
                     unsigned long long* d_out_n, int G, cudaStream_t s) {
     sa_k_uniq_count<<<G, 256, 0, s>>>(u, d_n, src_buf, w.cta_a);
+    sa_note_launch();
     sa_k_scan_partials<<<1, 1024, 0, s>>>(w.cta_a, w.cta_b, G, d_out_n, nullptr);
+    sa_note_launch();
     sa_k_uniq_emit<<<G, 256, 0, s>>>(u, d_n, src_buf, w.cta_a);
+    sa_note_launch();
 }
 
 static SaSortSpec spec_of(std::initializer_list<std::pair<uint8_t, uint8_t>> fields_lsd_first) {
@@ -235,13 +244,14 @@ static SaSortSpec spec_of(std::initializer_list<std::pair<uint8_t, uint8_t>> fie
     return sp;
 }
 
-void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t s) {
+void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s) {
     // Device-side counts live in the spare counter slots.
     unsigned long long* n0 = &w.ctr->pad[0];
     unsigned long long* n1 = &w.ctr->pad[1];
     unsigned long long* n2 = &w.ctr->pad[2];
     int* st = w.sort_in_buf;
     sa_k_dedup_prep<<<1, 1, 0, s>>>(w.ctr, w.surv_cap, n0, st);
+    sa_note_launch();
     cudaMemsetAsync(w.scope_count, 0, sizeof(uint32_t) * SA_MAX_SCOPES, s);
 
     // hspComp order: (scope, query_start asc, len desc, ref_start asc).
@@ -253,6 +263,7 @@ void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t s) {
     u.scope[0] = w.scope[0];
     u.scope[1] = w.scope[1];
     u.scope_flags = w.scope_flags;
+    u.scope_shift = scope_shift;
     if (mode == 0) {
         u.mode = 0;
         u.out_rec = w.out;
@@ -265,12 +276,14 @@ void sa_launch_dedup(SaWork& w, int mode, int G, cudaStream_t s) {
     u.mode = 0;
     sa_uniq(w, u, n0, st + 1 + plain.npass, n1, G, s);
     sa_k_flip_cur<<<1, 1, 0, s>>>(st, plain.npass);
+    sa_note_launch();
     // hspDiagComp: (scope, diag asc, ref_start asc, score desc), stable
     const SaSortSpec diag = spec_of({{F_SCORE, 1}, {F_RS, 0}, {F_DIAG, 0}, {F_SCOPE, 0}});
     sa_radix_sort_recs(w, diag, n1, st, G, s);
     u.mode = 1;
     sa_uniq(w, u, n1, st + 1 + diag.npass, n2, G, s);
     sa_k_flip_cur<<<1, 1, 0, s>>>(st, diag.npass);
+    sa_note_launch();
     // hspFinalComp: (scope, query_start asc, score desc, ref_start desc), stable
     const SaSortSpec fin = spec_of({{F_RS, 1}, {F_SCORE, 1}, {F_QS, 0}, {F_SCOPE, 0}});
     sa_radix_sort_recs(w, fin, n2, st, G, s);

@@ -4,6 +4,12 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# Small device workspaces for the test workloads (read at sa_initialize_processor).
+os.environ.setdefault("SA_SURV_CAP", str(1 << 22))
+os.environ.setdefault("SA_LONG_CAP", str(1 << 20))
+os.environ.setdefault("SA_BATCH_SLOT_CAP", str(1 << 24))
+os.environ.setdefault("SA_BATCH_SURV_CAP", str(1 << 22))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

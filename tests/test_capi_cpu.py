@@ -1,0 +1,92 @@
+"""C ABI surface and host-side logic, without a GPU.
+
+- the CUDA library loads and exports every entry point declared in include/*.h;
+- host C++ (scoring table, seeder words, reverse complement) matches the oracle;
+- calls that need a device fail with a status code, never a CPU fallback.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+import segalign_b200 as sa
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("segalign_b200.h", "segalign_b200_host.h"):
+        txt = open(os.path.join(ROOT, "include", h)).read()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names |= set(re.findall(r"\b(sa_[a-z0-9_]+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol(built):
+    lib = sa.load_library()
+    names = declared_symbols()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(sa.EXPORTS) == names
+
+
+@pytest.mark.parametrize("amb", ["", "n", "iupac", "n,3,40", "x,3,40"])
+@pytest.mark.parametrize("xdrop", [910, 500])
+def test_sub_mat_matches_oracle(built, amb, xdrop):
+    assert np.array_equal(sa.build_sub_mat(xdrop, amb), oracle.sub_mat(xdrop, amb))
+
+
+def test_sub_mat_bad_ambiguous(built):
+    with pytest.raises(sa.SegAlignError):
+        sa.build_sub_mat(910, "n,x,3")
+
+
+@pytest.mark.parametrize("shape", ["12of19", "14of22", "110100111"])
+@pytest.mark.parametrize("transition", [False, True])
+def test_host_seeder_matches_oracle(built, shape, transition):
+    rng = np.random.default_rng(11)
+    t = rng.choice(np.frombuffer(b"ACGTACGTACGTacgtN&", dtype=np.uint8), size=30000).tobytes()
+    p = oracle.params(shape=shape, transition=transition)
+    got = sa.host_seeds(t, 100, 29000 - p.seed_size, shape=shape, transition=transition)
+    want = oracle.chunk_seeds(t, 100, 29000 - p.seed_size, p)
+    assert np.array_equal(got, want)
+
+
+def test_host_revcomp_matches_oracle(built):
+    rng = np.random.default_rng(3)
+    t = rng.choice(np.frombuffer(b"ACGTacgtNn&RY", dtype=np.uint8), size=10000).tobytes()
+    assert sa.host_revcomp(t) == oracle.revcomp_text(t)
+
+
+def test_calls_without_device_fail_with_status(built):
+    lib = sa.load_library()
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("a GPU is present")
+    assert lib.sa_initialize_interface(-1) == -9  # SA_ERR_NO_DEVICE
+    # nothing is resident: every compute entry point refuses with a status
+    ptr, n = C.POINTER(C.c_uint8)(), C.c_uint64()
+    seeds = np.zeros(4, dtype=np.uint64)
+    r = lib.sa_seed_and_filter(seeds.ctypes.data_as(C.POINTER(C.c_uint64)), 4, 0, 0, C.byref(ptr), C.byref(n))
+    assert r == -2  # SA_ERR_STATE
+    with pytest.raises(sa.SegAlignError):
+        sa.SeedFilter().initialize_interface(-1)
+
+
+def test_seeder_run_validates_arguments(built):
+    lib = sa.load_library()
+    cfg = sa.SeederCfg(10_000_000, 0, 0, 3, 1, 0, 0, 0)  # chunk_size 0
+    fw, fl, rc, rl = C.POINTER(C.c_uint8)(), C.c_uint64(), C.POINTER(C.c_uint8)(), C.c_uint64()
+    r = lib.sa_seeder_run(C.byref(cfg), b"ACGT" * 10, 40, C.byref(fw), C.byref(fl), C.byref(rc), C.byref(rl), None)
+    assert r == -1
+
+
+def test_tuning_validation(built):
+    lib = sa.load_library()
+    assert lib.sa_set_tuning(12, -1, -1, -1) == -1    # not a multiple of 8
+    assert lib.sa_set_tuning(-1, 100, -1, -1) == -1   # not a multiple of 32
+    assert lib.sa_set_tuning(64, 256, 4, 1024) == 0
