@@ -134,6 +134,23 @@ int sa_rm_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, ui
 /* ClearQuery(), repeat_masker_src/seed_filter.cu:937-946. */
 int sa_rm_clear_query(void);
 
+/* No counterpart in the reference.  SeedAndFilter for callers that cannot
+ * let the library allocate device memory while they run (a host program
+ * that owns all device memory through its own fixed-budget pool, or a
+ * latency-bound loop that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  Same output as sa_seed_and_filter(), written to the
+ * caller's buffer out[0 .. out_cap); *out_len gets the record count (also
+ * when the buffer is too small, which returns SA_ERR_CAPACITY).  Per-call
+ * scratch lives in one fixed ~30 MB device array that every GPU using the
+ * library holds until exit; at most 262,144 seed words and 262,144 HSP
+ * candidates before deduplication per call, else SA_ERR_CAPACITY.  The first
+ * call on a device looks up that array's address: make it before any stream
+ * capture.  Calls share the array and run one at a time; calls that
+ * overlapped on the GPU would race.  Needs the resident target, table and
+ * query of the normal set-up calls. */
+int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t buffer, sa_segment* out,
+                               uint64_t out_cap, uint64_t* out_len);
+
 /* ---- batched form (no single reference counterpart) ---- */
 
 /* One unit = one SeedAndFilter call of the reference on the seed words the

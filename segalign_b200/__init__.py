@@ -46,7 +46,7 @@ EXPORTS = [
     "sa_rm_send_query_write_request", "sa_rm_seed_and_filter", "sa_rm_clear_query", "sa_free_segments",
     "sa_set_max_hits", "sa_set_rm_exclude_diagonal", "sa_last_call_stats", "sa_last_error", "sa_set_tuning",
     "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
-    "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches",
+    "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
 ]
 
 
@@ -127,6 +127,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                         _P(SeederStats)]),
             "sa_seed_and_filter_batch": (C.c_int, [_P(Unit), C.c_uint32, segpp, u64p, u64p]),
             "sa_set_timing": (C.c_int, [C.c_int]),
+            "sa_seed_and_filter_noalloc": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, _P(C.c_uint8),
+                                                     C.c_uint64, u64p]),
             "sa_kernel_launches": (C.c_uint64, []),
         }
         for name, (res, args) in sig.items():
@@ -264,6 +266,18 @@ class SeedFilter:
         self._chk(self.lib.sa_seed_and_filter(_u64p(s), len(s), int(rev), buffer, C.byref(ptr), C.byref(n)),
                   "SeedAndFilter")
         return _take_segments(self.lib, ptr, n.value)
+
+    def seed_and_filter_noalloc(self, seeds: np.ndarray, rev: bool, buffer: int = 0,
+                                out: np.ndarray | None = None) -> np.ndarray:
+        """SeedAndFilter without allocation: the result goes into `out` (SEGMENT_DTYPE records)."""
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        if out is None:
+            out = np.zeros(1 << 16, dtype=SEGMENT_DTYPE)
+        n = C.c_uint64()
+        self._chk(self.lib.sa_seed_and_filter_noalloc(_u64p(s), len(s), int(rev), buffer,
+                                                      out.ctypes.data_as(_P(C.c_uint8)), len(out), C.byref(n)),
+                  "SeedAndFilterNoAlloc")
+        return out[: n.value].copy()
 
     def clear_query(self, buffer: int = 0) -> None:
         self._chk(self.lib.sa_clear_query(buffer), "ClearQuery")

@@ -1157,6 +1157,33 @@ int sa_set_timing(int on) {
 
 uint64_t sa_kernel_launches(void) { return g_launches.load(); }
 
+}  // extern "C"
+
+int sa_resident_view(uint32_t buffer, SaResidentView* v) {
+    int r = check_ready(true);
+    if (r != SA_OK) return r;
+    Global& g = G();
+    if (buffer >= (uint32_t)kMaxBuffers) return SA_ERR_ARG;
+    const DevState& d = g.devs[0];
+    v->dev = d.dev;
+    v->num_sms = d.num_sms;
+    v->ref = d.ref.data;
+    v->ref_len = (uint32_t)d.ref.len;
+    v->index = d.index;
+    v->nbuckets = d.nbuckets;
+    v->pos = d.pos;
+    v->q_packed[0] = d.qf[buffer].data;
+    v->q_packed[1] = d.qr[buffer].data;
+    v->q_len = (uint32_t)d.qf[buffer].len;
+    v->max_seeds = g.max_seeds;
+    v->max_hits = max_hits_now();
+    v->params = g.params;
+    v->tuning = g.tuning;
+    return SA_OK;
+}
+
+extern "C" {
+
 int sa_set_max_hits(uint64_t max_hits) {
     G().max_hits_override = max_hits;
     return SA_OK;

@@ -132,6 +132,26 @@ void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s
 // ---- sa_pack.cu (batched seeding) ----
 void sa_launch_query_keys(const uint32_t* packed, uint64_t len, const SaParams& p, uint32_t* keys, cudaStream_t st);
 
+// Read-only view of the resident state of GPU 0 (sa_api.cu), for entry points
+// that live in other files.  Returns SA_OK (0) when target, table and the
+// processor are ready.
+struct SaResidentView {
+    int dev;
+    int num_sms;
+    const uint32_t* ref;
+    uint32_t ref_len;
+    const uint32_t* index;
+    uint64_t nbuckets;
+    const uint32_t* pos;
+    const uint32_t* q_packed[2];  // forward, reverse complement of the requested buffer
+    uint32_t q_len;
+    uint64_t max_seeds;
+    uint64_t max_hits;
+    SaParams params;
+    SaTuning tuning;
+};
+int sa_resident_view(uint32_t buffer, SaResidentView* v);
+
 // Counts kernel launches of this library (reported by sa_kernel_launches()).
 void sa_note_launch();
 
