@@ -53,6 +53,7 @@ def parse_args():
     ap.add_argument("--cpu-chunks", type=int, default=64, help="units in the bounded CPU sample")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return ap.parse_args()
 
 
@@ -260,6 +261,7 @@ def run_ours(args):
     barrier()
     l0 = sf.kernel_launches()
     dev_ms, hits, hsps, lane_ms, warp_ms, surv, tiles, nnz, longs = [], 0, 0, [], [], 0, 0, 0, 0
+    lk_ms, dd_ms = [], []
     with ClockSampler(gpu_index(local)) as clk:
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -270,6 +272,8 @@ def run_ours(args):
             dev_ms.append(st["ms_total"])
             lane_ms.append(st["ms_extend_lane"])
             warp_ms.append(st["ms_extend_warp"])
+            lk_ms.append(st["ms_lookup"])
+            dd_ms.append(st["ms_dedup"])
             hits, hsps, surv, tiles, nnz, longs = (st["num_hits"], st["num_hsps"], st["survivors"], st["tiles"],
                                                    st["seeds_with_hits"], st["long_hits"])
         barrier()
@@ -305,7 +309,8 @@ def run_ours(args):
                    "scale": args.scale},
         "hsps_per_s": hsps_all / (ms_step_max / 1000.0),
         "extensions_per_step": hits_all, "hsps_per_step": hsps_all,
-        "phase_ms": {"extend_lane": lane_ms_avg, "extend_warp": sum(warp_ms) / len(warp_ms),
+        "phase_ms": {"lookup": sum(lk_ms) / len(lk_ms), "extend_lane": lane_ms_avg,
+                     "extend_warp": sum(warp_ms) / len(warp_ms), "dedup": sum(dd_ms) / len(dd_ms),
                      "wall_per_step": 1000 * wall_s / args.steps},
         "table_build_ms": table_ms,
         "roofline": roofline,
@@ -357,7 +362,7 @@ def run_ours(args):
         out["batched_vs_plain"] = out["value"] / out["e2e"]["value"]
 
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only) ----
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         r = cpu_sample(w, args.cpu_chunks, threads)
         cpu_v = r["hits"] / r["seconds"]
