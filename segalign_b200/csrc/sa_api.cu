@@ -143,7 +143,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{64, 256, 4, 256, 296, 1024};
+    SaTuning tuning{4096, 256, 4, 256, 296, 1024};
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -277,7 +277,6 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
         {(void**)&w.unit_hit_end, batch ? 8 * nunits : 0},
         {(void**)&w.bounds, batch ? 8 * nunits * SA_BATCH_ITERS : 0},
         {(void**)&w.unit_iters, batch ? 4 * nunits : 0},
-        {(void**)&w.keys_arrays, batch ? 8 * SA_MAX_KEY_ARRAYS : 0},
     };
     w.flags = nullptr;
     uint64_t total = 0;
@@ -493,9 +492,9 @@ struct BatchResult {
     sa_call_stats timing{};
 };
 
-// Runs units [u0, u1) of `units` in one device pass.  Returns SA_ERR_CAPACITY
-// when the survivors do not fit (the caller splits the range).
-int run_batch_group(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uint32_t u1, bool want_out,
+// Runs units [u0, u1) in one device pass.  Returns SA_ERR_CAPACITY when the
+// survivors do not fit (the caller splits the range).
+int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t u0, uint32_t u1, bool want_out,
                     BatchResult& res) {
     Global& g = G();
     SaWork& w = s->w;
@@ -504,21 +503,18 @@ int run_batch_group(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uin
     const int S = g.params.transition ? 1 + g.params.kmer_size : 1;
     const uint32_t n = u1 - u0;
     std::vector<SaBatchUnit> bu(n);
-    std::vector<const uint32_t*> karr(SA_MAX_KEY_ARRAYS, nullptr);
     SaUnit* hu = s->h_units;
     uint64_t slots = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        const sa_unit& u = units[u0 + i];
-        const int rev = u.rev ? 1 : 0;
-        const Packed& q = rev ? d.qr[u.buffer] : d.qf[u.buffer];
+        const SaResolvedUnit& u = units[u0 + i];
         bu[i].slot_begin = slots;
         bu[i].q_start = u.start;
         bu[i].q_end = u.end;
-        bu[i].keys_index = u.buffer * 2 + rev;
+        bu[i].keys = u.keys;
         bu[i].unit = i;
-        karr[u.buffer * 2 + rev] = d.qkeys[u.buffer][rev];
-        hu[i].q_packed = q.data;
-        hu[i].q_len = (uint32_t)q.len;
+        bu[i].pad = 0;
+        hu[i].q_packed = u.q_packed;
+        hu[i].q_len = u.q_len;
         hu[i].rm_lo = hu[i].rm_hi = 0;
         hu[i].flags = 0;
         slots += (uint64_t)(u.end - u.start) * S;
@@ -534,11 +530,10 @@ int run_batch_group(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uin
     tm.mark(0);
     SA_CUDA_OK(cudaMemcpyAsync(w.bunits, bu.data(), sizeof(SaBatchUnit) * n, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.units, hu, sizeof(SaUnit) * n, cudaMemcpyHostToDevice, st));
-    SA_CUDA_OK(cudaMemcpyAsync((void*)w.keys_arrays, karr.data(), 8 * SA_MAX_KEY_ARRAYS, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.desc, hd, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemsetAsync(w.scope_flags, 0, 4 * n, st));
     SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
-    sa_launch_lookup_batch(w, d.index, (uint32_t)d.nbuckets, w.keys_arrays, n, g.params, Gr, st);
+    sa_launch_lookup_batch(w, d.index, (uint32_t)d.nbuckets, n, g.params, Gr, st);
     tm.mark(1);
     SaExtendArgs xa;
     xa.ref = d.ref.data;
@@ -594,7 +589,7 @@ int run_batch_group(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uin
     return SA_OK;
 }
 
-int run_batch_range(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uint32_t u1, bool want_out,
+int run_batch_range(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t u0, uint32_t u1, bool want_out,
                     BatchResult& res) {
     Global& g = G();
     const uint64_t S = g.params.transition ? 1 + g.params.kmer_size : 1;
@@ -629,6 +624,28 @@ int run_batch_range(DevState& d, Slot* s, const sa_unit* units, uint32_t u0, uin
         a = b;
     }
     return SA_OK;
+}
+
+// Units with an empty window are not run; the rest go through the batch slot.
+int run_resolved(const SaResolvedUnit* units, uint32_t n, bool want_out, BatchResult& res,
+                 std::vector<int64_t>& map) {
+    Global& g = G();
+    DevState& d = g.devs[0];
+    if (!d.batch) {
+        Slot* s = nullptr;
+        SA_TRY(make_slot(0, g.batch_slot_cap, g.batch_surv_cap, g.long_cap, &s, true));
+        d.batch = s;
+    }
+    std::vector<SaResolvedUnit> live;
+    map.assign(n, -1);
+    for (uint32_t i = 0; i < n; ++i)
+        if (units[i].end > units[i].start) {
+            map[i] = (int64_t)live.size();
+            live.push_back(units[i]);
+        }
+    res.recs.resize(live.size());
+    res.hits.assign(live.size(), 0);
+    return run_batch_range(d, d.batch, live.data(), 0, (uint32_t)live.size(), want_out, res);
 }
 
 }  // namespace
@@ -1088,24 +1105,17 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
         }
     }
     std::lock_guard<std::mutex> lk(g.batch_mu);
-    if (!d.batch) {
-        Slot* s = nullptr;
-        SA_TRY(make_slot(0, g.batch_slot_cap, g.batch_surv_cap, g.long_cap, &s, true));
-        d.batch = s;
+    std::vector<SaResolvedUnit> ru(n_units);
+    for (uint32_t i = 0; i < n_units; ++i) {
+        const int rev = units[i].rev ? 1 : 0;
+        SA_TRY(ensure_keys(d, units[i].buffer, rev));
+        const Packed& q = rev ? d.qr[units[i].buffer] : d.qf[units[i].buffer];
+        ru[i] = SaResolvedUnit{d.qkeys[units[i].buffer][rev], q.data, (uint32_t)q.len, units[i].start, units[i].end,
+                               rev};
     }
-    for (uint32_t i = 0; i < n_units; ++i) SA_TRY(ensure_keys(d, units[i].buffer, units[i].rev ? 1 : 0));
-    // units with an empty window produce a header only
-    std::vector<sa_unit> live;
-    std::vector<uint32_t> live_idx;
-    for (uint32_t i = 0; i < n_units; ++i)
-        if (units[i].end > units[i].start) {
-            live.push_back(units[i]);
-            live_idx.push_back(i);
-        }
     BatchResult res;
-    res.recs.resize(live.size());
-    res.hits.assign(live.size(), 0);
-    SA_TRY(run_batch_range(d, d.batch, live.data(), 0, (uint32_t)live.size(), out != nullptr, res));
+    std::vector<int64_t> map;
+    SA_TRY(run_resolved(ru.data(), n_units, out != nullptr, res, map));
     std::memset(&t_stats, 0, sizeof t_stats);
     t_stats.num_hits = res.tot.num_hits;
     t_stats.hits_extended = res.tot.extended;
@@ -1126,8 +1136,6 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
     for (auto& r : res.recs) total += r.size();
     sa_segment* o = (sa_segment*)malloc(sizeof(sa_segment) * (total ? total : 1));
     if (!o) return SA_ERR_NOMEM;
-    std::vector<int64_t> map(n_units, -1);
-    for (size_t k = 0; k < live_idx.size(); ++k) map[live_idx[k]] = (int64_t)k;
     uint64_t at = 0;
     for (uint32_t i = 0; i < n_units; ++i) {
         offsets[i] = at;
@@ -1158,6 +1166,32 @@ int sa_set_timing(int on) {
 uint64_t sa_kernel_launches(void) { return g_launches.load(); }
 
 }  // extern "C"
+
+int sa_run_units(const SaResolvedUnit* units, uint32_t n, bool want_out, SaRunResult* out) {
+    int r = check_ready(true);
+    if (r != SA_OK) return r;
+    Global& g = G();
+    std::lock_guard<std::mutex> lk(g.batch_mu);
+    BatchResult res;
+    std::vector<int64_t> map;
+    r = run_resolved(units, n, want_out, res, map);
+    if (r != SA_OK) return r;
+    out->recs->assign(n, {});
+    out->hits->assign(n, 0);
+    for (uint32_t i = 0; i < n; ++i)
+        if (map[i] >= 0) {
+            (*out->hits)[i] = res.hits[map[i]];
+            if (want_out) (*out->recs)[i] = std::move(res.recs[map[i]]);
+        }
+    out->tot = res.tot;
+    out->ms_total = res.timing.ms_total;
+    out->ms_lookup = res.timing.ms_lookup;
+    out->ms_extend_lane = res.timing.ms_extend_lane;
+    out->ms_extend_warp = res.timing.ms_extend_warp;
+    out->ms_dedup = res.timing.ms_dedup;
+    out->ms_copy = res.timing.ms_copy;
+    return SA_OK;
+}
 
 int sa_resident_view(uint32_t buffer, SaResidentView* v) {
     int r = check_ready(true);
@@ -1201,11 +1235,11 @@ int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hit
         t.lane_cap = lane_cap;
     }
     if (ext_block >= 0) {
-        if (ext_block % 32 || ext_block > 1024 || ext_block < 64) return SA_ERR_ARG;
+        if (ext_block != 256) return SA_ERR_ARG;  // the lane kernel is compiled for 256 threads
         t.ext_block = ext_block;
     }
     if (ext_ctas_per_sm >= 0) {
-        if (ext_ctas_per_sm < 1 || ext_ctas_per_sm > 16) return SA_ERR_ARG;
+        if (ext_ctas_per_sm < 2 || ext_ctas_per_sm > 4) return SA_ERR_ARG;
         t.ext_ctas_per_sm = ext_ctas_per_sm;
     }
     if (tile_hits >= 0) {

@@ -103,12 +103,33 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 }
 
 // ---------------------------------------------------------------------------
-// Phase A: one hit per lane with in-order warp refill.
+// Phase A: one hit per lane, with the next hit of each lane prefetched.
+//
+// A warp takes tiles of consecutive hits from a global counter.  Each lane
+// owns a current hit and a prefetched next hit: a refill round hands the next
+// hits of the tile, in order, to the lanes whose next slot is empty, and a
+// lane promotes its next hit the moment its current one finishes.  The
+// dependent loads that locate a hit (seed window of E, bucket start, query
+// position, target position, unit) are therefore issued one hit ahead of
+// their use.  A step scores 8 bases: the target and query words are carried
+// between steps (one new load per sequence), the two nibble streams are
+// merged into byte indices of a 256-entry score table, and the per-base
+// bounds test is only done in the step that reaches a sequence end.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 4)
+__device__ __forceinline__ void sa_merge8(uint32_t rw, uint32_t qw, uint32_t& lo, uint32_t& hi) {
+    // byte b of lo = (q << 4) | r of base 2b, byte b of hi = that of base 2b+1
+    lo = (rw & 0x0f0f0f0fu) | ((qw & 0x0f0f0f0fu) << 4);
+    hi = ((rw >> 4) & 0x0f0f0f0fu) | (qw & 0xf0f0f0f0u);
+}
+
+template <int MIN_CTAS>
+__global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
-    __shared__ int sub[64];
-    if (threadIdx.x < 64) sub[threadIdx.x] = P.sub_mat[threadIdx.x];
+    __shared__ int sub256[256];  // index (q << 4) | r
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        const int r = i & 15, q = i >> 4;
+        sub256[i] = (r < 8 && q < 8) ? P.sub_mat[r * 8 + q] : 0;
+    }
     __syncthreads();
     if (a.ctr->error) return;
     const int lane = threadIdx.x & 31;
@@ -116,89 +137,115 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
     const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
     const int xdrop = a.xdrop;
+    const uint32_t* __restrict__ ref = a.ref;
 
     uint64_t tile_next = 0, tile_end = 0, cur = 0;
     bool exhausted = (H == 0);
 
+    // prefetched next hit
+    bool nx = false;
+    uint32_t n_rl = 0, n_ql = 0, n_scope = 0, n_unit = 0;
+    // current hit
     bool has = false, nocap = false;
     uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0, uflags = 0, qlen = 0;
-    const uint32_t* qp = a.ref;
+    const uint32_t* __restrict__ qp = ref;
     int dir = 0;
-    uint32_t o = 0, avail = 0;
+    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0, carry_r = 0, carry_q = 0;
+    int64_t wr = 0, wq = 0;  // word index of the next load (right: upper word, left: lower word)
     int S = 0, best = 0, bpos = -1, Rbest = 0, Rpos = -1;
     uint32_t tiles = 0;
     unsigned long long tiles_acc = 0, ext_acc = 0;
 
     while (true) {
-        // ---- refill lanes without a hit, in hit order ----
-        uint32_t need = __ballot_sync(SA_FULL, !has);
-        while (need && !exhausted) {
+        // ---- refill: next slots of the tile's hits, in order ----
+        const uint32_t need = __ballot_sync(SA_FULL, !nx);
+        if (need && !exhausted) {
             if (tile_next >= tile_end) {
                 unsigned long long t0 = 0;
                 if (lane == 0) t0 = atomicAdd(&a.ctr->hit_cursor, (unsigned long long)a.tile_hits);
                 t0 = __shfl_sync(SA_FULL, t0, 0);
                 if (t0 >= H) {
                     exhausted = true;
-                    break;
+                } else {
+                    tile_next = t0;
+                    tile_end = (t0 + a.tile_hits < H) ? t0 + a.tile_hits : H;
+                    cur = sa_warp_find_seed(a.cs.E, nnz, t0);
                 }
-                tile_next = t0;
-                tile_end = (t0 + a.tile_hits < H) ? t0 + a.tile_hits : H;
-                cur = sa_warp_find_seed(a.cs.E, nnz, t0);
             }
-            const uint64_t left_in_tile = tile_end - tile_next;
-            const uint32_t m = min((uint32_t)__popc(need), (uint32_t)(left_in_tile < 32 ? left_in_tile : 32));
-            const uint32_t rank = __popc(need & lt);
-            const bool take = !has && rank < m;
-            const uint64_t h = tile_next + rank;
-            // The m hits span at most m consecutive compacted seeds from `cur`.
-            const uint64_t Ew = (cur + lane < nnz) ? a.cs.E[cur + lane] : ~0ull;
-            int k = 0;
+            if (!exhausted) {
+                const uint64_t left_in_tile = tile_end - tile_next;
+                const uint32_t m = min((uint32_t)__popc(need), (uint32_t)(left_in_tile < 32 ? left_in_tile : 32));
+                const uint32_t rank = __popc(need & lt);
+                const bool take = !nx && rank < m;
+                const uint64_t h = tile_next + rank;
+                // the m hits span at most m consecutive compacted seeds from `cur`
+                const uint64_t Ew = (cur + lane < nnz) ? a.cs.E[cur + lane] : ~0ull;
+                int k = 0;
 #pragma unroll
-            for (int s = 16; s >= 1; s >>= 1) {
-                uint64_t v = __shfl_sync(SA_FULL, Ew, k + s);
-                if (v <= h) k += s;
-            }
-            const uint64_t Ek = __shfl_sync(SA_FULL, Ew, k);
-            const uint32_t lm = __ballot_sync(SA_FULL, Ew <= tile_next + m - 1);
-            const uint64_t newcur = cur + (31 - __clz(lm));
-            if (take) {
-                const uint64_t c = cur + k;
-                const uint32_t t = a.cs.lo[c] + (uint32_t)(h - Ek);
-                rl = __ldg(a.pos_table + t) + seed_size;   // find_hits :192
-                ql = a.cs.qpos[c] + seed_size;            // find_hits :176
-                scope = a.cs.scope[c];
-                unit_id = a.cs.unit[c];
-                const SaUnit U = a.units[unit_id];
-                qp = U.q_packed;
-                qlen = U.q_len;
-                uflags = U.flags;
-                // rm: hits outside [ref_start, ref_end] are never extended
-                // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
-                bool skip = (uflags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
-                // Coordinates past either sequence end (a caller-supplied
-                // table or seed beyond the sequences) are rejected, not read.
-                if (rl > ref_len || ql > qlen) {
-                    atomicCAS(&a.ctr->error, 0ull, 5ull);
-                    skip = true;
+                for (int s = 16; s >= 1; s >>= 1) {
+                    const uint64_t v = __shfl_sync(SA_FULL, Ew, k + s);
+                    if (v <= h) k += s;
                 }
-                if (!skip) {
-                    has = true;
-                    nocap = false;
-                    dir = 0;
-                    o = 0;
-                    S = 0;
-                    best = 0;
-                    bpos = -1;
-                    tiles = 0;
-                    avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
-                    ++ext_acc;
+                const uint64_t Ek = __shfl_sync(SA_FULL, Ew, k);
+                // Next round starts at hit tile_next + m: its seed is the last
+                // window entry with E <= that hit, or cur + 32 when the window's
+                // last seed ends right before it.  Keeping `cur` at the seed of
+                // the round's first hit is what bounds a round to the window.
+                const uint64_t nxt = tile_next + m;
+                const uint32_t lm = __ballot_sync(SA_FULL, Ew <= nxt);
+                const uint64_t E32 = (cur + 32 < nnz) ? a.cs.E[cur + 32] : ~0ull;
+                if (take) {
+                    const uint64_t c = cur + k;
+                    n_rl = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - Ek)) + seed_size;  // find_hits :192
+                    n_ql = a.cs.qpos[c] + seed_size;                                         // find_hits :176
+                    n_scope = a.cs.scope[c];
+                    n_unit = a.cs.unit[c];
+                    nx = true;
                 }
+                cur = (lm == SA_FULL && E32 <= nxt) ? cur + 32 : cur + (31 - __clz(lm));
+                tile_next += m;
             }
-            tile_next += m;
-            cur = newcur;
-            need = __ballot_sync(SA_FULL, !has);
         }
-        if (!__any_sync(SA_FULL, has)) break;
+        // ---- promote the next hit of idle lanes ----
+        if (!has && nx) {
+            nx = false;
+            rl = n_rl;
+            ql = n_ql;
+            scope = n_scope;
+            unit_id = n_unit;
+            const SaUnit U = a.units[unit_id];
+            qp = U.q_packed;
+            qlen = U.q_len;
+            uflags = U.flags;
+            // rm: hits outside [ref_start, ref_end] are never extended
+            // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
+            bool skip = (uflags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+            // Coordinates past either sequence end (a caller-supplied table or
+            // seed beyond the sequences) are rejected, not read.
+            if (rl > ref_len || ql > qlen) {
+                atomicCAS(&a.ctr->error, 0ull, 5ull);
+                skip = true;
+            }
+            if (!skip) {
+                has = true;
+                nocap = false;
+                dir = 0;
+                o = 0;
+                S = 0;
+                best = 0;
+                bpos = -1;
+                tiles = 0;
+                avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
+                sh_r = (rl & 7u) * 4u;
+                sh_q = (ql & 7u) * 4u;
+                wr = (int64_t)(rl >> 3) + 1;
+                wq = (int64_t)(ql >> 3) + 1;
+                carry_r = __ldg(ref + (rl >> 3));
+                carry_q = __ldg(qp + (ql >> 3));
+                ++ext_acc;
+            }
+        }
+        if (!__any_sync(SA_FULL, has || nx) && exhausted) break;
 
         // ---- one 8-base step per busy lane ----
         bool finished = false, to_long = false;
@@ -206,31 +253,60 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         if (has) {
             uint32_t rw, qw;
             if (dir == 0) {
-                rw = sa_load8(a.ref, (int64_t)rl + o);
-                qw = sa_load8(qp, (int64_t)ql + o);
+                const uint32_t hr = __ldg(ref + wr), hq = __ldg(qp + wq);
+                rw = __funnelshift_r(carry_r, hr, sh_r);
+                qw = __funnelshift_r(carry_q, hq, sh_q);
+                carry_r = hr;
+                carry_q = hq;
+                ++wr;
+                ++wq;
             } else {
-                rw = sa_rev_nibbles(sa_load8(a.ref, (int64_t)rl - o - 8));
-                qw = sa_rev_nibbles(sa_load8(qp, (int64_t)ql - o - 8));
+                const uint32_t lr = __ldg(ref + wr), lq = __ldg(qp + wq);
+                rw = sa_rev_nibbles(__funnelshift_r(lr, carry_r, sh_r));
+                qw = sa_rev_nibbles(__funnelshift_r(lq, carry_q, sh_q));
+                carry_r = lr;
+                carry_q = lq;
+                --wr;
+                --wq;
             }
+            uint32_t mlo, mhi;
+            sa_merge8(rw, qw, mlo, mhi);
             bool alive = true;
             uint32_t stop = 0;
+            if (o + 8 <= avail) {
 #pragma unroll
-            for (int kk = 0; kk < 8; ++kk) {
-                const uint32_t off = o + kk;  // 0-based index along this direction
-                const int sc = sub[(((rw >> (4 * kk)) & 7u) << 3) | ((qw >> (4 * kk)) & 7u)];
-                if (alive) {
-                    if (off >= avail) {
+                for (int kk = 0; kk < 8; ++kk) {
+                    const uint32_t off = o + kk;  // 0-based index along this direction
+                    const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
+                    S += sc;
+                    if (alive && S > best) {
+                        best = S;
+                        bpos = (int)off + dir;  // left offsets are 1-based
+                    }
+                    if (alive && best - S > xdrop) {
                         alive = false;
                         stop = off;
-                    } else {
-                        S += sc;
-                        if (S > best) {
-                            best = S;
-                            bpos = (int)off + dir;  // left offsets are 1-based
-                        }
-                        if (best - S > xdrop) {
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    const uint32_t off = o + kk;
+                    const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
+                    if (alive) {
+                        if (off >= avail) {
                             alive = false;
                             stop = off;
+                        } else {
+                            S += sc;
+                            if (S > best) {
+                                best = S;
+                                bpos = (int)off + dir;
+                            }
+                            if (best - S > xdrop) {
+                                alive = false;
+                                stop = off;
+                            }
                         }
                     }
                 }
@@ -246,6 +322,13 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     best = 0;
                     bpos = 0;
                     avail = min(rl, ql);
+                    // left window of the first step: bases [rl-8, rl)
+                    const int64_t pr = (int64_t)rl - 8, pq = (int64_t)ql - 8;
+                    wr = pr >> 3;
+                    wq = pq >> 3;
+                    carry_r = __ldg(ref + wr + 1);
+                    carry_q = __ldg(qp + wq + 1);
+                    // sh_r, sh_q unchanged: (x - 8) & 7 == x & 7
                 } else {
                     finished = true;
                 }
@@ -263,7 +346,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     const int64_t r0 = (int64_t)rl - Lpos, q0 = (int64_t)ql - Lpos, nb = (int64_t)ext + 1;
                     for (int64_t i = 0; i < nb; i += 8) {
                         uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
-                        sa_count_matches8(sa_load8(a.ref, r0 + i), sa_load8(qp, q0 + i), nm, cnt);
+                        sa_count_matches8(sa_load8(ref, r0 + i), sa_load8(qp, q0 + i), nm, cnt);
                     }
                 }
                 sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
@@ -554,7 +637,12 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
 
 void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
                            cudaStream_t st) {
-    sa_k_extend_lane<<<num_sms * t.ext_ctas_per_sm, t.ext_block, 0, st>>>(sa_ext_args(w, x, t), p);
+    // Register budget follows the CTAs per SM: 4 -> <= 64 registers, 3 -> <= 85, 2 -> <= 128.
+    const SaExtK a = sa_ext_args(w, x, t);
+    const int grid = num_sms * t.ext_ctas_per_sm;
+    if (t.ext_ctas_per_sm >= 4) sa_k_extend_lane<4><<<grid, 256, 0, st>>>(a, p);
+    else if (t.ext_ctas_per_sm == 3) sa_k_extend_lane<3><<<grid, 256, 0, st>>>(a, p);
+    else sa_k_extend_lane<2><<<grid, 256, 0, st>>>(a, p);
     sa_note_launch();
 }
 

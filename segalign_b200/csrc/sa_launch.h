@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "sa_internal.cuh"
 
@@ -18,15 +19,36 @@ struct SaCallDesc {
 };
 
 #define SA_BATCH_ITERS 16
-#define SA_MAX_KEY_ARRAYS 16
 
 // Batched unit: a query window [start, end) of one packed query, seeded on the device.
 struct SaBatchUnit {
     uint64_t slot_begin;    // first seed slot of the unit in the flattened slot space
     uint32_t q_start, q_end;// seed positions j in [q_start, q_end)
-    uint32_t keys_index;    // which key array (query buffer x strand)
+    const uint32_t* keys;   // per-position seed keys of the unit's query strand
     uint32_t unit;          // index into the SaUnit table
+    uint32_t pad;
 };
+
+// A batched unit resolved to device pointers (library query buffer or a
+// serving request's own buffers).
+struct SaResolvedUnit {
+    const uint32_t* keys;      // per-position seed keys of this strand
+    const uint32_t* q_packed;  // packed strand (forward or reverse complement)
+    uint32_t q_len;
+    uint32_t start, end;       // seed positions [start, end)
+    int32_t rev;
+};
+
+struct SaRunResult {
+    // per unit: HSP records (body) and hits
+    std::vector<std::vector<SaRec>>* recs;
+    std::vector<uint64_t>* hits;
+    SaCounters tot;
+    double ms_total, ms_lookup, ms_extend_lane, ms_extend_warp, ms_dedup, ms_copy;
+};
+
+// Runs resolved units on GPU 0's batch workspace (one batch at a time).
+int sa_run_units(const SaResolvedUnit* units, uint32_t n, bool want_out, SaRunResult* res);
 
 // Workspace of one slot (one in-flight call).  Sizes are capacities.
 struct SaWork {
@@ -69,7 +91,6 @@ struct SaWork {
     unsigned long long* unit_hit_end;   // [SA_MAX_UNITS]
     unsigned long long* bounds;         // [SA_MAX_UNITS * SA_BATCH_ITERS]
     uint32_t* unit_iters;               // [SA_MAX_UNITS]
-    const uint32_t** keys_arrays;       // [SA_MAX_KEY_ARRAYS]
 };
 
 #define SA_MAX_CTAS 1024
@@ -106,8 +127,7 @@ void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint3
 // ---- sa_lookup.cu ----
 void sa_launch_lookup_seeds(SaWork& w, const uint32_t* index, uint32_t nbuckets,
                             const SaParams& p, int G, cudaStream_t st);
-void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets,
-                            const uint32_t* const* keys_arrays, uint32_t n_bunits,
+void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, uint32_t n_bunits,
                             const SaParams& p, int G, cudaStream_t st);
 
 // ---- sa_extend.cu ----

@@ -161,7 +161,6 @@ struct SaSlotInfo {
 };
 
 __device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu, uint32_t u, uint64_t s,
-                                              const uint32_t* const* __restrict__ keys_arrays,
                                               const uint32_t* __restrict__ index, uint32_t nbuckets, int S) {
     SaSlotInfo r;
     const SaBatchUnit B = bu[u];
@@ -169,7 +168,7 @@ __device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu
     r.unit = B.unit;
     r.j = B.q_start + (uint32_t)(off / S);
     const uint32_t v = (uint32_t)(off % S);
-    uint32_t key = __ldg(keys_arrays[B.keys_index] + r.j);
+    uint32_t key = __ldg(B.keys + r.j);
     r.lo = 0;
     r.cnt = 0;
     if (key != SA_INVALID_KEY) {
@@ -185,7 +184,7 @@ __device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu
 
 __global__ void __launch_bounds__(256)
 sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc,
-                   const uint32_t* const* keys_arrays, const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
+                   const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
                    uint32_t* __restrict__ s_lo, uint32_t* __restrict__ s_cnt, unsigned long long* cta_a,
                    unsigned long long* cta_b) {
     uint64_t a, b;
@@ -194,7 +193,7 @@ sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restr
     unsigned long long hits = 0, nz = 0;
     for (uint64_t s = a + threadIdx.x; s < b; s += 256) {
         const uint32_t u = sa_find_unit(bu, nu, s);
-        const SaSlotInfo si = sa_slot(bu, u, s, keys_arrays, index, nbuckets, S);
+        const SaSlotInfo si = sa_slot(bu, u, s, index, nbuckets, S);
         s_lo[s] = si.lo;
         s_cnt[s] = si.cnt;
         hits += si.cnt;
@@ -322,11 +321,10 @@ __global__ void sa_k_bscope(SaSeedList cs, const unsigned long long* __restrict_
     }
 }
 
-void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, const uint32_t* const* keys_arrays,
-                            uint32_t n_bunits, const SaParams& p, int G, cudaStream_t st) {
+void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, uint32_t n_bunits, const SaParams& p,
+                            int G, cudaStream_t st) {
     const int S = p.transition ? 1 + p.kmer_size : 1;
-    sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, keys_arrays, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a,
-                                          w.cta_b);
+    sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a, w.cta_b);
     sa_note_launch();
     sa_k_scan_partials<<<1, 1024, 0, st>>>(w.cta_a, w.cta_b, G, &w.ctr->num_hits, &w.ctr->nnz);
     sa_note_launch();

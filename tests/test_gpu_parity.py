@@ -85,16 +85,19 @@ def test_max_hits_iterations(setup, max_hits):
         sf.set_max_hits(0)
 
 
-@pytest.mark.parametrize("lane_cap", [8, 32, 512])
-def test_tuning_does_not_change_results(setup, lane_cap):
+@pytest.mark.parametrize("lane_cap,ctas,tile", [(8, 2, 64), (8, 4, 1024), (32, 4, 1024), (64, 3, 100),
+                                                (512, 3, 1024), (4096, 3, 256), (512, 2, 4096)])
+def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile):
+    """Every tuning gives the same HSPs and extends every hit exactly once (tile counts)."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
     seeds = host_seeds(w.query, 250_000, 500_000)
-    want, _ = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
-    sf.set_tuning(lane_cap=lane_cap, tile_hits=64 if lane_cap == 8 else 1024)
+    want, st = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile)
     try:
-        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap}")
+        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas}")
+        assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(lane_cap=64, tile_hits=1024)
+        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=4, tile_hits=1024)
 
 
 def test_host_table_upload(setup):
