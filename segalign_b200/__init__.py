@@ -47,6 +47,7 @@ EXPORTS = [
     "sa_set_max_hits", "sa_set_rm_exclude_diagonal", "sa_last_call_stats", "sa_last_error", "sa_set_tuning",
     "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
     "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
+    "sa_set_tuning_param", "sa_get_tuning_param",
 ]
 
 
@@ -127,6 +128,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                         _P(SeederStats)]),
             "sa_seed_and_filter_batch": (C.c_int, [_P(Unit), C.c_uint32, segpp, u64p, u64p]),
             "sa_set_timing": (C.c_int, [C.c_int]),
+            "sa_set_tuning_param": (C.c_int, [C.c_char_p, C.c_int]),
+            "sa_get_tuning_param": (C.c_int, [C.c_char_p]),
             "sa_seed_and_filter_noalloc": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, _P(C.c_uint8),
                                                      C.c_uint64, u64p]),
             "sa_kernel_launches": (C.c_uint64, []),
@@ -323,8 +326,14 @@ class SeedFilter:
     def set_rm_exclude_diagonal(self, on: bool) -> None:
         self._chk(self.lib.sa_set_rm_exclude_diagonal(int(on)), "set_rm_exclude_diagonal")
 
-    def set_tuning(self, lane_cap=-1, ext_block=-1, ext_ctas_per_sm=-1, tile_hits=-1) -> None:
+    def set_tuning(self, lane_cap=-1, ext_block=-1, ext_ctas_per_sm=-1, tile_hits=-1, **named) -> None:
+        for k, v in named.items():  # step_bases, range_ctas
+            self._chk(self.lib.sa_set_tuning_param(k.encode(), int(v)), f"set_tuning({k})")
         self._chk(self.lib.sa_set_tuning(lane_cap, ext_block, ext_ctas_per_sm, tile_hits), "set_tuning")
+
+    def get_tuning(self) -> dict:
+        names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas")
+        return {n: int(self.lib.sa_get_tuning_param(n.encode())) for n in names}
 
     def set_timing(self, on: bool) -> None:
         self.lib.sa_set_timing(int(on))

@@ -143,7 +143,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{4096, 256, 4, 256, 296, 1024};
+    SaTuning tuning{4096, 256, 3, 256, 296, 256, 16};
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -1226,6 +1226,44 @@ int sa_set_max_hits(uint64_t max_hits) {
 int sa_set_rm_exclude_diagonal(int on) {
     G().rm_exclude_diag = on ? 1 : 0;
     return SA_OK;
+}
+
+int sa_set_tuning_param(const char* name, int value) {
+    if (!name) return SA_ERR_ARG;
+    SaTuning& t = G().tuning;
+    const std::string n = name;
+    if (n == "lane_cap") return sa_set_tuning(value, -1, -1, -1);
+    if (n == "ext_ctas_per_sm") return sa_set_tuning(-1, -1, value, -1);
+    if (n == "tile_hits") return sa_set_tuning(-1, -1, -1, value);
+    if (n == "step_bases") {
+        if (value != 8 && value != 16) return SA_ERR_ARG;
+        t.step_bases = value;
+        return SA_OK;
+    }
+    if (n == "range_ctas") {
+        if (value < 1 || value > SA_MAX_CTAS) return SA_ERR_ARG;
+        t.range_ctas = value;
+        return SA_OK;
+    }
+    if (n == "long_ctas_per_sm") {
+        if (value < 1 || value > 8) return SA_ERR_ARG;
+        t.long_block = 256;
+        return SA_OK;
+    }
+    sa_set_error(SA_ERR_ARG, "unknown tuning parameter %s", name);
+    return SA_ERR_ARG;
+}
+
+int sa_get_tuning_param(const char* name) {
+    if (!name) return SA_ERR_ARG;
+    const SaTuning& t = G().tuning;
+    const std::string n = name;
+    if (n == "lane_cap") return t.lane_cap;
+    if (n == "ext_ctas_per_sm") return t.ext_ctas_per_sm;
+    if (n == "tile_hits") return t.tile_hits;
+    if (n == "step_bases") return t.step_bases;
+    if (n == "range_ctas") return t.range_ctas;
+    return SA_ERR_ARG;
 }
 
 int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits) {

@@ -122,7 +122,46 @@ __device__ __forceinline__ void sa_merge8(uint32_t rw, uint32_t qw, uint32_t& lo
     hi = ((rw >> 4) & 0x0f0f0f0fu) | (qw & 0xf0f0f0f0u);
 }
 
-template <int MIN_CTAS>
+// Scores 8 bases of one direction: nibble pairs merged in (mlo, mhi), base k
+// at 0-based offset off0 + k.  `fast` = all 8 in bounds.
+template <bool FAST>
+__device__ __forceinline__ void sa_score8(const int* sub256, uint32_t mlo, uint32_t mhi, uint32_t off0, uint32_t avail,
+                                          int dir, int xdrop, int& S, int& best, int& bpos, bool& alive,
+                                          uint32_t& stop) {
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+        const uint32_t off = off0 + kk;
+        const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
+        if (FAST) {
+            S += sc;
+            if (alive && S > best) {
+                best = S;
+                bpos = (int)off + dir;  // left offsets are 1-based
+            }
+            if (alive && best - S > xdrop) {
+                alive = false;
+                stop = off;
+            }
+        } else if (alive) {
+            if (off >= avail) {
+                alive = false;
+                stop = off;
+            } else {
+                S += sc;
+                if (S > best) {
+                    best = S;
+                    bpos = (int)off + dir;
+                }
+                if (best - S > xdrop) {
+                    alive = false;
+                    stop = off;
+                }
+            }
+        }
+    }
+}
+
+template <int MIN_CTAS, int STEP>
 __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
     __shared__ int sub256[256];  // index (q << 4) | r
@@ -150,8 +189,12 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0, uflags = 0, qlen = 0;
     const uint32_t* __restrict__ qp = ref;
     int dir = 0;
-    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0, carry_r = 0, carry_q = 0;
-    int64_t wr = 0, wq = 0;  // word index of the next load (right: upper word, left: lower word)
+    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0;
+    // Sequence words of the current direction, loaded one step ahead: c* is
+    // the word shared with the previous step, n1/n2 the words of the coming
+    // step (n2 unused with 8-base steps); w* the index of the next load.
+    uint32_t c_r = 0, c_q = 0, n1_r = 0, n1_q = 0, n2_r = 0, n2_q = 0;
+    int64_t wr = 0, wq = 0;
     int S = 0, best = 0, bpos = -1, Rbest = 0, Rpos = -1;
     uint32_t tiles = 0;
     unsigned long long tiles_acc = 0, ext_acc = 0;
@@ -238,77 +281,89 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
                 sh_r = (rl & 7u) * 4u;
                 sh_q = (ql & 7u) * 4u;
-                wr = (int64_t)(rl >> 3) + 1;
-                wq = (int64_t)(ql >> 3) + 1;
-                carry_r = __ldg(ref + (rl >> 3));
-                carry_q = __ldg(qp + (ql >> 3));
+                const int64_t r0 = (int64_t)(rl >> 3), q0 = (int64_t)(ql >> 3);
+                c_r = __ldg(ref + r0);
+                c_q = __ldg(qp + q0);
+                n1_r = __ldg(ref + r0 + 1);
+                n1_q = __ldg(qp + q0 + 1);
+                if (STEP == 16) {
+                    n2_r = __ldg(ref + r0 + 2);
+                    n2_q = __ldg(qp + q0 + 2);
+                }
+                wr = r0 + (STEP == 16 ? 3 : 2);
+                wq = q0 + (STEP == 16 ? 3 : 2);
                 ++ext_acc;
             }
         }
         if (!__any_sync(SA_FULL, has || nx) && exhausted) break;
 
-        // ---- one 8-base step per busy lane ----
+        // ---- one STEP-base step per busy lane ----
         bool finished = false, to_long = false;
         int keep = 0, score = 0, Lpos = 0;
         if (has) {
-            uint32_t rw, qw;
-            if (dir == 0) {
-                const uint32_t hr = __ldg(ref + wr), hq = __ldg(qp + wq);
-                rw = __funnelshift_r(carry_r, hr, sh_r);
-                qw = __funnelshift_r(carry_q, hq, sh_q);
-                carry_r = hr;
-                carry_q = hq;
-                ++wr;
-                ++wq;
-            } else {
-                const uint32_t lr = __ldg(ref + wr), lq = __ldg(qp + wq);
-                rw = sa_rev_nibbles(__funnelshift_r(lr, carry_r, sh_r));
-                qw = sa_rev_nibbles(__funnelshift_r(lq, carry_q, sh_q));
-                carry_r = lr;
-                carry_q = lq;
-                --wr;
-                --wq;
-            }
-            uint32_t mlo, mhi;
-            sa_merge8(rw, qw, mlo, mhi);
             bool alive = true;
             uint32_t stop = 0;
-            if (o + 8 <= avail) {
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {
-                    const uint32_t off = o + kk;  // 0-based index along this direction
-                    const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
-                    S += sc;
-                    if (alive && S > best) {
-                        best = S;
-                        bpos = (int)off + dir;  // left offsets are 1-based
-                    }
-                    if (alive && best - S > xdrop) {
-                        alive = false;
-                        stop = off;
-                    }
+            // words of this step -> 8-base windows A (offsets o..o+7) and B (o+8..o+15)
+            uint32_t rwA, qwA, rwB = 0, qwB = 0;
+            if (dir == 0) {
+                rwA = __funnelshift_r(c_r, n1_r, sh_r);
+                qwA = __funnelshift_r(c_q, n1_q, sh_q);
+                if (STEP == 16) {
+                    rwB = __funnelshift_r(n1_r, n2_r, sh_r);
+                    qwB = __funnelshift_r(n1_q, n2_q, sh_q);
+                    c_r = n2_r;
+                    c_q = n2_q;
+                    n1_r = __ldg(ref + wr);
+                    n1_q = __ldg(qp + wq);
+                    n2_r = __ldg(ref + wr + 1);
+                    n2_q = __ldg(qp + wq + 1);
+                    wr += 2;
+                    wq += 2;
+                } else {
+                    c_r = n1_r;
+                    c_q = n1_q;
+                    n1_r = __ldg(ref + wr);
+                    n1_q = __ldg(qp + wq);
+                    ++wr;
+                    ++wq;
                 }
             } else {
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {
-                    const uint32_t off = o + kk;
-                    const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
-                    if (alive) {
-                        if (off >= avail) {
-                            alive = false;
-                            stop = off;
-                        } else {
-                            S += sc;
-                            if (S > best) {
-                                best = S;
-                                bpos = (int)off + dir;
-                            }
-                            if (best - S > xdrop) {
-                                alive = false;
-                                stop = off;
-                            }
-                        }
-                    }
+                // left: c = upper word, n1 = the word below it, n2 below n1
+                rwA = sa_rev_nibbles(__funnelshift_r(n1_r, c_r, sh_r));
+                qwA = sa_rev_nibbles(__funnelshift_r(n1_q, c_q, sh_q));
+                if (STEP == 16) {
+                    rwB = sa_rev_nibbles(__funnelshift_r(n2_r, n1_r, sh_r));
+                    qwB = sa_rev_nibbles(__funnelshift_r(n2_q, n1_q, sh_q));
+                    c_r = n2_r;
+                    c_q = n2_q;
+                    n1_r = __ldg(ref + wr);
+                    n1_q = __ldg(qp + wq);
+                    n2_r = __ldg(ref + wr - 1);
+                    n2_q = __ldg(qp + wq - 1);
+                    wr -= 2;
+                    wq -= 2;
+                } else {
+                    c_r = n1_r;
+                    c_q = n1_q;
+                    n1_r = __ldg(ref + wr);
+                    n1_q = __ldg(qp + wq);
+                    --wr;
+                    --wq;
+                }
+            }
+            uint32_t mlo, mhi;
+            sa_merge8(rwA, qwA, mlo, mhi);
+            if (o + STEP <= avail) {
+                sa_score8<true>(sub256, mlo, mhi, o, avail, dir, xdrop, S, best, bpos, alive, stop);
+                if (STEP == 16 && alive) {
+                    sa_merge8(rwB, qwB, mlo, mhi);
+                    sa_score8<true>(sub256, mlo, mhi, o + 8, avail, dir, xdrop, S, best, bpos, alive, stop);
+                }
+            } else {
+                sa_score8<false>(sub256, mlo, mhi, o, avail, dir, xdrop, S, best, bpos, alive, stop);
+                if (STEP == 16 && alive) {
+                    sa_merge8(rwB, qwB, mlo, mhi);
+                    sa_score8<false>(sub256, mlo, mhi, o + 8, avail, dir, xdrop, S, best, bpos, alive, stop);
                 }
             }
             if (!alive) {
@@ -322,18 +377,24 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     best = 0;
                     bpos = 0;
                     avail = min(rl, ql);
-                    // left window of the first step: bases [rl-8, rl)
-                    const int64_t pr = (int64_t)rl - 8, pq = (int64_t)ql - 8;
-                    wr = pr >> 3;
-                    wq = pq >> 3;
-                    carry_r = __ldg(ref + wr + 1);
-                    carry_q = __ldg(qp + wq + 1);
-                    // sh_r, sh_q unchanged: (x - 8) & 7 == x & 7
+                    // left: the first 8-base window is bases [rl-8, rl), low word
+                    // L0 = floor((rl-8)/8); shifts are unchanged ((x-8) & 7 == x & 7)
+                    const int64_t L0r = ((int64_t)rl - 8) >> 3, L0q = ((int64_t)ql - 8) >> 3;
+                    c_r = __ldg(ref + L0r + 1);
+                    c_q = __ldg(qp + L0q + 1);
+                    n1_r = __ldg(ref + L0r);
+                    n1_q = __ldg(qp + L0q);
+                    if (STEP == 16) {
+                        n2_r = __ldg(ref + L0r - 1);
+                        n2_q = __ldg(qp + L0q - 1);
+                    }
+                    wr = L0r - (STEP == 16 ? 2 : 1);
+                    wq = L0q - (STEP == 16 ? 2 : 1);
                 } else {
                     finished = true;
                 }
             } else {
-                o += 8;
+                o += STEP;
                 if (o >= a.lane_cap && !nocap) to_long = true;
             }
             if (finished) {
@@ -640,9 +701,17 @@ void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, 
     // Register budget follows the CTAs per SM: 4 -> <= 64 registers, 3 -> <= 85, 2 -> <= 128.
     const SaExtK a = sa_ext_args(w, x, t);
     const int grid = num_sms * t.ext_ctas_per_sm;
-    if (t.ext_ctas_per_sm >= 4) sa_k_extend_lane<4><<<grid, 256, 0, st>>>(a, p);
-    else if (t.ext_ctas_per_sm == 3) sa_k_extend_lane<3><<<grid, 256, 0, st>>>(a, p);
-    else sa_k_extend_lane<2><<<grid, 256, 0, st>>>(a, p);
+    const bool s16 = t.step_bases == 16;
+    if (t.ext_ctas_per_sm >= 4) {
+        if (s16) sa_k_extend_lane<4, 16><<<grid, 256, 0, st>>>(a, p);
+        else sa_k_extend_lane<4, 8><<<grid, 256, 0, st>>>(a, p);
+    } else if (t.ext_ctas_per_sm == 3) {
+        if (s16) sa_k_extend_lane<3, 16><<<grid, 256, 0, st>>>(a, p);
+        else sa_k_extend_lane<3, 8><<<grid, 256, 0, st>>>(a, p);
+    } else {
+        if (s16) sa_k_extend_lane<2, 16><<<grid, 256, 0, st>>>(a, p);
+        else sa_k_extend_lane<2, 8><<<grid, 256, 0, st>>>(a, p);
+    }
     sa_note_launch();
 }
 

@@ -87,7 +87,9 @@ def test_seeder_run_validates_arguments(built):
 
 def test_tuning_validation(built):
     lib = sa.load_library()
-    assert lib.sa_set_tuning(12, -1, -1, -1) == -1    # not a multiple of 8
+    assert lib.sa_set_tuning(12, -1, -1, -1) == -1    # not a multiple of the step
+    assert lib.sa_set_tuning_param(b"step_bases", 12) == -1
+    assert lib.sa_set_tuning_param(b"no_such_knob", 1) == -1
     assert lib.sa_set_tuning(-1, 128, -1, -1) == -1   # the lane kernel is built for 256 threads
     assert lib.sa_set_tuning(64, 256, 4, 1024) == 0
     assert lib.sa_set_tuning(512, 256, 3, 1024) == 0

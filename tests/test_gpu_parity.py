@@ -85,19 +85,20 @@ def test_max_hits_iterations(setup, max_hits):
         sf.set_max_hits(0)
 
 
-@pytest.mark.parametrize("lane_cap,ctas,tile", [(8, 2, 64), (8, 4, 1024), (32, 4, 1024), (64, 3, 100),
-                                                (512, 3, 1024), (4096, 3, 256), (512, 2, 4096)])
-def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile):
+@pytest.mark.parametrize("lane_cap,ctas,tile,step", [(8, 2, 64, 8), (16, 4, 1024, 16), (32, 4, 1024, 8),
+                                                     (64, 3, 100, 16), (512, 3, 1024, 8), (4096, 3, 256, 16),
+                                                     (512, 2, 4096, 16)])
+def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
     """Every tuning gives the same HSPs and extends every hit exactly once (tile counts)."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
     seeds = host_seeds(w.query, 250_000, 500_000)
     want, st = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
-    sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile)
+    sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile, step_bases=step)
     try:
-        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas}")
+        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas} step={step}")
         assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=4, tile_hits=1024)
+        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=256, step_bases=16)
 
 
 def test_host_table_upload(setup):
