@@ -141,9 +141,9 @@ int sa_rm_clear_query(void);
  * cudaMalloc/cudaFree).  Same output as sa_seed_and_filter(), written to the
  * caller's buffer out[0 .. out_cap); *out_len gets the record count (also
  * when the buffer is too small, which returns SA_ERR_CAPACITY).  Per-call
- * scratch lives in one fixed ~30 MB device array that every GPU using the
- * library holds until exit; at most 262,144 seed words and 262,144 HSP
- * candidates before deduplication per call, else SA_ERR_CAPACITY.  The first
+ * scratch lives in one fixed ~40 MB device array that every GPU using the
+ * library holds until exit; at most 262,144 seed words and 262,144 distinct
+ * HSPs per call, else SA_ERR_CAPACITY.  The first
  * call on a device looks up that array's address: make it before any stream
  * capture.  Calls share the array and run one at a time; calls that
  * overlapped on the GPU would race.  Needs the resident target, table and

@@ -262,6 +262,8 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
         {(void**)&w.rec[1], sizeof(SaRec) * surv_cap},
         {(void**)&w.scope[0], 4 * surv_cap},
         {(void**)&w.scope[1], 4 * surv_cap},
+        {(void**)&w.hset.keys, 16 * 2 * surv_cap},
+        {(void**)&w.hset.score, 4 * 2 * surv_cap},
         {(void**)&w.out, sizeof(SaRec) * surv_cap},
         {(void**)&w.out_scope, 4 * surv_cap},
         {(void**)&w.scope_count, 4 * SA_MAX_SCOPES},
@@ -376,6 +378,7 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
     sa_launch_lookup_seeds(w, d.index, (uint32_t)d.nbuckets, g.params, Gr, st);
+    sa_launch_hash_init(w, st);
     tm.mark(1);
     SaExtendArgs xa;
     xa.ref = d.ref.data;
@@ -534,6 +537,7 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     SA_CUDA_OK(cudaMemsetAsync(w.scope_flags, 0, 4 * n, st));
     SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
     sa_launch_lookup_batch(w, d.index, (uint32_t)d.nbuckets, n, g.params, Gr, st);
+    sa_launch_hash_init(w, st);
     tm.mark(1);
     SaExtendArgs xa;
     xa.ref = d.ref.data;
@@ -553,7 +557,7 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
     SaCounters c = *s->h_ctr;
-    if (c.surv_overflow) return SA_ERR_CAPACITY;
+    if (c.hash_overflow || c.error == 4) return SA_ERR_CAPACITY;
     if (c.error) return map_device_error(c.error);
     res.tot.num_hits += c.num_hits;
     res.tot.extended += c.extended;
@@ -933,10 +937,15 @@ int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_si
     // MAX_HITS = MAX_HITS_PER_GB * (float)(totalGlobalMem / 1 GiB) (:784, :791)
     float gb = (float)(g.devs[0].total_mem / 1073741824.0f);
     g.max_hits_default = (uint64_t)(int)(4194304 * gb);
-    g.surv_cap = env_u64("SA_SURV_CAP", 1ull << 25);
+    auto pow2_floor = [](uint64_t v) {
+        uint64_t p = 1;
+        while (p * 2 <= v) p <<= 1;
+        return p;
+    };
+    g.surv_cap = pow2_floor(env_u64("SA_SURV_CAP", 1ull << 25));
     g.long_cap = env_u64("SA_LONG_CAP", 1ull << 24);
     g.batch_slot_cap = env_u64("SA_BATCH_SLOT_CAP", 1ull << 28);
-    g.batch_surv_cap = env_u64("SA_BATCH_SURV_CAP", 1ull << 29);
+    g.batch_surv_cap = pow2_floor(env_u64("SA_BATCH_SURV_CAP", 1ull << 29));
     const int per_gpu = (int)env_u64("SA_SLOTS_PER_GPU", 2);
     for (size_t di = 0; di < g.devs.size(); ++di) {
         for (int k = 0; k < per_gpu; ++k) {

@@ -38,9 +38,7 @@ struct SaExtK {
     SaCounters* ctr;
     SaLongHit* long_q;
     uint64_t long_cap;
-    SaRec* surv;
-    uint32_t* surv_scope;
-    uint64_t surv_cap;
+    SaHashSet hset;
     uint32_t seed_size;
     int32_t xdrop, hspthresh, noentropy;
     uint32_t lane_cap;
@@ -177,6 +175,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
     const int xdrop = a.xdrop;
     const uint32_t* __restrict__ ref = a.ref;
+    const unsigned long long hmask = a.ctr->hash_mask;
 
     uint64_t tile_next = 0, tile_end = 0, cur = 0;
     bool exhausted = (H == 0);
@@ -441,29 +440,18 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
         }
-        // ---- survivor appends (warp-aggregated) ----
+        // ---- kept HSPs into the call's set of distinct HSPs ----
         {
             const bool emit = finished && keep;
             const uint32_t em = __ballot_sync(SA_FULL, emit);
             if (em) {
-                const int leader = __ffs(em) - 1;
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(em));
-                base = __shfl_sync(SA_FULL, base, leader);
+                if (lane == __ffs(em) - 1) atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(em));
                 if (emit) {
-                    const unsigned long long idx = base + __popc(em & lt);
-                    if (idx < a.surv_cap) {
-                        SaRec r;
-                        r.ref_start = rl - (uint32_t)Lpos;  // :606-608
-                        r.query_start = ql - (uint32_t)Lpos;
-                        r.len = (uint32_t)(Rpos + Lpos);
-                        r.score = score;
-                        if (uflags & 2u) r.query_start = ref_len - 1 - (r.query_start + r.len);  // rm :704-707
-                        a.surv[idx] = r;
-                        a.surv_scope[idx] = scope;
-                    } else {
-                        atomicAdd(&a.ctr->surv_overflow, 1ull);
-                    }
+                    const uint32_t rs = rl - (uint32_t)Lpos;  // :606-608
+                    uint32_t qs = ql - (uint32_t)Lpos;
+                    const uint32_t len = (uint32_t)(Rpos + Lpos);
+                    if (uflags & 2u) qs = ref_len - 1 - (qs + len);  // rm :704-707
+                    sa_hash_insert(a.hset, hmask, scope, rs, qs, len, score, &a.ctr->hash_overflow);
                 }
             }
         }
@@ -655,19 +643,12 @@ sa_k_extend_warp(SaExtK a, SaParams P) {
             int keep, score;
             sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
             if (keep) {
-                const unsigned long long o = atomicAdd(&a.ctr->surv_count, 1ull);
-                if (o < a.surv_cap) {
-                    SaRec r;
-                    r.ref_start = rl - (uint32_t)Lr.pos;
-                    r.query_start = ql - (uint32_t)Lr.pos;
-                    r.len = (uint32_t)ext;
-                    r.score = score;
-                    if (U.flags & 2u) r.query_start = a.ref_len - 1 - (r.query_start + r.len);
-                    a.surv[o] = r;
-                    a.surv_scope[o] = L.scope;
-                } else {
-                    atomicAdd(&a.ctr->surv_overflow, 1ull);
-                }
+                atomicAdd(&a.ctr->surv_count, 1ull);
+                const uint32_t rs = rl - (uint32_t)Lr.pos;
+                uint32_t qs = ql - (uint32_t)Lr.pos;
+                const uint32_t len = (uint32_t)ext;
+                if (U.flags & 2u) qs = a.ref_len - 1 - (qs + len);
+                sa_hash_insert(a.hset, a.ctr->hash_mask, L.scope, rs, qs, len, score, &a.ctr->hash_overflow);
             }
         }
     }
@@ -684,9 +665,7 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.ctr = w.ctr;
     a.long_q = w.long_q;
     a.long_cap = w.long_cap;
-    a.surv = w.rec[0];
-    a.surv_scope = w.scope[0];
-    a.surv_cap = w.surv_cap;
+    a.hset = w.hset;
     a.seed_size = x.seed_size;
     a.xdrop = x.xdrop;
     a.hspthresh = x.hspthresh;

@@ -86,8 +86,66 @@ struct SaCounters {
     unsigned long long uniq_count;     // records after dedup
     unsigned long long num_iter;       // MAX_HITS iterations
     unsigned long long error;          // nonzero = device-side error code
-    unsigned long long pad[3];
+    unsigned long long hash_mask;      // slots - 1 of this call's HSP hash set
+    unsigned long long hash_overflow;  // inserts that found no free slot
+    unsigned long long pad[3];         // device-side counts of the dedup stages
 };
+
+// Open-addressing set of distinct HSPs of one call: slot = 16-byte key
+// {(scope << 32) | ref_start, (query_start << 32) | len} claimed with a
+// 128-bit compare-and-swap (all ones = empty), plus the score.  Within one
+// scope the score is a function of the key (sum of substitution scores over
+// the segment, entropy of its base counts), so equal keys are equal records.
+struct SaHashSet {
+    unsigned long long* keys;  // [2 * slots]
+    int32_t* score;            // [slots]
+};
+
+#define SA_HASH_MAX_PROBES 4096
+
+__device__ __forceinline__ void sa_cas128(unsigned long long* p, unsigned long long c0, unsigned long long c1,
+                                          unsigned long long v0, unsigned long long v1, unsigned long long& o0,
+                                          unsigned long long& o1) {
+    asm volatile(
+        "{\n\t.reg .b128 d, b, c;\n\t"
+        "mov.b128 b, {%2, %3};\n\t"
+        "mov.b128 c, {%4, %5};\n\t"
+        "atom.global.cas.b128 d, [%6], b, c;\n\t"
+        "mov.b128 {%0, %1}, d;\n\t}"
+        : "=l"(o0), "=l"(o1)
+        : "l"(c0), "l"(c1), "l"(v0), "l"(v1), "l"(p)
+        : "memory");
+}
+
+__device__ __forceinline__ unsigned long long sa_hash_mix(unsigned long long a, unsigned long long b) {
+    unsigned long long x = a * 0x9e3779b97f4a7c15ull ^ (b + 0x632be59bd9b4e019ull + (a << 6) + (a >> 2));
+    x ^= x >> 31;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 29;
+    return x;
+}
+
+// Inserts one HSP; returns true when it was new.  Sets *overflow when no slot
+// was found within SA_HASH_MAX_PROBES (the set is too small).
+__device__ __forceinline__ bool sa_hash_insert(const SaHashSet& hs, unsigned long long mask, uint32_t scope,
+                                               uint32_t rs, uint32_t qs, uint32_t len, int32_t score,
+                                               unsigned long long* overflow) {
+    const unsigned long long k0 = ((unsigned long long)scope << 32) | rs;
+    const unsigned long long k1 = ((unsigned long long)qs << 32) | len;
+    unsigned long long h = sa_hash_mix(k0, k1) & mask;
+    for (int probe = 0; probe < SA_HASH_MAX_PROBES; ++probe) {
+        unsigned long long o0, o1;
+        sa_cas128(hs.keys + 2 * h, ~0ull, ~0ull, k0, k1, o0, o1);
+        if (o0 == ~0ull && o1 == ~0ull) {
+            hs.score[h] = score;
+            return true;
+        }
+        if (o0 == k0 && o1 == k1) return false;
+        h = (h + 1) & mask;
+    }
+    atomicAdd(overflow, 1ull);
+    return false;
+}
 
 // ---------------------------------------------------------------------------
 // Device helpers

@@ -7,16 +7,16 @@
 // cannot afford the device-wide synchronisation cudaMalloc and cudaFree may
 // perform while other streams are busy.  sa_seed_and_filter_noalloc() serves
 // them: its per-call scratch (seed words, bucket bounds, hit prefixes, the
-// compacted seed list, the long-extension queue, survivor and sort buffers,
-// counters) is carved out of one file-scope __device__ array of fixed size,
+// compacted seed list, the long-extension queue, the set of distinct HSPs,
+// sort buffers, counters) is carved out of one file-scope __device__ array of fixed size,
 // SA_NOALLOC_BYTES, which every GPU that loads the library holds until the
 // process exits.  The result is copied into a buffer the caller provides.
 //
 // Set-up: the first call on a device looks up the array's device address
 // with cudaGetSymbolAddress while that device is current; make that first
 // call before any stream capture.  Limits: at most SA_NOALLOC_MAX_SEEDS seed
-// words and SA_NOALLOC_MAX_SURVIVORS HSP candidates before deduplication per
-// call; larger calls are rejected with SA_ERR_CAPACITY.  All calls share the
+// words and SA_NOALLOC_MAX_SURVIVORS distinct HSPs per call; larger calls are
+// rejected with SA_ERR_CAPACITY.  All calls share the
 // array and it keeps the last call's contents: each call clears its counters
 // first, and calls run one at a time in this process (a host lock; each call
 // finishes on the GPU before it returns).  Calls that overlapped on the GPU
@@ -44,6 +44,7 @@ constexpr uint64_t kParts[] = {
     8 * SA_MAX_CTAS, 8 * SA_MAX_CTAS, 8 * SA_MAX_ITERS,  // cta_a, cta_b, limits
     sizeof(SaLongHit) * SA_NOALLOC_LONG_CAP,             // long queue
     sizeof(SaRec) * kSurv, sizeof(SaRec) * kSurv, 4 * kSurv, 4 * kSurv,  // rec[2], scope[2]
+    16 * 2 * kSurv, 4 * 2 * kSurv,                       // HSP set: keys, scores
     sizeof(SaRec) * kSurv, 4 * kSurv,                    // out, out_scope
     4 * SA_MAX_SCOPES, 4 * SA_MAX_SCOPES,                // scope_count, scope_flags
     4 * 256 * SA_SORT_MAX_DIGITS, 4 * 256 * (uint64_t)SA_MAX_CTAS + 4 * 64, 4 * (SA_SORT_MAX_DIGITS + 2),
@@ -108,6 +109,8 @@ void carve(void* base, SaWork& w) {
     take((void**)&w.rec[1]);
     take((void**)&w.scope[0]);
     take((void**)&w.scope[1]);
+    take((void**)&w.hset.keys);
+    take((void**)&w.hset.score);
     take((void**)&w.out);
     take((void**)&w.out_scope);
     take((void**)&w.scope_count);
@@ -174,6 +177,7 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, flags, sizeof flags, cudaMemcpyHostToDevice, st));
     const int G = std::min(v.tuning.range_ctas, SA_MAX_CTAS);
     sa_launch_lookup_seeds(w, v.index, (uint32_t)v.nbuckets, v.params, G, st);
+    sa_launch_hash_init(w, st);
     SaExtendArgs xa;
     xa.ref = v.ref;
     xa.ref_len = v.ref_len;
@@ -189,9 +193,8 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     SaCounters c;
     SA_CUDA_OK(cudaMemcpyAsync(&c, w.ctr, sizeof c, cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
-    if (c.surv_overflow) {
-        sa_set_error(SA_ERR_CAPACITY, "more than %u HSP candidates before deduplication (no-allocation limit)",
-                     SA_NOALLOC_MAX_SURVIVORS);
+    if (c.hash_overflow || c.error == 4) {
+        sa_set_error(SA_ERR_CAPACITY, "more than %u distinct HSPs (no-allocation limit)", SA_NOALLOC_MAX_SURVIVORS);
         return SA_ERR_CAPACITY;
     }
     if (c.error) {

@@ -210,11 +210,67 @@ sa_k_uniq_emit(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, 
 // st[0] <- 1 - final buffer of the last sort (the buffer the unique step wrote).
 __global__ void sa_k_flip_cur(int* st, int np) { st[0] = st[1 + np] ^ 1; }
 
+// Sizes the call's HSP set: the smallest power of two >= 2 * hits (at least
+// 1024), at most `max_slots` (a power of two), and marks every slot empty.
+__global__ void sa_k_hash_init(SaHashSet hs, SaCounters* ctr, unsigned long long max_slots) {
+    unsigned long long want = 2 * ctr->num_hits;
+    if (want < 1024) want = 1024;
+    unsigned long long slots = 1;
+    while (slots < want && slots < max_slots) slots <<= 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctr->hash_mask = slots - 1;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < 2 * slots;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        hs.keys[i] = ~0ull;
+}
+
+// Distinct HSPs out of the set into rec/scope (any order: the sort that
+// follows is total).  More distinct HSPs than `cap` is a capacity error.
+__global__ void __launch_bounds__(256)
+sa_k_hash_compact(SaHashSet hs, SaCounters* ctr, SaRec* rec, uint32_t* scope, uint64_t cap, unsigned long long* n_out) {
+    const unsigned long long slots = ctr->hash_mask + 1;
+    const int lane = threadIdx.x & 31;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < slots; base += stride) {
+        const unsigned long long s = base + threadIdx.x;
+        unsigned long long k0 = ~0ull, k1 = ~0ull;
+        if (s < slots) {
+            k0 = hs.keys[2 * s];
+            k1 = hs.keys[2 * s + 1];
+        }
+        const bool occ = k0 != ~0ull;
+        const uint32_t m = __ballot_sync(0xffffffffu, occ);
+        if (!m) continue;
+        unsigned long long at = 0;
+        if (lane == __ffs(m) - 1) at = atomicAdd(n_out, (unsigned long long)__popc(m));
+        at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+        if (occ) {
+            const unsigned long long i = at + __popc(m & sa_lanemask_lt());
+            if (i < cap) {
+                SaRec r;
+                r.ref_start = (uint32_t)k0;
+                r.query_start = (uint32_t)(k1 >> 32);
+                r.len = (uint32_t)k1;
+                r.score = hs.score[s];
+                rec[i] = r;
+                scope[i] = (uint32_t)(k0 >> 32);
+            } else {
+                atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_SURV_OVERFLOW);
+            }
+        }
+    }
+}
+
 __global__ void sa_k_dedup_prep(SaCounters* ctr, uint64_t cap, unsigned long long* n0, int* st) {
-    unsigned long long n = ctr->surv_count;
-    if (ctr->surv_overflow) atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_SURV_OVERFLOW);
-    *n0 = n < cap ? n : cap;
+    if (ctr->hash_overflow || *n0 > cap) atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_SURV_OVERFLOW);
+    if (*n0 > cap) *n0 = cap;
     st[0] = 0;
+}
+
+void sa_launch_hash_init(SaWork& w, cudaStream_t st) {
+    unsigned long long max_slots = 1;
+    while (max_slots * 2 <= 2 * w.surv_cap) max_slots <<= 1;
+    sa_k_hash_init<<<148 * 8, 256, 0, st>>>(w.hset, w.ctr, max_slots);
+    sa_note_launch();
 }
 
 __global__ void sa_k_copy_u64(unsigned long long* dst, const unsigned long long* src) { *dst = *src; }
@@ -250,6 +306,8 @@ void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s
     unsigned long long* n1 = &w.ctr->pad[1];
     unsigned long long* n2 = &w.ctr->pad[2];
     int* st = w.sort_in_buf;
+    sa_k_hash_compact<<<148 * 8, 256, 0, s>>>(w.hset, w.ctr, w.rec[0], w.scope[0], w.surv_cap, n0);
+    sa_note_launch();
     sa_k_dedup_prep<<<1, 1, 0, s>>>(w.ctr, w.surv_cap, n0, st);
     sa_note_launch();
     cudaMemsetAsync(w.scope_count, 0, sizeof(uint32_t) * SA_MAX_SCOPES, s);
