@@ -28,6 +28,7 @@
 #include "sa_radix.cuh"
 
 #define SA_FULL 0xffffffffu
+#define SA_LANE_TILE 224  // hits per warp tile of the lane-per-hit kernel (shared-memory records)
 
 struct SaExtK {
     const uint32_t* ref;
@@ -76,8 +77,14 @@ __device__ __forceinline__ uint64_t sa_warp_find_seed(const uint64_t* __restrict
 // c[] are the match counts per base over the HSP, already summed.
 __device__ __forceinline__ void sa_keep_score(int total, int ext, const int* cnt, bool entropy_branch,
                                               int hspthresh, int* keep, int* score) {
+    if (!entropy_branch) {
+        // E = 1.0: (int)((double)(float)total * 1.0) == (int)(float)total, score == total
+        *keep = (int)(float)total >= hspthresh;
+        *score = total;
+        return;
+    }
     double E = 1.0;  // entropy[warp_id] = 1.0f
-    if (entropy_branch) {
+    {
         short c0 = (short)cnt[0], c1 = (short)cnt[1], c2 = (short)cnt[2], c3 = (short)cnt[3];
         if ((int)c0 + (int)c1 + (int)c2 + (int)c3 >= 20) {
             double n = (double)(ext + 1);
@@ -114,60 +121,41 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 // merged into byte indices of a 256-entry score table, and the per-base
 // bounds test is only done in the step that reaches a sequence end.
 // ---------------------------------------------------------------------------
+// Byte b of lo (hi) = byte offset ((q << 3) | r) * 4 of the score of base 2b
+// (2b+1) in a 64-entry int table; codes are 0..7, so a byte never carries.
 __device__ __forceinline__ void sa_merge8(uint32_t rw, uint32_t qw, uint32_t& lo, uint32_t& hi) {
-    // byte b of lo = (q << 4) | r of base 2b, byte b of hi = that of base 2b+1
-    lo = (rw & 0x0f0f0f0fu) | ((qw & 0x0f0f0f0fu) << 4);
-    hi = ((rw >> 4) & 0x0f0f0f0fu) | (qw & 0xf0f0f0f0u);
+    lo = ((qw & 0x07070707u) << 5) | ((rw & 0x07070707u) << 2);
+    hi = (((qw >> 4) & 0x07070707u) << 5) | (((rw >> 4) & 0x07070707u) << 2);
 }
 
-// Scores 8 bases of one direction: nibble pairs merged in (mlo, mhi), base k
-// at 0-based offset off0 + k.  `fast` = all 8 in bounds.
+// Scores 8 bases of one direction (merged in lo/hi) at step-relative indices
+// k0 .. k0+7.  S = running score, best = running maximum (from 0), pk = step-
+// relative index of the last strict increase of best in this step, alive
+// cleared at the first base with best - S > xdrop.  FAST: all 8 in bounds;
+// else bases at off0 + k >= avail end the direction first.
 template <bool FAST>
-__device__ __forceinline__ void sa_score8(const int* sub256, uint32_t mlo, uint32_t mhi, uint32_t off0, uint32_t avail,
-                                          int dir, int xdrop, int& S, int& best, int& bpos, bool& alive,
-                                          uint32_t& stop) {
+__device__ __forceinline__ void sa_score8(const char* sub64b, uint32_t lo, uint32_t hi, int k0, uint32_t off0,
+                                          uint32_t avail, int xdrop, int& S, int& best, int& pk, bool& alive) {
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
-        const uint32_t off = off0 + kk;
-        const int sc = sub256[(((kk & 1) ? mhi : mlo) >> (8 * (kk >> 1))) & 0xffu];
-        if (FAST) {
-            S += sc;
-            if (alive && S > best) {
-                best = S;
-                bpos = (int)off + dir;  // left offsets are 1-based
-            }
-            if (alive && best - S > xdrop) {
-                alive = false;
-                stop = off;
-            }
-        } else if (alive) {
-            if (off >= avail) {
-                alive = false;
-                stop = off;
-            } else {
-                S += sc;
-                if (S > best) {
-                    best = S;
-                    bpos = (int)off + dir;
-                }
-                if (best - S > xdrop) {
-                    alive = false;
-                    stop = off;
-                }
-            }
-        }
+        const uint32_t byte = __byte_perm((kk & 1) ? hi : lo, 0, 0x4440 | (kk >> 1));
+        const int sc = *reinterpret_cast<const int*>(sub64b + byte);
+        if (!FAST && off0 + kk >= avail) alive = false;
+        S += sc;
+        const bool up = alive && S > best;
+        best = up ? S : best;
+        pk = up ? k0 + kk : pk;
+        alive = alive && (best - S <= xdrop);
     }
 }
 
 template <int MIN_CTAS, int STEP>
 __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
-    __shared__ int sub256[256];  // index (q << 4) | r
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        const int r = i & 15, q = i >> 4;
-        sub256[i] = (r < 8 && q < 8) ? P.sub_mat[r * 8 + q] : 0;
-    }
+    __shared__ int sub64[64];  // entry (q << 3) | r = score of target code r vs query code q
+    if (threadIdx.x < 64) sub64[threadIdx.x] = P.sub_mat[(threadIdx.x & 7) * 8 + (threadIdx.x >> 3)];
     __syncthreads();
+    const char* sub64b = reinterpret_cast<const char*>(sub64);
     if (a.ctr->error) return;
     const int lane = threadIdx.x & 31;
     const uint32_t lt = sa_lanemask_lt();
@@ -177,7 +165,13 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     const uint32_t* __restrict__ ref = a.ref;
     const unsigned long long hmask = a.ctr->hash_mask;
 
-    uint64_t tile_next = 0, tile_end = 0, cur = 0;
+    // Warp tile of hits expanded into shared memory: record i of the tile is
+    // {ref_loc, query_loc, scope, unit} of hit t0 + i.
+    constexpr int TILE = SA_LANE_TILE;
+    __shared__ uint4 s_hits[8][TILE];
+    __shared__ unsigned long long s_E[8][TILE + 1];
+    const int wid = threadIdx.x >> 5;
+    uint32_t tile_pos = 0, tile_n = 0;
     bool exhausted = (H == 0);
 
     // prefetched next hit
@@ -194,58 +188,67 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     // step (n2 unused with 8-base steps); w* the index of the next load.
     uint32_t c_r = 0, c_q = 0, n1_r = 0, n1_q = 0, n2_r = 0, n2_q = 0;
     int64_t wr = 0, wq = 0;
-    int S = 0, best = 0, bpos = -1, Rbest = 0, Rpos = -1;
+    // best position = upd_o + pk: upd_o = offset of the step that last raised
+    // best, pk = index inside that step
+    int S = 0, best = 0, pk = 0, Rbest = 0, Rpos = -1;
+    uint32_t upd_o = 0;
     uint32_t tiles = 0;
     unsigned long long tiles_acc = 0, ext_acc = 0;
 
     while (true) {
         // ---- refill: next slots of the tile's hits, in order ----
         const uint32_t need = __ballot_sync(SA_FULL, !nx);
-        if (need && !exhausted) {
-            if (tile_next >= tile_end) {
+        if (need && !(exhausted && tile_pos >= tile_n)) {
+            if (tile_pos >= tile_n) {
+                // Take the next tile of hits and expand it: the hits of the
+                // tile span at most TILE consecutive hit-bearing seeds from the
+                // one holding its first hit, so E over that window locates each
+                // hit's seed by binary search.
                 unsigned long long t0 = 0;
-                if (lane == 0) t0 = atomicAdd(&a.ctr->hit_cursor, (unsigned long long)a.tile_hits);
+                if (lane == 0) t0 = atomicAdd(&a.ctr->hit_cursor, (unsigned long long)TILE);
                 t0 = __shfl_sync(SA_FULL, t0, 0);
                 if (t0 >= H) {
                     exhausted = true;
+                    tile_n = tile_pos = 0;
                 } else {
-                    tile_next = t0;
-                    tile_end = (t0 + a.tile_hits < H) ? t0 + a.tile_hits : H;
-                    cur = sa_warp_find_seed(a.cs.E, nnz, t0);
+                    const uint32_t n = (uint32_t)min((unsigned long long)TILE, H - t0);
+                    const uint64_t c0 = sa_warp_find_seed(a.cs.E, nnz, t0);
+                    const uint32_t nw = (uint32_t)min((uint64_t)n, nnz - c0);  // seeds of the window
+                    for (uint32_t i = lane; i <= nw; i += 32) s_E[wid][i] = a.cs.E[c0 + i];  // E[nnz] == H
+                    __syncwarp();
+                    for (uint32_t i = lane; i < n; i += 32) {
+                        const unsigned long long h = t0 + i;
+                        uint32_t lo = 0, hi = nw;  // last k in [0, nw) with E[c0+k] <= h
+                        while (hi - lo > 1) {
+                            const uint32_t mid = (lo + hi) >> 1;
+                            if (s_E[wid][mid] <= h) lo = mid;
+                            else hi = mid;
+                        }
+                        const uint64_t c = c0 + lo;
+                        uint4 r;
+                        r.x = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - s_E[wid][lo])) + seed_size;  // find_hits :192
+                        r.y = a.cs.qpos[c] + seed_size;                                                      // find_hits :176
+                        r.z = a.cs.scope[c];
+                        r.w = a.cs.unit[c];
+                        s_hits[wid][i] = r;
+                    }
+                    __syncwarp();
+                    tile_n = n;
+                    tile_pos = 0;
                 }
             }
-            if (!exhausted) {
-                const uint64_t left_in_tile = tile_end - tile_next;
-                const uint32_t m = min((uint32_t)__popc(need), (uint32_t)(left_in_tile < 32 ? left_in_tile : 32));
+            if (tile_pos < tile_n) {
+                const uint32_t m = min((uint32_t)__popc(need), tile_n - tile_pos);
                 const uint32_t rank = __popc(need & lt);
-                const bool take = !nx && rank < m;
-                const uint64_t h = tile_next + rank;
-                // the m hits span at most m consecutive compacted seeds from `cur`
-                const uint64_t Ew = (cur + lane < nnz) ? a.cs.E[cur + lane] : ~0ull;
-                int k = 0;
-#pragma unroll
-                for (int s = 16; s >= 1; s >>= 1) {
-                    const uint64_t v = __shfl_sync(SA_FULL, Ew, k + s);
-                    if (v <= h) k += s;
-                }
-                const uint64_t Ek = __shfl_sync(SA_FULL, Ew, k);
-                // Next round starts at hit tile_next + m: its seed is the last
-                // window entry with E <= that hit, or cur + 32 when the window's
-                // last seed ends right before it.  Keeping `cur` at the seed of
-                // the round's first hit is what bounds a round to the window.
-                const uint64_t nxt = tile_next + m;
-                const uint32_t lm = __ballot_sync(SA_FULL, Ew <= nxt);
-                const uint64_t E32 = (cur + 32 < nnz) ? a.cs.E[cur + 32] : ~0ull;
-                if (take) {
-                    const uint64_t c = cur + k;
-                    n_rl = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - Ek)) + seed_size;  // find_hits :192
-                    n_ql = a.cs.qpos[c] + seed_size;                                         // find_hits :176
-                    n_scope = a.cs.scope[c];
-                    n_unit = a.cs.unit[c];
+                if (!nx && rank < m) {
+                    const uint4 r = s_hits[wid][tile_pos + rank];
+                    n_rl = r.x;
+                    n_ql = r.y;
+                    n_scope = r.z;
+                    n_unit = r.w;
                     nx = true;
                 }
-                cur = (lm == SA_FULL && E32 <= nxt) ? cur + 32 : cur + (31 - __clz(lm));
-                tile_next += m;
+                tile_pos += m;
             }
         }
         // ---- promote the next hit of idle lanes ----
@@ -275,7 +278,8 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 o = 0;
                 S = 0;
                 best = 0;
-                bpos = -1;
+                pk = 0;
+                upd_o = 0;
                 tiles = 0;
                 avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
                 sh_r = (rl & 7u) * 4u;
@@ -294,14 +298,13 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 ++ext_acc;
             }
         }
-        if (!__any_sync(SA_FULL, has || nx) && exhausted) break;
+        if (!__any_sync(SA_FULL, has || nx) && exhausted && tile_pos >= tile_n) break;
 
         // ---- one STEP-base step per busy lane ----
         bool finished = false, to_long = false;
         int keep = 0, score = 0, Lpos = 0;
         if (has) {
             bool alive = true;
-            uint32_t stop = 0;
             // words of this step -> 8-base windows A (offsets o..o+7) and B (o+8..o+15)
             uint32_t rwA, qwA, rwB = 0, qwB = 0;
             if (dir == 0) {
@@ -350,31 +353,37 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     --wq;
                 }
             }
-            uint32_t mlo, mhi;
-            sa_merge8(rwA, qwA, mlo, mhi);
+            const int best_in = best;
+            uint32_t lo, hi;
+            sa_merge8(rwA, qwA, lo, hi);
             if (o + STEP <= avail) {
-                sa_score8<true>(sub256, mlo, mhi, o, avail, dir, xdrop, S, best, bpos, alive, stop);
-                if (STEP == 16 && alive) {
-                    sa_merge8(rwB, qwB, mlo, mhi);
-                    sa_score8<true>(sub256, mlo, mhi, o + 8, avail, dir, xdrop, S, best, bpos, alive, stop);
+                sa_score8<true>(sub64b, lo, hi, 0, o, avail, xdrop, S, best, pk, alive);
+                if (STEP == 16) {
+                    sa_merge8(rwB, qwB, lo, hi);
+                    sa_score8<true>(sub64b, lo, hi, 8, o + 8, avail, xdrop, S, best, pk, alive);
                 }
             } else {
-                sa_score8<false>(sub256, mlo, mhi, o, avail, dir, xdrop, S, best, bpos, alive, stop);
-                if (STEP == 16 && alive) {
-                    sa_merge8(rwB, qwB, mlo, mhi);
-                    sa_score8<false>(sub256, mlo, mhi, o + 8, avail, dir, xdrop, S, best, bpos, alive, stop);
+                sa_score8<false>(sub64b, lo, hi, 0, o, avail, xdrop, S, best, pk, alive);
+                if (STEP == 16) {
+                    sa_merge8(rwB, qwB, lo, hi);
+                    sa_score8<false>(sub64b, lo, hi, 8, o + 8, avail, xdrop, S, best, pk, alive);
                 }
             }
+            if (best != best_in) upd_o = o;
             if (!alive) {
-                tiles += (stop >> 5) + 1;
+                // Steps start at multiples of STEP (8 or 16), so the stop offset
+                // lies in 32-base tile o >> 5 whichever base of the step it is.
+                tiles += (o >> 5) + 1;
+                const int pos = best > 0 ? (int)(upd_o + pk) : -1;
                 if (dir == 0) {
                     Rbest = best;
-                    Rpos = bpos;
+                    Rpos = pos;  // -1 when no positive score
                     dir = 1;
                     o = 0;
                     S = 0;
                     best = 0;
-                    bpos = 0;
+                    pk = 0;
+                    upd_o = 0;
                     avail = min(rl, ql);
                     // left: the first 8-base window is bases [rl-8, rl), low word
                     // L0 = floor((rl-8)/8); shifts are unchanged ((x-8) & 7 == x & 7)
@@ -397,7 +406,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 if (o >= a.lane_cap && !nocap) to_long = true;
             }
             if (finished) {
-                Lpos = bpos;
+                Lpos = best > 0 ? (int)(upd_o + pk) + 1 : 0;  // left offsets are 1-based
                 const int total = Rbest + best;
                 const int ext = Rpos + Lpos;
                 int cnt[4] = {0, 0, 0, 0};
