@@ -143,7 +143,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{4096, 256, 3, 256, 296, 256, 16};
+    SaTuning tuning{4096, 256, 3, 256, 296, 224, 16};
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -175,13 +175,25 @@ void set_shape_positions(SaParams& p, const std::string& shape) {
     p.seed_size = (int)shape.size();
 }
 
+// Allocates a packed sequence of len bases followed by its reversed copy
+// (sa_rev_words), all words E-filled.
 int alloc_packed(Packed& pk, uint64_t len) {
     pk.release();
-    uint64_t nw = (len + 7) / 8 + 2 * SA_PADW;
-    SA_CUDA_OK(cudaMalloc(&pk.base, nw * sizeof(uint32_t)));
+    const uint64_t nw = sa_rev_words(len);
+    SA_CUDA_OK(cudaMalloc(&pk.base, 2 * nw * sizeof(uint32_t)));
     pk.data = pk.base + SA_PADW;
     pk.len = len;
+    sa_launch_pad_fill(pk.base, 2 * nw, 0);
     return SA_OK;
+}
+
+// Writes the reversed copy of pk once its forward words are in place.
+void finish_packed(Packed& pk) { sa_launch_reverse_packed(pk.data, pk.len, pk.data + sa_rev_words(pk.len), false, 0); }
+
+// rc = reverse complement of pk (both allocated by alloc_packed), with its reversed copy.
+void make_rc_packed(const Packed& pk, Packed& rc) {
+    sa_launch_reverse_packed(pk.data, pk.len, rc.data, true, 0);
+    finish_packed(rc);
 }
 
 // Uploads text[0, len) and packs it into pk (and its reverse complement into rc if given).
@@ -189,9 +201,6 @@ int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed*
     SA_CUDA_OK(cudaSetDevice(d.dev));
     SA_TRY(alloc_packed(pk, len));
     if (rc) SA_TRY(alloc_packed(*rc, len));
-    uint64_t nw = (len + 7) / 8 + 2 * SA_PADW;
-    sa_launch_pad_fill(pk.base, nw, 0);
-    if (rc) sa_launch_pad_fill(rc->base, nw, 0);
     char* d_text = nullptr;
     const uint64_t chunk = 1ull << 28;  // 256 MiB text per round
     SA_CUDA_OK(cudaMalloc(&d_text, std::min<uint64_t>(len ? len : 1, chunk) + 16));
@@ -205,7 +214,8 @@ int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed*
         // chunk is a multiple of 8 bases, so word boundaries line up
         sa_launch_pack_text(d_text, n, pk.data + off / 8, 0);
     }
-    if (rc) sa_launch_rc_packed(pk.data, len, rc->data, 0);
+    finish_packed(pk);
+    if (rc) make_rc_packed(pk, *rc);
     cudaError_t e = cudaDeviceSynchronize();
     cudaFree(d_text);
     if (e != cudaSuccess) return sa_cuda_fail(e, "pack", __FILE__, __LINE__);
@@ -1023,8 +1033,7 @@ int sa_rm_send_query_write_request(void) {
         }
         SA_CUDA_OK(cudaSetDevice(d.dev));
         SA_TRY(alloc_packed(d.ref_rc, d.ref.len));
-        sa_launch_pad_fill(d.ref_rc.base, (d.ref.len + 7) / 8 + 2 * SA_PADW, 0);
-        sa_launch_rc_packed(d.ref.data, d.ref.len, d.ref_rc.data, 0);
+        make_rc_packed(d.ref, d.ref_rc);
         SA_CUDA_OK(cudaDeviceSynchronize());
     }
     return SA_OK;
@@ -1277,22 +1286,27 @@ int sa_get_tuning_param(const char* name) {
 
 int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits) {
     SaTuning& t = G().tuning;
-    if (lane_cap >= 0) {
-        if (lane_cap % 8 || lane_cap < 8) return SA_ERR_ARG;
-        t.lane_cap = lane_cap;
+    if (lane_cap >= 0 && (lane_cap % 8 || lane_cap < 8)) {
+        sa_set_error(SA_ERR_ARG, "lane_cap must be a positive multiple of 8 (got %d)", lane_cap);
+        return SA_ERR_ARG;
     }
-    if (ext_block >= 0) {
-        if (ext_block != 256) return SA_ERR_ARG;  // the lane kernel is compiled for 256 threads
-        t.ext_block = ext_block;
+    if (ext_block >= 0 && ext_block != 256) {
+        sa_set_error(SA_ERR_ARG, "ext_block must be 256: the lane kernel is compiled for 256 threads");
+        return SA_ERR_ARG;
     }
-    if (ext_ctas_per_sm >= 0) {
-        if (ext_ctas_per_sm < 2 || ext_ctas_per_sm > 4) return SA_ERR_ARG;
-        t.ext_ctas_per_sm = ext_ctas_per_sm;
+    if (ext_ctas_per_sm >= 0 && (ext_ctas_per_sm < 2 || ext_ctas_per_sm > 4)) {
+        sa_set_error(SA_ERR_ARG, "ext_ctas_per_sm must be 2, 3 or 4 (got %d)", ext_ctas_per_sm);
+        return SA_ERR_ARG;
     }
-    if (tile_hits >= 0) {
-        if (tile_hits < 32) return SA_ERR_ARG;
-        t.tile_hits = tile_hits;
+    if (tile_hits >= 0 && (tile_hits < 32 || tile_hits > 1024)) {
+        // the lane kernel keeps 8 warp tiles of 24 bytes per hit in shared memory
+        sa_set_error(SA_ERR_ARG, "tile_hits must be in [32, 1024] (got %d)", tile_hits);
+        return SA_ERR_ARG;
     }
+    if (lane_cap >= 0) t.lane_cap = lane_cap;
+    if (ext_block >= 0) t.ext_block = ext_block;
+    if (ext_ctas_per_sm >= 0) t.ext_ctas_per_sm = ext_ctas_per_sm;
+    if (tile_hits >= 0) t.tile_hits = tile_hits;
     return SA_OK;
 }
 

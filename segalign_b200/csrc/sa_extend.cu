@@ -15,20 +15,20 @@
 //     busy by handing out the next hits of its tile, in order, to lanes that
 //     finish ("refill").  Hits are expanded on the fly from the compacted seed
 //     list.  The short random-hit extensions that dominate the hit count
-//     finish here in one or two 8-base steps.
+//     finish here in a few steps.
 //   phase B (sa_k_extend_warp): hits whose extension passes `lane_cap` bases in
 //     one direction move to a queue and are redone by one warp per hit,
 //     256 bases per step.  Each lane scans 8 bases; warp scans carry the
 //     running sum and maximum.
 // Survivors are appended with warp-aggregated atomics, together with their
 // dedup scope.
+#include <algorithm>
 #include <climits>
 
 #include "sa_launch.h"
 #include "sa_radix.cuh"
 
 #define SA_FULL 0xffffffffu
-#define SA_LANE_TILE 224  // hits per warp tile of the lane-per-hit kernel (shared-memory records)
 
 struct SaExtK {
     const uint32_t* ref;
@@ -108,18 +108,37 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 }
 
 // ---------------------------------------------------------------------------
-// Phase A: one hit per lane, with the next hit of each lane prefetched.
+// Phase A: one hit per lane.
 //
-// A warp takes tiles of consecutive hits from a global counter.  Each lane
-// owns a current hit and a prefetched next hit: a refill round hands the next
-// hits of the tile, in order, to the lanes whose next slot is empty, and a
-// lane promotes its next hit the moment its current one finishes.  The
-// dependent loads that locate a hit (seed window of E, bucket start, query
-// position, target position, unit) are therefore issued one hit ahead of
-// their use.  A step scores 8 bases: the target and query words are carried
-// between steps (one new load per sequence), the two nibble streams are
-// merged into byte indices of a 256-entry score table, and the per-base
-// bounds test is only done in the step that reaches a sequence end.
+// A warp takes tiles of consecutive hits from a global counter and expands
+// each tile once into shared memory ({ref_loc, query_loc, scope, unit} per
+// hit).  Each lane owns a current hit and a prefetched next hit; a refill
+// round hands the next records of the tile, in order, to the lanes whose next
+// slot is empty, and a lane promotes its next hit the moment its current one
+// finishes.  Both directions of a hit run the same rightward scan: the left
+// extension from (rl, ql) is the right extension from (ref_len - rl,
+// qlen - ql) in the reversed copies that follow every packed sequence, so
+// lanes in different directions execute the same instructions.  A step
+// scores STEP bases as 8-base windows; the target and query words of the
+// next step are loaded while the current one is scored.
+//
+// Fast scoring form.  Inside a step, scores are kept relative to the best
+// score at the step start and packed with the base index k (0..STEP-1):
+//     P(k) = SCALE * (S(k) - best_in) + (STEP - 1 - k),   SCALE = 2 * STEP,
+// so a running max over P yields the best score together with the FIRST base
+// that reached it; the best carried in from earlier steps enters as
+// SCALE - 1, which no base of the step ties.  The X-drop stop test runs once
+// per 8-base window: with m = the window's minimum score and b = the best
+// score at the window's end, a base of the window stops the scan iff
+// b - m > xdrop, provided 7 * max(0, max_sub) <= xdrop (max_sub = largest
+// substitution score).  If b was reached at or before the minimum's base,
+// that base itself has best - S = b - m; otherwise b - m is a climb over at
+// most 7 bases, <= xdrop, and no base has best - S above b - m.  The same
+// bound shows that no base after a stop in the window can raise the best
+// (that takes a climb of more than xdrop), so the window's best is the best
+// at the stop.  Bases past the sequence end score -(xdrop + 1): the first of
+// them stops the scan.  Parameters outside the bound use the exact form,
+// which tests every base.
 // ---------------------------------------------------------------------------
 // Byte b of lo (hi) = byte offset ((q << 3) | r) * 4 of the score of base 2b
 // (2b+1) in a 64-entry int table; codes are 0..7, so a byte never carries.
@@ -128,19 +147,43 @@ __device__ __forceinline__ void sa_merge8(uint32_t rw, uint32_t qw, uint32_t& lo
     hi = (((qw >> 4) & 0x07070707u) << 5) | (((rw >> 4) & 0x07070707u) << 2);
 }
 
-// Scores 8 bases of one direction (merged in lo/hi) at step-relative indices
-// k0 .. k0+7.  S = running score, best = running maximum (from 0), pk = step-
-// relative index of the last strict increase of best in this step, alive
-// cleared at the first base with best - S > xdrop.  FAST: all 8 in bounds;
-// else bases at off0 + k >= avail end the direction first.
-template <bool FAST>
-__device__ __forceinline__ void sa_score8(const char* sub64b, uint32_t lo, uint32_t hi, int k0, uint32_t off0,
-                                          uint32_t avail, int xdrop, int& S, int& best, int& pk, bool& alive) {
+__device__ __forceinline__ int sa_tbl(const char* tblb, uint32_t lo, uint32_t hi, int kk) {
+    const uint32_t byte = __byte_perm((kk & 1) ? hi : lo, 0, 0x4440 | (kk >> 1));
+    return *reinterpret_cast<const int*>(tblb + byte);
+}
+
+// Fast form, one 8-base window.  P = packed running score, B = packed
+// running best; `at` takes B at the end of each window up to and including
+// the one that stops; `stop` is set by that window.  EDGE: bases at
+// off0 + k >= avail score `neg`.
+template <bool EDGE, int SH>
+__device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, uint32_t hi, uint32_t off0,
+                                               uint32_t avail, int neg, int xdrop, int& P, int& B, int& at,
+                                               bool& stop) {
+    int mn = INT_MAX;
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
-        const uint32_t byte = __byte_perm((kk & 1) ? hi : lo, 0, 0x4440 | (kk >> 1));
-        const int sc = *reinterpret_cast<const int*>(sub64b + byte);
-        if (!FAST && off0 + kk >= avail) alive = false;
+        int t = sa_tbl(tblb, lo, hi, kk);
+        if (EDGE && off0 + kk >= avail) t = neg;
+        P += t;
+        B = max(B, P);
+        mn = min(mn, P);
+    }
+    if (!stop) at = B;
+    stop = stop || ((B >> SH) - (mn >> SH) > xdrop);
+}
+
+// Exact form, one 8-base window at step-relative indices k0..k0+7: S =
+// running score, best = running maximum (from 0), pk = step-relative index
+// of the last strict increase of best, alive cleared at the first base with
+// best - S > xdrop or (EDGE) at off0 + k >= avail.
+template <bool EDGE>
+__device__ __forceinline__ void sa_window_exact(const char* tblb, uint32_t lo, uint32_t hi, int k0, uint32_t off0,
+                                                uint32_t avail, int xdrop, int& S, int& best, int& pk, bool& alive) {
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+        const int sc = sa_tbl(tblb, lo, hi, kk);
+        if (EDGE && off0 + kk >= avail) alive = false;
         S += sc;
         const bool up = alive && S > best;
         best = up ? S : best;
@@ -149,49 +192,69 @@ __device__ __forceinline__ void sa_score8(const char* sub64b, uint32_t lo, uint3
     }
 }
 
-template <int MIN_CTAS, int STEP>
+// Dynamic shared memory of the lane kernel for `tile` hits per warp tile.
+static size_t sa_lane_smem(uint32_t tile) {
+    return 256 + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 4;
+}
+
+template <int MIN_CTAS, int STEP, bool EXACT>
 __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
-    __shared__ int sub64[64];  // entry (q << 3) | r = score of target code r vs query code q
-    if (threadIdx.x < 64) sub64[threadIdx.x] = P.sub_mat[(threadIdx.x & 7) * 8 + (threadIdx.x >> 3)];
+    constexpr int NW = STEP / 8;                  // 8-base windows per step
+    constexpr int SCALE = 2 * STEP;               // packed score scale (fast form)
+    constexpr int SH = STEP == 8 ? 4 : 5;         // log2(SCALE)
+    static_assert(STEP == 8 || STEP == 16, "8- or 16-base steps");
+    // Shared memory: score table (64 ints), then per warp: tile records,
+    // tile E window, and a 64-entry ring of kept HSPs awaiting insertion.
+    extern __shared__ __align__(16) unsigned char sa_smem[];
+    const uint32_t TILE = a.tile_hits;
+    int* tbl = reinterpret_cast<int*>(sa_smem);  // entry (q << 3) | r: target code r vs query code q
+    if (threadIdx.x < 64) {
+        const int sc = P.sub_mat[(threadIdx.x & 7) * 8 + (threadIdx.x >> 3)];
+        tbl[threadIdx.x] = EXACT ? sc : sc * SCALE - 1;
+    }
     __syncthreads();
-    const char* sub64b = reinterpret_cast<const char*>(sub64);
+    const char* tblb = reinterpret_cast<const char*>(tbl);
     if (a.ctr->error) return;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t lt = sa_lanemask_lt();
+    uint4* const s_hits = reinterpret_cast<uint4*>(sa_smem + 256) + wid * TILE;
+    unsigned long long* const s_E =
+        reinterpret_cast<unsigned long long*>(sa_smem + 256 + 128 * (size_t)TILE) + wid * (TILE + 1);
+    unsigned char* const em_base = sa_smem + 256 + 128 * (size_t)TILE + 64 * (size_t)(TILE + 1);
+    uint4* const s_em = reinterpret_cast<uint4*>(em_base) + wid * 64;
+    int* const s_es = reinterpret_cast<int*>(em_base + 8 * 64 * 16) + wid * 64;
+
     const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
     const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
     const int xdrop = a.xdrop;
+    const int neg = -(xdrop + 1) * SCALE - 1;  // fast form: a base past the sequence end
     const uint32_t* __restrict__ ref = a.ref;
+    const uint32_t* __restrict__ ref_rev = ref + sa_rev_words(ref_len);
     const unsigned long long hmask = a.ctr->hash_mask;
 
-    // Warp tile of hits expanded into shared memory: record i of the tile is
-    // {ref_loc, query_loc, scope, unit} of hit t0 + i.
-    constexpr int TILE = SA_LANE_TILE;
-    __shared__ uint4 s_hits[8][TILE];
-    __shared__ unsigned long long s_E[8][TILE + 1];
-    const int wid = threadIdx.x >> 5;
     uint32_t tile_pos = 0, tile_n = 0;
     bool exhausted = (H == 0);
+    uint32_t em_head = 0, em_tail = 0;  // ring of kept HSPs (warp-uniform cursors)
 
     // prefetched next hit
     bool nx = false;
     uint32_t n_rl = 0, n_ql = 0, n_scope = 0, n_unit = 0;
     // current hit
-    bool has = false, nocap = false;
+    bool has = false, nocap = false, setup = false;
     uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0, uflags = 0, qlen = 0;
     const uint32_t* __restrict__ qp = ref;
     int dir = 0;
+    // scan of the current direction: offset, bases available, word shifts,
+    // words w[0..NW] of the coming step, next word addresses
     uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0;
-    // Sequence words of the current direction, loaded one step ahead: c* is
-    // the word shared with the previous step, n1/n2 the words of the coming
-    // step (n2 unused with 8-base steps); w* the index of the next load.
-    uint32_t c_r = 0, c_q = 0, n1_r = 0, n1_q = 0, n2_r = 0, n2_q = 0;
-    int64_t wr = 0, wq = 0;
-    // best position = upd_o + pk: upd_o = offset of the step that last raised
-    // best, pk = index inside that step
-    int S = 0, best = 0, pk = 0, Rbest = 0, Rpos = -1;
-    uint32_t upd_o = 0;
+    uint32_t w_r[NW + 1], w_q[NW + 1];
+#pragma unroll
+    for (int j = 0; j <= NW; ++j) w_r[j] = w_q[j] = 0;
+    const uint32_t* __restrict__ pr = ref;
+    const uint32_t* __restrict__ pq = ref;
+    // running score, best, offset of the first base reaching best
+    int S = 0, best = 0, bpos = 0, Rbest = 0, Rpos = -1;
     uint32_t tiles = 0;
     unsigned long long tiles_acc = 0, ext_acc = 0;
 
@@ -214,23 +277,23 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     const uint32_t n = (uint32_t)min((unsigned long long)TILE, H - t0);
                     const uint64_t c0 = sa_warp_find_seed(a.cs.E, nnz, t0);
                     const uint32_t nw = (uint32_t)min((uint64_t)n, nnz - c0);  // seeds of the window
-                    for (uint32_t i = lane; i <= nw; i += 32) s_E[wid][i] = a.cs.E[c0 + i];  // E[nnz] == H
+                    for (uint32_t i = lane; i <= nw; i += 32) s_E[i] = a.cs.E[c0 + i];  // E[nnz] == H
                     __syncwarp();
                     for (uint32_t i = lane; i < n; i += 32) {
                         const unsigned long long h = t0 + i;
                         uint32_t lo = 0, hi = nw;  // last k in [0, nw) with E[c0+k] <= h
                         while (hi - lo > 1) {
                             const uint32_t mid = (lo + hi) >> 1;
-                            if (s_E[wid][mid] <= h) lo = mid;
+                            if (s_E[mid] <= h) lo = mid;
                             else hi = mid;
                         }
                         const uint64_t c = c0 + lo;
                         uint4 r;
-                        r.x = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - s_E[wid][lo])) + seed_size;  // find_hits :192
-                        r.y = a.cs.qpos[c] + seed_size;                                                      // find_hits :176
+                        r.x = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - s_E[lo])) + seed_size;  // find_hits :192
+                        r.y = a.cs.qpos[c] + seed_size;                                                 // find_hits :176
                         r.z = a.cs.scope[c];
                         r.w = a.cs.unit[c];
-                        s_hits[wid][i] = r;
+                        s_hits[i] = r;
                     }
                     __syncwarp();
                     tile_n = n;
@@ -241,7 +304,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 const uint32_t m = min((uint32_t)__popc(need), tile_n - tile_pos);
                 const uint32_t rank = __popc(need & lt);
                 if (!nx && rank < m) {
-                    const uint4 r = s_hits[wid][tile_pos + rank];
+                    const uint4 r = s_hits[tile_pos + rank];
                     n_rl = r.x;
                     n_ql = r.y;
                     n_scope = r.z;
@@ -274,130 +337,107 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             if (!skip) {
                 has = true;
                 nocap = false;
+                setup = true;
                 dir = 0;
-                o = 0;
-                S = 0;
-                best = 0;
-                pk = 0;
-                upd_o = 0;
                 tiles = 0;
-                avail = (rl < ref_len && ql < qlen) ? min(ref_len - rl, qlen - ql) : 0u;
-                sh_r = (rl & 7u) * 4u;
-                sh_q = (ql & 7u) * 4u;
-                const int64_t r0 = (int64_t)(rl >> 3), q0 = (int64_t)(ql >> 3);
-                c_r = __ldg(ref + r0);
-                c_q = __ldg(qp + q0);
-                n1_r = __ldg(ref + r0 + 1);
-                n1_q = __ldg(qp + q0 + 1);
-                if (STEP == 16) {
-                    n2_r = __ldg(ref + r0 + 2);
-                    n2_q = __ldg(qp + q0 + 2);
-                }
-                wr = r0 + (STEP == 16 ? 3 : 2);
-                wq = q0 + (STEP == 16 ? 3 : 2);
                 ++ext_acc;
             }
         }
         if (!__any_sync(SA_FULL, has || nx) && exhausted && tile_pos >= tile_n) break;
 
+        // ---- start of a direction: new hit (right) or after its right end (left) ----
+        if (setup) {
+            setup = false;
+            const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
+            avail = min(ref_len - sr, qlen - sq);
+            sh_r = (sr & 7u) * 4u;
+            sh_q = (sq & 7u) * 4u;
+            pr = (dir ? ref_rev : ref) + (sr >> 3);
+            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
+#pragma unroll
+            for (int j = 0; j <= NW; ++j) {
+                w_r[j] = __ldg(pr + j);
+                w_q[j] = __ldg(pq + j);
+            }
+            pr += NW + 1;
+            pq += NW + 1;
+            o = 0;
+            S = 0;
+            best = 0;
+            bpos = 0;
+        }
+
         // ---- one STEP-base step per busy lane ----
         bool finished = false, to_long = false;
         int keep = 0, score = 0, Lpos = 0;
         if (has) {
-            bool alive = true;
-            // words of this step -> 8-base windows A (offsets o..o+7) and B (o+8..o+15)
-            uint32_t rwA, qwA, rwB = 0, qwB = 0;
-            if (dir == 0) {
-                rwA = __funnelshift_r(c_r, n1_r, sh_r);
-                qwA = __funnelshift_r(c_q, n1_q, sh_q);
-                if (STEP == 16) {
-                    rwB = __funnelshift_r(n1_r, n2_r, sh_r);
-                    qwB = __funnelshift_r(n1_q, n2_q, sh_q);
-                    c_r = n2_r;
-                    c_q = n2_q;
-                    n1_r = __ldg(ref + wr);
-                    n1_q = __ldg(qp + wq);
-                    n2_r = __ldg(ref + wr + 1);
-                    n2_q = __ldg(qp + wq + 1);
-                    wr += 2;
-                    wq += 2;
-                } else {
-                    c_r = n1_r;
-                    c_q = n1_q;
-                    n1_r = __ldg(ref + wr);
-                    n1_q = __ldg(qp + wq);
-                    ++wr;
-                    ++wq;
-                }
-            } else {
-                // left: c = upper word, n1 = the word below it, n2 below n1
-                rwA = sa_rev_nibbles(__funnelshift_r(n1_r, c_r, sh_r));
-                qwA = sa_rev_nibbles(__funnelshift_r(n1_q, c_q, sh_q));
-                if (STEP == 16) {
-                    rwB = sa_rev_nibbles(__funnelshift_r(n2_r, n1_r, sh_r));
-                    qwB = sa_rev_nibbles(__funnelshift_r(n2_q, n1_q, sh_q));
-                    c_r = n2_r;
-                    c_q = n2_q;
-                    n1_r = __ldg(ref + wr);
-                    n1_q = __ldg(qp + wq);
-                    n2_r = __ldg(ref + wr - 1);
-                    n2_q = __ldg(qp + wq - 1);
-                    wr -= 2;
-                    wq -= 2;
-                } else {
-                    c_r = n1_r;
-                    c_q = n1_q;
-                    n1_r = __ldg(ref + wr);
-                    n1_q = __ldg(qp + wq);
-                    --wr;
-                    --wq;
-                }
+            uint32_t rwin[NW], qwin[NW];
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+                rwin[j] = __funnelshift_r(w_r[j], w_r[j + 1], sh_r);
+                qwin[j] = __funnelshift_r(w_q[j], w_q[j + 1], sh_q);
             }
-            const int best_in = best;
+            w_r[0] = w_r[NW];
+            w_q[0] = w_q[NW];
+#pragma unroll
+            for (int j = 1; j <= NW; ++j) {
+                w_r[j] = __ldg(pr + j - 1);
+                w_q[j] = __ldg(pq + j - 1);
+            }
+            pr += NW;
+            pq += NW;
+            const bool edge = o + STEP > avail;
+            bool stop = false;
             uint32_t lo, hi;
-            sa_merge8(rwA, qwA, lo, hi);
-            if (o + STEP <= avail) {
-                sa_score8<true>(sub64b, lo, hi, 0, o, avail, xdrop, S, best, pk, alive);
-                if (STEP == 16) {
-                    sa_merge8(rwB, qwB, lo, hi);
-                    sa_score8<true>(sub64b, lo, hi, 8, o + 8, avail, xdrop, S, best, pk, alive);
+            if (EXACT) {
+                bool alive = true;
+                int pk = 0;
+                const int best_in = best;
+                if (!edge) {
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        sa_merge8(rwin[j], qwin[j], lo, hi);
+                        sa_window_exact<false>(tblb, lo, hi, 8 * j, o + 8 * j, avail, xdrop, S, best, pk, alive);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        sa_merge8(rwin[j], qwin[j], lo, hi);
+                        sa_window_exact<true>(tblb, lo, hi, 8 * j, o + 8 * j, avail, xdrop, S, best, pk, alive);
+                    }
                 }
+                if (best != best_in) bpos = (int)o + pk;
+                stop = !alive;
             } else {
-                sa_score8<false>(sub64b, lo, hi, 0, o, avail, xdrop, S, best, pk, alive);
-                if (STEP == 16) {
-                    sa_merge8(rwB, qwB, lo, hi);
-                    sa_score8<false>(sub64b, lo, hi, 8, o + 8, avail, xdrop, S, best, pk, alive);
+                int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
+                if (!edge) {
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        sa_merge8(rwin[j], qwin[j], lo, hi);
+                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, neg, xdrop, Pk, B, at, stop);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        sa_merge8(rwin[j], qwin[j], lo, hi);
+                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, neg, xdrop, Pk, B, at, stop);
+                    }
                 }
+                const int low = at & (SCALE - 1);
+                if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
+                const int best_in = best;
+                best = best_in + (at >> SH);
+                S = best_in + (Pk >> SH);  // exact after a full step without a stop
             }
-            if (best != best_in) upd_o = o;
-            if (!alive) {
+            if (stop) {
                 // Steps start at multiples of STEP (8 or 16), so the stop offset
                 // lies in 32-base tile o >> 5 whichever base of the step it is.
                 tiles += (o >> 5) + 1;
-                const int pos = best > 0 ? (int)(upd_o + pk) : -1;
                 if (dir == 0) {
                     Rbest = best;
-                    Rpos = pos;  // -1 when no positive score
+                    Rpos = best > 0 ? bpos : -1;  // -1 when no positive score
                     dir = 1;
-                    o = 0;
-                    S = 0;
-                    best = 0;
-                    pk = 0;
-                    upd_o = 0;
-                    avail = min(rl, ql);
-                    // left: the first 8-base window is bases [rl-8, rl), low word
-                    // L0 = floor((rl-8)/8); shifts are unchanged ((x-8) & 7 == x & 7)
-                    const int64_t L0r = ((int64_t)rl - 8) >> 3, L0q = ((int64_t)ql - 8) >> 3;
-                    c_r = __ldg(ref + L0r + 1);
-                    c_q = __ldg(qp + L0q + 1);
-                    n1_r = __ldg(ref + L0r);
-                    n1_q = __ldg(qp + L0q);
-                    if (STEP == 16) {
-                        n2_r = __ldg(ref + L0r - 1);
-                        n2_q = __ldg(qp + L0q - 1);
-                    }
-                    wr = L0r - (STEP == 16 ? 2 : 1);
-                    wq = L0q - (STEP == 16 ? 2 : 1);
+                    setup = true;
                 } else {
                     finished = true;
                 }
@@ -406,7 +446,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 if (o >= a.lane_cap && !nocap) to_long = true;
             }
             if (finished) {
-                Lpos = best > 0 ? (int)(upd_o + pk) + 1 : 0;  // left offsets are 1-based
+                Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
                 const int total = Rbest + best;
                 const int ext = Rpos + Lpos;
                 int cnt[4] = {0, 0, 0, 0};
@@ -449,19 +489,45 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
         }
-        // ---- kept HSPs into the call's set of distinct HSPs ----
+        // ---- kept HSPs: into the warp's ring, inserted 32 at a time into
+        // the call's set of distinct HSPs ----
         {
             const bool emit = finished && keep;
             const uint32_t em = __ballot_sync(SA_FULL, emit);
             if (em) {
-                if (lane == __ffs(em) - 1) atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(em));
                 if (emit) {
                     const uint32_t rs = rl - (uint32_t)Lpos;  // :606-608
                     uint32_t qs = ql - (uint32_t)Lpos;
                     const uint32_t len = (uint32_t)(Rpos + Lpos);
                     if (uflags & 2u) qs = ref_len - 1 - (qs + len);  // rm :704-707
-                    sa_hash_insert(a.hset, hmask, scope, rs, qs, len, score, &a.ctr->hash_overflow);
+                    const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
+                    s_em[slot] = make_uint4(rs, qs, len, scope);
+                    s_es[slot] = score;
                 }
+                em_tail += __popc(em);
+                if (em_tail - em_head >= 32) {
+                    __syncwarp();
+                    const uint32_t slot = (em_head + lane) & 63u;
+                    const uint4 r = s_em[slot];
+                    const int sc = s_es[slot];
+                    __syncwarp();  // slots are rewritten by later appends
+                    em_head += 32;
+                    if (lane == 0) atomicAdd(&a.ctr->surv_count, 32ull);
+                    sa_hash_insert(a.hset, hmask, r.w, r.x, r.y, r.z, sc, &a.ctr->hash_overflow);
+                }
+            }
+        }
+    }
+    // remaining kept HSPs of the ring
+    {
+        const uint32_t left = em_tail - em_head;
+        __syncwarp();
+        if (left) {
+            if (lane == 0) atomicAdd(&a.ctr->surv_count, (unsigned long long)left);
+            if ((uint32_t)lane < left) {
+                const uint32_t slot = (em_head + lane) & 63u;
+                const uint4 r = s_em[slot];
+                sa_hash_insert(a.hset, hmask, r.w, r.x, r.y, r.z, s_es[slot], &a.ctr->hash_overflow);
             }
         }
     }
@@ -684,22 +750,45 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     return a;
 }
 
+// The fast scoring form holds when 7 * max(0, max_sub) <= xdrop (see the
+// phase A notes); the magnitude limits keep its packed scores inside 31 bits.
+static bool sa_lane_fast_form(const SaParams& p) {
+    int mx = 0, mn = 0;
+    for (int i = 0; i < 64; ++i) {
+        mx = std::max(mx, p.sub_mat[i]);
+        mn = std::min(mn, p.sub_mat[i]);
+    }
+    return p.xdrop >= 0 && p.xdrop <= (1 << 16) && 7ll * mx <= p.xdrop && mn >= -(1 << 20);
+}
+
+template <int C, int STEP, bool EXACT>
+static void sa_lane_launch(const SaExtK& a, const SaParams& p, int grid, size_t smem, cudaStream_t st) {
+    cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    sa_k_extend_lane<C, STEP, EXACT><<<grid, 256, smem, st>>>(a, p);
+}
+
+template <int C>
+static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, int grid, size_t smem,
+                             cudaStream_t st) {
+    if (step == 16) {
+        if (exact) sa_lane_launch<C, 16, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 16, false>(a, p, grid, smem, st);
+    } else {
+        if (exact) sa_lane_launch<C, 8, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 8, false>(a, p, grid, smem, st);
+    }
+}
+
 void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
                            cudaStream_t st) {
     // Register budget follows the CTAs per SM: 4 -> <= 64 registers, 3 -> <= 85, 2 -> <= 128.
     const SaExtK a = sa_ext_args(w, x, t);
     const int grid = num_sms * t.ext_ctas_per_sm;
-    const bool s16 = t.step_bases == 16;
-    if (t.ext_ctas_per_sm >= 4) {
-        if (s16) sa_k_extend_lane<4, 16><<<grid, 256, 0, st>>>(a, p);
-        else sa_k_extend_lane<4, 8><<<grid, 256, 0, st>>>(a, p);
-    } else if (t.ext_ctas_per_sm == 3) {
-        if (s16) sa_k_extend_lane<3, 16><<<grid, 256, 0, st>>>(a, p);
-        else sa_k_extend_lane<3, 8><<<grid, 256, 0, st>>>(a, p);
-    } else {
-        if (s16) sa_k_extend_lane<2, 16><<<grid, 256, 0, st>>>(a, p);
-        else sa_k_extend_lane<2, 8><<<grid, 256, 0, st>>>(a, p);
-    }
+    const size_t smem = sa_lane_smem(a.tile_hits);
+    const bool exact = !sa_lane_fast_form(p);
+    if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, grid, smem, st);
+    else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, grid, smem, st);
+    else sa_lane_dispatch<2>(a, p, t.step_bases, exact, grid, smem, st);
     sa_note_launch();
 }
 

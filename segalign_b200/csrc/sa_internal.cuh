@@ -6,6 +6,11 @@
 // Every packed array carries SA_PADW words of padding on both sides (filled
 // with E codes) so that 8-base windows next to either end can be loaded
 // without bounds checks; scoring itself never reads past the sequence.
+// Every packed sequence of the library is followed, in the same allocation,
+// by its reversed copy (base i = base len-1-i of the sequence, with its own
+// padding): word 0 of the copy lies sa_rev_words(len) words after word 0 of
+// the sequence.  A leftward extension from position p is a rightward scan of
+// the copy from position len - p.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -14,6 +19,9 @@
 #define SA_NUC 8
 #define SA_WARP 32
 #define SA_INVALID_KEY 0xffffffffu
+
+// Words from word 0 of a packed sequence of `len` bases to word 0 of its reversed copy.
+__host__ __device__ __forceinline__ uint64_t sa_rev_words(uint64_t len) { return (len + 7) / 8 + 2 * SA_PADW; }
 
 // Filter parameters (src/seed_filter.cu:20-27; InitializeProcessor :780-796).
 struct SaParams {

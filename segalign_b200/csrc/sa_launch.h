@@ -112,7 +112,8 @@ struct SaTuning {
 
 // ---- sa_pack.cu ----
 void sa_launch_pack_text(const char* d_text, uint64_t len, uint32_t* packed, cudaStream_t st);
-void sa_launch_rc_packed(const uint32_t* in, uint64_t len, uint32_t* out, cudaStream_t st);
+// out = in reversed (complement: reverse complement); out needs (len + 7) / 8 words.
+void sa_launch_reverse_packed(const uint32_t* in, uint64_t len, uint32_t* out, bool complement, cudaStream_t st);
 void sa_launch_pad_fill(uint32_t* packed_base, uint64_t nwords_with_pad, cudaStream_t st);
 // Table build: keys of target positions, ordered compaction of valid ones.
 void sa_launch_table_keys(const uint32_t* ref, uint32_t start, uint64_t num_steps, uint32_t step,

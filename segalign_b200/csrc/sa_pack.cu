@@ -87,22 +87,25 @@ __global__ void sa_k_pack_text(const uint8_t* __restrict__ text, uint64_t len, u
     }
 }
 
-// Reverse complement of a packed sequence: rc[i] = comp(in[len-1-i]),
-// A<->T, C<->G, L/N/X/E unchanged (src/seed_filter.cu:96-125).
-__global__ void sa_k_rc_packed(const uint32_t* __restrict__ in, uint64_t len, uint32_t* __restrict__ out,
-                               uint64_t nwords) {
+// Reversed copy of a packed sequence: out[i] = in[len-1-i]; with COMP the
+// codes 0..3 are complemented as well (reverse complement, A<->T, C<->G;
+// L/N/X/E unchanged; src/seed_filter.cu:96-125).  Bases past len are E.
+template <bool COMP>
+__global__ void sa_k_reverse_packed(const uint32_t* __restrict__ in, uint64_t len, uint32_t* __restrict__ out,
+                                    uint64_t nwords) {
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nwords;
          w += (uint64_t)gridDim.x * blockDim.x) {
-        // rc bases 8w..8w+7 come from in[len-1-8w-k]; load in[len-8w-8 .. len-8w)
+        // output bases 8w..8w+7 come from in[len-1-8w-k]; load in[len-8w-8 .. len-8w)
         int64_t p = (int64_t)len - (int64_t)(8 * w) - 8;
         uint32_t x = sa_load8(in, p);
         // reverse nibble order
         x = __byte_perm(x, 0, 0x0123);
         x = ((x >> 4) & 0x0f0f0f0fu) | ((x & 0x0f0f0f0fu) << 4);
-        // complement codes 0..3 (bit 2 clear) by xor 3
-        uint32_t m = (~(x >> 2)) & 0x11111111u;
-        x ^= m * 3u;
-        // bases past len are E
+        if (COMP) {
+            // complement codes 0..3 (bit 2 clear) by xor 3
+            uint32_t m = (~(x >> 2)) & 0x11111111u;
+            x ^= m * 3u;
+        }
         uint64_t b = w * 8;
         if (b + 8 > len) {
 #pragma unroll
@@ -126,11 +129,12 @@ void sa_launch_pack_text(const char* d_text, uint64_t len, uint32_t* packed, cud
     sa_note_launch();
 }
 
-void sa_launch_rc_packed(const uint32_t* in, uint64_t len, uint32_t* out, cudaStream_t st) {
+void sa_launch_reverse_packed(const uint32_t* in, uint64_t len, uint32_t* out, bool complement, cudaStream_t st) {
     uint64_t nwords = (len + 7) / 8;
     if (!nwords) return;
     int blocks = (int)std::min<uint64_t>((nwords + 255) / 256, 148ull * 16);
-    sa_k_rc_packed<<<blocks, 256, 0, st>>>(in, len, out, nwords);
+    if (complement) sa_k_reverse_packed<true><<<blocks, 256, 0, st>>>(in, len, out, nwords);
+    else sa_k_reverse_packed<false><<<blocks, 256, 0, st>>>(in, len, out, nwords);
     sa_note_launch();
 }
 

@@ -93,3 +93,6 @@ def test_tuning_validation(built):
     assert lib.sa_set_tuning(-1, 128, -1, -1) == -1   # the lane kernel is built for 256 threads
     assert lib.sa_set_tuning(64, 256, 4, 1024) == 0
     assert lib.sa_set_tuning(512, 256, 3, 1024) == 0
+    assert lib.sa_set_tuning(-1, -1, -1, 2048) == -1  # shared-memory tiles hold at most 1024 hits
+    assert lib.sa_get_tuning_param(b"tile_hits") == 1024
+    assert lib.sa_set_tuning(4096, 256, 3, 224) == 0
