@@ -89,11 +89,12 @@ __device__ __forceinline__ void sa_keep_score(int total, int ext, const int* cnt
         if ((int)c0 + (int)c1 + (int)c2 + (int)c3 >= 20) {
             double n = (double)(ext + 1);
             double e = 0.0;
-            short cs[4] = {c0, c1, c2, c3};
-#pragma unroll
+            // one log at a time (same accumulation order): keeps the register peak low
+#pragma unroll 1
             for (int b = 0; b < 4; ++b) {
-                double q = (double)cs[b] / n;
-                double lg = (cs[b] != 0) ? log((double)cs[b] / n) : 0.0;
+                const short cb = b == 0 ? c0 : b == 1 ? c1 : b == 2 ? c2 : c3;
+                double q = (double)cb / n;
+                double lg = (cb != 0) ? log((double)cb / n) : 0.0;
                 e = fma(q, lg, e);
             }
             E = -e / (double)logf(4.0f);
@@ -192,9 +193,52 @@ __device__ __forceinline__ void sa_window_exact(const char* tblb, uint32_t lo, u
     }
 }
 
+// Keep test of `n` (<= 32) ring candidates from slot `head` on, one per lane:
+// entropy factor from the per-base match counts over the HSP when the total
+// is in the entropy range (src/seed_filter.cu:580-621), then insertion of the
+// kept ones into the call's set of distinct HSPs (rm: query start flipped on
+// the reverse strand, repeat_masker_src/seed_filter.cu:704-707).  Called by
+// the whole warp; leaves the slots free for reuse.
+__device__ __forceinline__ void sa_flush_candidates(const SaExtK& a, const uint4* s_em, const uint2* s_ex,
+                                                    uint32_t head, uint32_t n) {
+    const int lane = threadIdx.x & 31;
+    const bool on = (uint32_t)lane < n;
+    uint4 r = make_uint4(0, 0, 0, 0);
+    uint2 x = make_uint2(0, 0);
+    if (on) {
+        const uint32_t slot = (head + lane) & 63u;
+        r = s_em[slot];
+        x = s_ex[slot];
+    }
+    __syncwarp();  // slots are rewritten by later appends
+    int keep = 0, score = 0;
+    SaUnit U{};
+    if (on) {
+        U = a.units[x.y];
+        const int total = (int)x.x, ext = (int)r.z;
+        int cnt[4] = {0, 0, 0, 0};
+        const bool eb = sa_entropy_branch(a, total);
+        if (eb) {
+            const int64_t nb = (int64_t)ext + 1;
+            for (int64_t i = 0; i < nb; i += 8) {
+                uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
+                sa_count_matches8(sa_load8(a.ref, (int64_t)r.x + i), sa_load8(U.q_packed, (int64_t)r.y + i), nm, cnt);
+            }
+        }
+        sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
+    }
+    const uint32_t km = __ballot_sync(SA_FULL, keep != 0);
+    if (lane == 0 && km) atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(km));
+    if (keep) {
+        uint32_t qs = r.y;
+        if (U.flags & 2u) qs = a.ref_len - 1 - (qs + r.z);
+        sa_hash_insert(a.hset, a.ctr->hash_mask, r.w, r.x, qs, r.z, score, &a.ctr->hash_overflow);
+    }
+}
+
 // Dynamic shared memory of the lane kernel for `tile` hits per warp tile.
 static size_t sa_lane_smem(uint32_t tile) {
-    return 256 + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 4;
+    return 256 + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 8;
 }
 
 template <int MIN_CTAS, int STEP, bool EXACT>
@@ -205,7 +249,8 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     constexpr int SH = STEP == 8 ? 4 : 5;         // log2(SCALE)
     static_assert(STEP == 8 || STEP == 16, "8- or 16-base steps");
     // Shared memory: score table (64 ints), then per warp: tile records,
-    // tile E window, and a 64-entry ring of kept HSPs awaiting insertion.
+    // tile E window, and a 64-entry ring of candidate HSPs awaiting the keep
+    // test and insertion.
     extern __shared__ __align__(16) unsigned char sa_smem[];
     const uint32_t TILE = a.tile_hits;
     int* tbl = reinterpret_cast<int*>(sa_smem);  // entry (q << 3) | r: target code r vs query code q
@@ -223,15 +268,12 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         reinterpret_cast<unsigned long long*>(sa_smem + 256 + 128 * (size_t)TILE) + wid * (TILE + 1);
     unsigned char* const em_base = sa_smem + 256 + 128 * (size_t)TILE + 64 * (size_t)(TILE + 1);
     uint4* const s_em = reinterpret_cast<uint4*>(em_base) + wid * 64;
-    int* const s_es = reinterpret_cast<int*>(em_base + 8 * 64 * 16) + wid * 64;
+    uint2* const s_ex = reinterpret_cast<uint2*>(em_base + 8 * 64 * 16) + wid * 64;
 
     const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
     const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
     const int xdrop = a.xdrop;
-    const int neg = -(xdrop + 1) * SCALE - 1;  // fast form: a base past the sequence end
     const uint32_t* __restrict__ ref = a.ref;
-    const uint32_t* __restrict__ ref_rev = ref + sa_rev_words(ref_len);
-    const unsigned long long hmask = a.ctr->hash_mask;
 
     uint32_t tile_pos = 0, tile_n = 0;
     bool exhausted = (H == 0);
@@ -242,8 +284,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     uint32_t n_rl = 0, n_ql = 0, n_scope = 0, n_unit = 0;
     // current hit
     bool has = false, nocap = false, setup = false;
-    uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0, uflags = 0, qlen = 0;
-    const uint32_t* __restrict__ qp = ref;
+    uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0;
     int dir = 0;
     // scan of the current direction: offset, bases available, word shifts,
     // words w[0..NW] of the coming step, next word addresses
@@ -255,8 +296,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     const uint32_t* __restrict__ pq = ref;
     // running score, best, offset of the first base reaching best
     int S = 0, best = 0, bpos = 0, Rbest = 0, Rpos = -1;
-    uint32_t tiles = 0;
-    unsigned long long tiles_acc = 0, ext_acc = 0;
+    uint32_t tiles = 0, tiles_acc = 0, ext_acc = 0;  // per-lane statistics (32-bit per lane)
 
     while (true) {
         // ---- refill: next slots of the tile's hits, in order ----
@@ -322,15 +362,12 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             scope = n_scope;
             unit_id = n_unit;
             const SaUnit U = a.units[unit_id];
-            qp = U.q_packed;
-            qlen = U.q_len;
-            uflags = U.flags;
             // rm: hits outside [ref_start, ref_end] are never extended
             // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
-            bool skip = (uflags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+            bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
             // Coordinates past either sequence end (a caller-supplied table or
             // seed beyond the sequences) are rejected, not read.
-            if (rl > ref_len || ql > qlen) {
+            if (rl > ref_len || ql > U.q_len) {
                 atomicCAS(&a.ctr->error, 0ull, 5ull);
                 skip = true;
             }
@@ -343,16 +380,19 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 ++ext_acc;
             }
         }
-        if (!__any_sync(SA_FULL, has || nx) && exhausted && tile_pos >= tile_n) break;
+        const bool done = !__any_sync(SA_FULL, has || nx) && exhausted && tile_pos >= tile_n;
 
         // ---- start of a direction: new hit (right) or after its right end (left) ----
         if (setup) {
             setup = false;
+            const SaUnit U = a.units[unit_id];
+            const uint32_t* __restrict__ qp = U.q_packed;
+            const uint32_t qlen = U.q_len;
             const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
             avail = min(ref_len - sr, qlen - sq);
             sh_r = (sr & 7u) * 4u;
             sh_q = (sq & 7u) * 4u;
-            pr = (dir ? ref_rev : ref) + (sr >> 3);
+            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
             pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
 #pragma unroll
             for (int j = 0; j <= NW; ++j) {
@@ -369,7 +409,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
 
         // ---- one STEP-base step per busy lane ----
         bool finished = false, to_long = false;
-        int keep = 0, score = 0, Lpos = 0;
+        int Lpos = 0, total = 0;
         if (has) {
             uint32_t rwin[NW], qwin[NW];
 #pragma unroll
@@ -414,13 +454,15 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, neg, xdrop, Pk, B, at, stop);
+                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, xdrop, Pk, B, at, stop);
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, neg, xdrop, Pk, B, at, stop);
+                        // a base past the sequence end scores -(xdrop + 1)
+                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(xdrop + 1) * SCALE - 1, xdrop,
+                                                 Pk, B, at, stop);
                     }
                 }
                 const int low = at & (SCALE - 1);
@@ -447,18 +489,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             }
             if (finished) {
                 Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
-                const int total = Rbest + best;
-                const int ext = Rpos + Lpos;
-                int cnt[4] = {0, 0, 0, 0};
-                const bool eb = sa_entropy_branch(a, total);
-                if (eb) {
-                    const int64_t r0 = (int64_t)rl - Lpos, q0 = (int64_t)ql - Lpos, nb = (int64_t)ext + 1;
-                    for (int64_t i = 0; i < nb; i += 8) {
-                        uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
-                        sa_count_matches8(sa_load8(ref, r0 + i), sa_load8(qp, q0 + i), nm, cnt);
-                    }
-                }
-                sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
+                total = Rbest + best;
                 tiles_acc += tiles;
                 has = false;
             }
@@ -489,47 +520,27 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
         }
-        // ---- kept HSPs: into the warp's ring, inserted 32 at a time into
-        // the call's set of distinct HSPs ----
+        // ---- candidate HSPs (total >= hspthresh; the entropy factor is at
+        // most 1, so lower totals are never kept) into the warp's ring ----
         {
-            const bool emit = finished && keep;
+            const bool emit = finished && (int)(float)total >= a.hspthresh;
             const uint32_t em = __ballot_sync(SA_FULL, emit);
-            if (em) {
-                if (emit) {
-                    const uint32_t rs = rl - (uint32_t)Lpos;  // :606-608
-                    uint32_t qs = ql - (uint32_t)Lpos;
-                    const uint32_t len = (uint32_t)(Rpos + Lpos);
-                    if (uflags & 2u) qs = ref_len - 1 - (qs + len);  // rm :704-707
-                    const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
-                    s_em[slot] = make_uint4(rs, qs, len, scope);
-                    s_es[slot] = score;
-                }
-                em_tail += __popc(em);
-                if (em_tail - em_head >= 32) {
-                    __syncwarp();
-                    const uint32_t slot = (em_head + lane) & 63u;
-                    const uint4 r = s_em[slot];
-                    const int sc = s_es[slot];
-                    __syncwarp();  // slots are rewritten by later appends
-                    em_head += 32;
-                    if (lane == 0) atomicAdd(&a.ctr->surv_count, 32ull);
-                    sa_hash_insert(a.hset, hmask, r.w, r.x, r.y, r.z, sc, &a.ctr->hash_overflow);
-                }
+            if (emit) {
+                const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
+                // {ref_start, query_start (before the rm flip), len, scope}, {total, unit} (:606-608)
+                s_em[slot] = make_uint4(rl - (uint32_t)Lpos, ql - (uint32_t)Lpos, (uint32_t)(Rpos + Lpos), scope);
+                s_ex[slot] = make_uint2((uint32_t)total, unit_id);
+            }
+            em_tail += __popc(em);
+            // full batches of 32; at the end, whatever is left
+            while (em_tail - em_head >= 32 || (done && em_tail != em_head)) {
+                const uint32_t n = min(em_tail - em_head, 32u);
+                __syncwarp();
+                sa_flush_candidates(a, s_em, s_ex, em_head, n);
+                em_head += n;
             }
         }
-    }
-    // remaining kept HSPs of the ring
-    {
-        const uint32_t left = em_tail - em_head;
-        __syncwarp();
-        if (left) {
-            if (lane == 0) atomicAdd(&a.ctr->surv_count, (unsigned long long)left);
-            if ((uint32_t)lane < left) {
-                const uint32_t slot = (em_head + lane) & 63u;
-                const uint4 r = s_em[slot];
-                sa_hash_insert(a.hset, hmask, r.w, r.x, r.y, r.z, s_es[slot], &a.ctr->hash_overflow);
-            }
-        }
+        if (done) break;
     }
     // flush statistics
     unsigned long long t = tiles_acc, e = ext_acc;

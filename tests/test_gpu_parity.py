@@ -121,7 +121,7 @@ def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
         compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas} step={step}")
         assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=224, step_bases=16)
+        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=16)
 
 
 def test_host_table_upload(setup):
