@@ -217,7 +217,7 @@ const char* sa_last_error(void);
 int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits);
 
 /* Named tuning parameters: "lane_cap", "ext_ctas_per_sm" (2..4), "tile_hits" (32..1024),
- * "step_bases" (8 or 16 bases scored per lane step), "range_ctas" (CTAs of the
+ * "step_bases" (8, 16 or 32 bases scored per lane step), "range_ctas" (CTAs of the
  * lookup/sort kernels).  Results never depend on them.  Returns SA_OK or
  * SA_ERR_ARG; sa_get_tuning_param returns the current value. */
 int sa_set_tuning_param(const char* name, int value);

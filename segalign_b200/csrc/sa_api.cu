@@ -143,7 +143,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{4096, 256, 3, 256, 296, 160, 16};
+    SaTuning tuning{4096, 256, 3, 256, 296, 160, 32};
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -1254,7 +1254,10 @@ int sa_set_tuning_param(const char* name, int value) {
     if (n == "ext_ctas_per_sm") return sa_set_tuning(-1, -1, value, -1);
     if (n == "tile_hits") return sa_set_tuning(-1, -1, -1, value);
     if (n == "step_bases") {
-        if (value != 8 && value != 16) return SA_ERR_ARG;
+        if (value != 8 && value != 16 && value != 32) {
+            sa_set_error(SA_ERR_ARG, "step_bases must be 8, 16 or 32 (got %d)", value);
+            return SA_ERR_ARG;
+        }
         t.step_bases = value;
         return SA_OK;
     }

@@ -29,6 +29,7 @@
 #include "sa_radix.cuh"
 
 #define SA_FULL 0xffffffffu
+#define SA_LANE_TABLES 256  // lane kernel: the 64-entry score table
 
 struct SaExtK {
     const uint32_t* ref;
@@ -238,7 +239,7 @@ __device__ __forceinline__ void sa_flush_candidates(const SaExtK& a, const uint4
 
 // Dynamic shared memory of the lane kernel for `tile` hits per warp tile.
 static size_t sa_lane_smem(uint32_t tile) {
-    return 256 + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 8;
+    return SA_LANE_TABLES + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 8;
 }
 
 template <int MIN_CTAS, int STEP, bool EXACT>
@@ -246,14 +247,18 @@ __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
     constexpr int NW = STEP / 8;                  // 8-base windows per step
     constexpr int SCALE = 2 * STEP;               // packed score scale (fast form)
-    constexpr int SH = STEP == 8 ? 4 : 5;         // log2(SCALE)
-    static_assert(STEP == 8 || STEP == 16, "8- or 16-base steps");
+    constexpr int SH = STEP == 8 ? 4 : STEP == 16 ? 5 : 6;  // log2(SCALE)
+    static_assert(STEP == 8 || STEP == 16 || STEP == 32, "8-, 16- or 32-base steps");
+    // Read-ahead: the last step reads up to 2 * NW + 1 words past the last base.
+    static_assert(2 * NW + 2 <= SA_PADW, "padding shorter than the read-ahead");
     // Shared memory: score table (64 ints), then per warp: tile records,
     // tile E window, and a 64-entry ring of candidate HSPs awaiting the keep
     // test and insertion.
     extern __shared__ __align__(16) unsigned char sa_smem[];
     const uint32_t TILE = a.tile_hits;
-    int* tbl = reinterpret_cast<int*>(sa_smem);  // entry (q << 3) | r: target code r vs query code q
+    // entry (q << 3) | r: target code r vs query code q.  Codes 0..3 use
+    // entries 0..27 only, one per bank: lookups of A/C/G/T pairs never conflict.
+    int* tbl = reinterpret_cast<int*>(sa_smem);
     if (threadIdx.x < 64) {
         const int sc = P.sub_mat[(threadIdx.x & 7) * 8 + (threadIdx.x >> 3)];
         tbl[threadIdx.x] = EXACT ? sc : sc * SCALE - 1;
@@ -263,20 +268,19 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     if (a.ctr->error) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t lt = sa_lanemask_lt();
-    uint4* const s_hits = reinterpret_cast<uint4*>(sa_smem + 256) + wid * TILE;
+    uint4* const s_hits = reinterpret_cast<uint4*>(sa_smem + SA_LANE_TABLES) + wid * TILE;
     unsigned long long* const s_E =
-        reinterpret_cast<unsigned long long*>(sa_smem + 256 + 128 * (size_t)TILE) + wid * (TILE + 1);
-    unsigned char* const em_base = sa_smem + 256 + 128 * (size_t)TILE + 64 * (size_t)(TILE + 1);
+        reinterpret_cast<unsigned long long*>(sa_smem + SA_LANE_TABLES + 128 * (size_t)TILE) + wid * (TILE + 1);
+    unsigned char* const em_base = sa_smem + SA_LANE_TABLES + 128 * (size_t)TILE + 64 * (size_t)(TILE + 1);
     uint4* const s_em = reinterpret_cast<uint4*>(em_base) + wid * 64;
     uint2* const s_ex = reinterpret_cast<uint2*>(em_base + 8 * 64 * 16) + wid * 64;
 
-    const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
-    const uint32_t ref_len = a.ref_len, seed_size = a.seed_size;
-    const int xdrop = a.xdrop;
+    // H, nnz, ref_len, seed_size and xdrop are read where used (registers
+    // are the lane kernel's limit)
     const uint32_t* __restrict__ ref = a.ref;
 
     uint32_t tile_pos = 0, tile_n = 0;
-    bool exhausted = (H == 0);
+    bool exhausted = false;
     uint32_t em_head = 0, em_tail = 0;  // ring of kept HSPs (warp-uniform cursors)
 
     // prefetched next hit
@@ -310,6 +314,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 unsigned long long t0 = 0;
                 if (lane == 0) t0 = atomicAdd(&a.ctr->hit_cursor, (unsigned long long)TILE);
                 t0 = __shfl_sync(SA_FULL, t0, 0);
+                const uint64_t H = a.ctr->num_hits, nnz = a.ctr->nnz;
                 if (t0 >= H) {
                     exhausted = true;
                     tile_n = tile_pos = 0;
@@ -329,8 +334,8 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                         }
                         const uint64_t c = c0 + lo;
                         uint4 r;
-                        r.x = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - s_E[lo])) + seed_size;  // find_hits :192
-                        r.y = a.cs.qpos[c] + seed_size;                                                 // find_hits :176
+                        r.x = __ldg(a.pos_table + a.cs.lo[c] + (uint32_t)(h - s_E[lo])) + a.seed_size;  // find_hits :192
+                        r.y = a.cs.qpos[c] + a.seed_size;                                                 // find_hits :176
                         r.z = a.cs.scope[c];
                         r.w = a.cs.unit[c];
                         s_hits[i] = r;
@@ -367,7 +372,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
             // Coordinates past either sequence end (a caller-supplied table or
             // seed beyond the sequences) are rejected, not read.
-            if (rl > ref_len || ql > U.q_len) {
+            if (rl > a.ref_len || ql > U.q_len) {
                 atomicCAS(&a.ctr->error, 0ull, 5ull);
                 skip = true;
             }
@@ -388,6 +393,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             const SaUnit U = a.units[unit_id];
             const uint32_t* __restrict__ qp = U.q_packed;
             const uint32_t qlen = U.q_len;
+            const uint32_t ref_len = a.ref_len;
             const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
             avail = min(ref_len - sr, qlen - sq);
             sh_r = (sr & 7u) * 4u;
@@ -437,13 +443,13 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_exact<false>(tblb, lo, hi, 8 * j, o + 8 * j, avail, xdrop, S, best, pk, alive);
+                        sa_window_exact<false>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_exact<true>(tblb, lo, hi, 8 * j, o + 8 * j, avail, xdrop, S, best, pk, alive);
+                        sa_window_exact<true>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
                     }
                 }
                 if (best != best_in) bpos = (int)o + pk;
@@ -454,15 +460,15 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, xdrop, Pk, B, at, stop);
+                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < NW; ++j) {
                         sa_merge8(rwin[j], qwin[j], lo, hi);
                         // a base past the sequence end scores -(xdrop + 1)
-                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(xdrop + 1) * SCALE - 1, xdrop,
-                                                 Pk, B, at, stop);
+                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
+                                                 a.xdrop, Pk, B, at, stop);
                     }
                 }
                 const int low = at & (SCALE - 1);
@@ -472,7 +478,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 S = best_in + (Pk >> SH);  // exact after a full step without a stop
             }
             if (stop) {
-                // Steps start at multiples of STEP (8 or 16), so the stop offset
+                // Steps start at multiples of STEP (8, 16 or 32), so the stop offset
                 // lies in 32-base tile o >> 5 whichever base of the step it is.
                 tiles += (o >> 5) + 1;
                 if (dir == 0) {
@@ -762,14 +768,18 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
 }
 
 // The fast scoring form holds when 7 * max(0, max_sub) <= xdrop (see the
-// phase A notes); the magnitude limits keep its packed scores inside 31 bits.
-static bool sa_lane_fast_form(const SaParams& p) {
-    int mx = 0, mn = 0;
+// phase A notes) and its packed scores stay inside 31 bits: a step starts at
+// >= -xdrop * SCALE and adds STEP scores of >= min_sub * SCALE - 1 (or
+// -(xdrop + 1) * SCALE - 1 past a sequence end).
+static bool sa_lane_fast_form(const SaParams& p, int step) {
+    long long mx = 0, mn = 0;
     for (int i = 0; i < 64; ++i) {
-        mx = std::max(mx, p.sub_mat[i]);
-        mn = std::min(mn, p.sub_mat[i]);
+        mx = std::max<long long>(mx, p.sub_mat[i]);
+        mn = std::min<long long>(mn, p.sub_mat[i]);
     }
-    return p.xdrop >= 0 && p.xdrop <= (1 << 16) && 7ll * mx <= p.xdrop && mn >= -(1 << 20);
+    const long long scale = 2ll * step, x = p.xdrop;
+    const long long low = std::min(mn, -(x + 1)) * scale - 1;
+    return x >= 0 && 7 * mx <= x && x * scale - low * step < (1ll << 31) && mx * scale * step < (1ll << 31);
 }
 
 template <int C, int STEP, bool EXACT>
@@ -781,7 +791,10 @@ static void sa_lane_launch(const SaExtK& a, const SaParams& p, int grid, size_t 
 template <int C>
 static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, int grid, size_t smem,
                              cudaStream_t st) {
-    if (step == 16) {
+    if (step == 32) {
+        if (exact) sa_lane_launch<C, 32, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 32, false>(a, p, grid, smem, st);
+    } else if (step == 16) {
         if (exact) sa_lane_launch<C, 16, true>(a, p, grid, smem, st);
         else sa_lane_launch<C, 16, false>(a, p, grid, smem, st);
     } else {
@@ -796,7 +809,7 @@ void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, 
     const SaExtK a = sa_ext_args(w, x, t);
     const int grid = num_sms * t.ext_ctas_per_sm;
     const size_t smem = sa_lane_smem(a.tile_hits);
-    const bool exact = !sa_lane_fast_form(p);
+    const bool exact = !sa_lane_fast_form(p, t.step_bases);
     if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, grid, smem, st);
     else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, grid, smem, st);
     else sa_lane_dispatch<2>(a, p, t.step_bases, exact, grid, smem, st);

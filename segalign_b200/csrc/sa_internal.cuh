@@ -15,7 +15,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#define SA_PADW 8  // padding words on each side of a packed sequence
+#define SA_PADW 16  // padding words on each side of a packed sequence (>= the lane kernel's read-ahead)
 #define SA_NUC 8
 #define SA_WARP 32
 #define SA_INVALID_KEY 0xffffffffu

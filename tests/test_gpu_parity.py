@@ -69,7 +69,7 @@ def test_seeder_pipeline_matches_oracle(setup):
     assert len(fw) + len(rc) > 200
 
 
-@pytest.mark.parametrize("xdrop,step", [(300, 16), (699, 16), (700, 16), (699, 8), (700, 8)])
+@pytest.mark.parametrize("xdrop,step", [(300, 16), (699, 16), (700, 16), (699, 8), (700, 8), (699, 32), (700, 32)])
 def test_xdrop_scoring_forms(setup, xdrop, step):
     """With HOXD70 (largest score 100) an xdrop of at least 7 x 100 takes the
     lane kernel's windowed stop test, a smaller one its per-base test; both
@@ -88,7 +88,7 @@ def test_xdrop_scoring_forms(setup, xdrop, step):
             compare_segments(got, want, f"xdrop={xdrop} step={step} rev={rev}")
             assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(step_bases=16)
+        sf.set_tuning(step_bases=32)
         sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
 
 
@@ -110,7 +110,7 @@ def test_max_hits_iterations(setup, max_hits):
 
 @pytest.mark.parametrize("lane_cap,ctas,tile,step", [(8, 2, 64, 8), (16, 4, 1024, 16), (32, 4, 1024, 8),
                                                      (64, 3, 100, 16), (512, 3, 1024, 8), (4096, 3, 256, 16),
-                                                     (512, 2, 1024, 16)])
+                                                     (512, 2, 1024, 16), (32, 3, 160, 32), (4096, 2, 64, 32)])
 def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
     """Every tuning gives the same HSPs and extends every hit exactly once (tile counts)."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
@@ -121,7 +121,7 @@ def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
         compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas} step={step}")
         assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=16)
+        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=32)
 
 
 def test_host_table_upload(setup):
