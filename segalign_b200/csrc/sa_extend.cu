@@ -13,15 +13,15 @@
 // This file computes the same quantities in two phases:
 //   phase A (sa_k_extend_lane): one hit per lane.  A warp keeps its 32 lanes
 //     busy by handing out the next hits of its tile, in order, to lanes that
-//     finish ("refill").  Hits are expanded on the fly from the compacted seed
+//     finish.  Hits are expanded on the fly from the compacted seed
 //     list.  The short random-hit extensions that dominate the hit count
 //     finish here in a few steps.
 //   phase B (sa_k_extend_warp): hits whose extension passes `lane_cap` bases in
 //     one direction move to a queue and are redone by one warp per hit,
 //     256 bases per step.  Each lane scans 8 bases; warp scans carry the
 //     running sum and maximum.
-// Survivors are appended with warp-aggregated atomics, together with their
-// dedup scope.
+// Kept HSPs, with their dedup scope, go into the call's set of distinct HSPs
+// (SaHashSet), which the dedup stage compacts and sorts.
 #include <algorithm>
 #include <climits>
 
@@ -114,10 +114,9 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 //
 // A warp takes tiles of consecutive hits from a global counter and expands
 // each tile once into shared memory ({ref_loc, query_loc, scope, unit} per
-// hit).  Each lane owns a current hit and a prefetched next hit; a refill
-// round hands the next records of the tile, in order, to the lanes whose next
-// slot is empty, and a lane promotes its next hit the moment its current one
-// finishes.  Both directions of a hit run the same rightward scan: the left
+// hit).  At the top of every iteration the lanes without a hit take the next
+// records of the tile, in order, and start them in the same iteration.
+// Both directions of a hit run the same rightward scan: the left
 // extension from (rl, ql) is the right extension from (ref_len - rl,
 // qlen - ql) in the reversed copies that follow every packed sequence, so
 // lanes in different directions execute the same instructions.  A step
@@ -283,9 +282,6 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     bool exhausted = false;
     uint32_t em_head = 0, em_tail = 0;  // ring of kept HSPs (warp-uniform cursors)
 
-    // prefetched next hit
-    bool nx = false;
-    uint32_t n_rl = 0, n_ql = 0, n_scope = 0, n_unit = 0;
     // current hit
     bool has = false, nocap = false, setup = false;
     uint32_t rl = 0, ql = 0, scope = 0, unit_id = 0;
@@ -303,9 +299,10 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     uint32_t tiles = 0, tiles_acc = 0, ext_acc = 0;  // per-lane statistics (32-bit per lane)
 
     while (true) {
-        // ---- refill: next slots of the tile's hits, in order ----
-        const uint32_t need = __ballot_sync(SA_FULL, !nx);
-        if (need && !(exhausted && tile_pos >= tile_n)) {
+        // ---- idle lanes take the next hits of the warp tile, in order ----
+        const uint32_t idle = __ballot_sync(SA_FULL, !has);
+        bool fresh = false;
+        if (idle && !(exhausted && tile_pos >= tile_n)) {
             if (tile_pos >= tile_n) {
                 // Take the next tile of hits and expand it: the hits of the
                 // tile span at most TILE consecutive hit-bearing seeds from the
@@ -346,72 +343,68 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
             if (tile_pos < tile_n) {
-                const uint32_t m = min((uint32_t)__popc(need), tile_n - tile_pos);
-                const uint32_t rank = __popc(need & lt);
-                if (!nx && rank < m) {
+                const uint32_t m = min((uint32_t)__popc(idle), tile_n - tile_pos);
+                const uint32_t rank = __popc(idle & lt);
+                if (!has && rank < m) {
                     const uint4 r = s_hits[tile_pos + rank];
-                    n_rl = r.x;
-                    n_ql = r.y;
-                    n_scope = r.z;
-                    n_unit = r.w;
-                    nx = true;
+                    rl = r.x;
+                    ql = r.y;
+                    scope = r.z;
+                    unit_id = r.w;
+                    fresh = true;
                 }
                 tile_pos += m;
             }
         }
-        // ---- promote the next hit of idle lanes ----
-        if (!has && nx) {
-            nx = false;
-            rl = n_rl;
-            ql = n_ql;
-            scope = n_scope;
-            unit_id = n_unit;
-            const SaUnit U = a.units[unit_id];
-            // rm: hits outside [ref_start, ref_end] are never extended
-            // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
-            bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
-            // Coordinates past either sequence end (a caller-supplied table or
-            // seed beyond the sequences) are rejected, not read.
-            if (rl > a.ref_len || ql > U.q_len) {
-                atomicCAS(&a.ctr->error, 0ull, 5ull);
-                skip = true;
-            }
-            if (!skip) {
-                has = true;
-                nocap = false;
-                setup = true;
-                dir = 0;
-                tiles = 0;
-                ++ext_acc;
-            }
-        }
-        const bool done = !__any_sync(SA_FULL, has || nx) && exhausted && tile_pos >= tile_n;
 
-        // ---- start of a direction: new hit (right) or after its right end (left) ----
-        if (setup) {
-            setup = false;
+        // ---- start of a direction: a fresh hit (right), or the left side of
+        // the current hit after its right end ----
+        if (fresh || setup) {
             const SaUnit U = a.units[unit_id];
-            const uint32_t* __restrict__ qp = U.q_packed;
-            const uint32_t qlen = U.q_len;
-            const uint32_t ref_len = a.ref_len;
-            const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
-            avail = min(ref_len - sr, qlen - sq);
-            sh_r = (sr & 7u) * 4u;
-            sh_q = (sq & 7u) * 4u;
-            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
-            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
-#pragma unroll
-            for (int j = 0; j <= NW; ++j) {
-                w_r[j] = __ldg(pr + j);
-                w_q[j] = __ldg(pq + j);
+            if (fresh) {
+                // rm: hits outside [ref_start, ref_end] are never extended
+                // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
+                bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+                // Coordinates past either sequence end (a caller-supplied table or
+                // seed beyond the sequences) are rejected, not read.
+                if (rl > a.ref_len || ql > U.q_len) {
+                    atomicCAS(&a.ctr->error, 0ull, 5ull);
+                    skip = true;
+                }
+                if (!skip) {
+                    has = true;
+                    nocap = false;
+                    setup = true;
+                    dir = 0;
+                    tiles = 0;
+                    ++ext_acc;
+                }
             }
-            pr += NW + 1;
-            pq += NW + 1;
-            o = 0;
-            S = 0;
-            best = 0;
-            bpos = 0;
+            if (setup) {
+                setup = false;
+                const uint32_t* __restrict__ qp = U.q_packed;
+                const uint32_t qlen = U.q_len;
+                const uint32_t ref_len = a.ref_len;
+                const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
+                avail = min(ref_len - sr, qlen - sq);
+                sh_r = (sr & 7u) * 4u;
+                sh_q = (sq & 7u) * 4u;
+                pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
+                pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
+#pragma unroll
+                for (int j = 0; j <= NW; ++j) {
+                    w_r[j] = __ldg(pr + j);
+                    w_q[j] = __ldg(pq + j);
+                }
+                pr += NW + 1;
+                pq += NW + 1;
+                o = 0;
+                S = 0;
+                best = 0;
+                bpos = 0;
+            }
         }
+        const bool done = !__any_sync(SA_FULL, has) && exhausted && tile_pos >= tile_n;
 
         // ---- one STEP-base step per busy lane ----
         bool finished = false, to_long = false;
