@@ -303,6 +303,10 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
         *p.ptr = at;
         at += (p.bytes + 255) & ~255ull;
     }
+    // the HSP set's list of claimed slots lives in rec[1], free until the sort
+    w.hset.used = reinterpret_cast<unsigned long long*>(w.rec[1]);
+    w.hset.used_cap = surv_cap;
+    w.hash_clean = false;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMallocHost(&s->h_ctr, sizeof(SaCounters)) != cudaSuccess ||
         cudaMallocHost(&s->h_desc, sizeof(SaCallDesc)) != cudaSuccess ||
@@ -408,6 +412,7 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
     SaCounters c = *s->h_ctr;
+    sa_note_hash_state(w, c);
     std::memset(&t_stats, 0, sizeof t_stats);
     t_stats.num_seeds = n;
     t_stats.num_hits = c.num_hits;
@@ -567,6 +572,7 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
     SaCounters c = *s->h_ctr;
+    sa_note_hash_state(w, c);
     if (c.hash_overflow || c.error == 4) return SA_ERR_CAPACITY;
     if (c.error) return map_device_error(c.error);
     res.tot.num_hits += c.num_hits;

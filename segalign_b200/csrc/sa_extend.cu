@@ -229,11 +229,13 @@ __device__ __forceinline__ void sa_flush_candidates(const SaExtK& a, const uint4
     }
     const uint32_t km = __ballot_sync(SA_FULL, keep != 0);
     if (lane == 0 && km) atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(km));
+    unsigned long long claimed = ~0ull;
     if (keep) {
         uint32_t qs = r.y;
         if (U.flags & 2u) qs = a.ref_len - 1 - (qs + r.z);
-        sa_hash_insert(a.hset, a.ctr->hash_mask, r.w, r.x, qs, r.z, score, &a.ctr->hash_overflow);
+        claimed = sa_hash_insert(a.hset, a.ctr->hash_mask, r.w, r.x, qs, r.z, score, &a.ctr->hash_overflow);
     }
+    sa_hash_note_used(a.hset, &a.ctr->hash_used, claimed);
 }
 
 // Dynamic shared memory of the lane kernel for `tile` hits per warp tile.
@@ -733,7 +735,12 @@ sa_k_extend_warp(SaExtK a, SaParams P) {
                 uint32_t qs = ql - (uint32_t)Lr.pos;
                 const uint32_t len = (uint32_t)ext;
                 if (U.flags & 2u) qs = a.ref_len - 1 - (qs + len);
-                sa_hash_insert(a.hset, a.ctr->hash_mask, L.scope, rs, qs, len, score, &a.ctr->hash_overflow);
+                const unsigned long long cl =
+                    sa_hash_insert(a.hset, a.ctr->hash_mask, L.scope, rs, qs, len, score, &a.ctr->hash_overflow);
+                if (cl != ~0ull) {
+                    const unsigned long long i = atomicAdd(&a.ctr->hash_used, 1ull);
+                    if (i < a.hset.used_cap) a.hset.used[i] = cl;
+                }
             }
         }
     }

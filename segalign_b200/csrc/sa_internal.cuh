@@ -96,6 +96,7 @@ struct SaCounters {
     unsigned long long error;          // nonzero = device-side error code
     unsigned long long hash_mask;      // slots - 1 of this call's HSP hash set
     unsigned long long hash_overflow;  // inserts that found no free slot
+    unsigned long long hash_used;      // slots claimed in the HSP set (entries of its used list)
     unsigned long long pad[3];         // device-side counts of the dedup stages
 };
 
@@ -104,9 +105,14 @@ struct SaCounters {
 // 128-bit compare-and-swap (all ones = empty), plus the score.  Within one
 // scope the score is a function of the key (sum of substitution scores over
 // the segment, entropy of its base counts), so equal keys are equal records.
+// Every claimed slot is also appended to `used`; the compaction reads the
+// distinct HSPs from that list and empties those slots again, so the set is
+// left empty for the next call without clearing the whole table.
 struct SaHashSet {
     unsigned long long* keys;  // [2 * slots]
     int32_t* score;            // [slots]
+    unsigned long long* used;  // [used_cap] claimed slots, in claim order
+    unsigned long long used_cap;
 };
 
 #define SA_HASH_MAX_PROBES 4096
@@ -133,11 +139,12 @@ __device__ __forceinline__ unsigned long long sa_hash_mix(unsigned long long a, 
     return x;
 }
 
-// Inserts one HSP; returns true when it was new.  Sets *overflow when no slot
-// was found within SA_HASH_MAX_PROBES (the set is too small).
-__device__ __forceinline__ bool sa_hash_insert(const SaHashSet& hs, unsigned long long mask, uint32_t scope,
-                                               uint32_t rs, uint32_t qs, uint32_t len, int32_t score,
-                                               unsigned long long* overflow) {
+// Inserts one HSP; returns the slot it claimed when it was new, else ~0.
+// Counts an overflow when no slot was found within SA_HASH_MAX_PROBES (the
+// set is too small).  The caller records claimed slots (sa_hash_note_used).
+__device__ __forceinline__ unsigned long long sa_hash_insert(const SaHashSet& hs, unsigned long long mask,
+                                                             uint32_t scope, uint32_t rs, uint32_t qs, uint32_t len,
+                                                             int32_t score, unsigned long long* overflow) {
     const unsigned long long k0 = ((unsigned long long)scope << 32) | rs;
     const unsigned long long k1 = ((unsigned long long)qs << 32) | len;
     unsigned long long h = sa_hash_mix(k0, k1) & mask;
@@ -146,13 +153,32 @@ __device__ __forceinline__ bool sa_hash_insert(const SaHashSet& hs, unsigned lon
         sa_cas128(hs.keys + 2 * h, ~0ull, ~0ull, k0, k1, o0, o1);
         if (o0 == ~0ull && o1 == ~0ull) {
             hs.score[h] = score;
-            return true;
+            return h;
         }
-        if (o0 == k0 && o1 == k1) return false;
+        if (o0 == k0 && o1 == k1) return ~0ull;
         h = (h + 1) & mask;
     }
     atomicAdd(overflow, 1ull);
-    return false;
+    return ~0ull;
+}
+
+__device__ __forceinline__ uint32_t sa_lanemask_lt();
+
+// Appends the slots claimed by the lanes of a warp (slot != ~0) to the set's
+// used list; called by all 32 lanes together.
+__device__ __forceinline__ void sa_hash_note_used(const SaHashSet& hs, unsigned long long* hash_used,
+                                                  unsigned long long slot) {
+    const bool c = slot != ~0ull;
+    const uint32_t m = __ballot_sync(0xffffffffu, c);
+    if (!m) return;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(hash_used, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (c) {
+        const unsigned long long i = base + __popc(m & sa_lanemask_lt());
+        if (i < hs.used_cap) hs.used[i] = slot;
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -72,7 +72,8 @@ struct SaWork {
     uint32_t* scope[2];
     uint32_t* flags;        // [surv_cap]
     uint64_t surv_cap;
-    SaHashSet hset;         // [2 * surv_cap] slots: distinct HSPs of the call
+    SaHashSet hset;         // [2 * surv_cap] slots: distinct HSPs of the call; used list aliases rec[1]
+    bool hash_clean;        // host: every slot of hset is empty (no full clear needed)
     SaRec* out;             // [surv_cap] deduplicated records (device)
     uint32_t* out_scope;
     uint32_t* scope_count;  // [SA_MAX_SCOPES]
@@ -150,6 +151,8 @@ void sa_launch_extend_warp(SaWork& w, const SaExtendArgs& a, const SaParams& p, 
 // ---- sa_sort.cu ----
 // Sizes the call's HSP set from its hit count (<= 2 * surv_cap slots) and empties it.
 void sa_launch_hash_init(SaWork& w, cudaStream_t st);
+// After the host has read a call's counters: whether the HSP set was left empty.
+void sa_note_hash_state(SaWork& w, const SaCounters& c);
 // mode 0 = plain dedup; 1 = rm (adds diagonal sort/unique and final sort).
 // scope_shift: records are counted per (scope >> scope_shift) and flags are
 // looked up the same way (0 for single calls, 4 for batches: scope = unit<<4 | iteration).

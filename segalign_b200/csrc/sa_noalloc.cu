@@ -69,6 +69,7 @@ namespace {
 std::mutex g_noalloc_mu;
 constexpr int kMaxDevices = 64;
 void* g_scratch_ptr[kMaxDevices] = {};
+bool g_hash_clean[kMaxDevices] = {};  // the array's HSP set is known to be empty
 
 // Per-device set-up, with `dev` current: the device address of the array.
 int scratch_address(int dev, void** ptr) {
@@ -124,6 +125,9 @@ void carve(void* base, SaWork& w) {
     w.seed_cap = kSeeds;
     w.surv_cap = kSurv;
     w.long_cap = SA_NOALLOC_LONG_CAP;
+    // the HSP set's list of claimed slots lives in rec[1], free until the sort
+    w.hset.used = reinterpret_cast<unsigned long long*>(w.rec[1]);
+    w.hset.used_cap = kSurv;
 }
 
 }  // namespace
@@ -159,6 +163,8 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     if (r != SA_OK) return r;
     SaWork w;
     carve(base, w);
+    w.hash_clean = g_hash_clean[v.dev];
+    g_hash_clean[v.dev] = false;  // set again once this call is seen to complete
     cudaStream_t st = cudaStreamPerThread;
     SaCallDesc desc{};
     desc.num_seeds = num_seeds;
@@ -193,6 +199,8 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     SaCounters c;
     SA_CUDA_OK(cudaMemcpyAsync(&c, w.ctr, sizeof c, cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaStreamSynchronize(st));
+    sa_note_hash_state(w, c);
+    g_hash_clean[v.dev] = w.hash_clean;
     if (c.hash_overflow || c.error == 4) {
         sa_set_error(SA_ERR_CAPACITY, "more than %u distinct HSPs (no-allocation limit)", SA_NOALLOC_MAX_SURVIVORS);
         return SA_ERR_CAPACITY;

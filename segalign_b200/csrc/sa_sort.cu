@@ -211,52 +211,42 @@ sa_k_uniq_emit(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, 
 __global__ void sa_k_flip_cur(int* st, int np) { st[0] = st[1 + np] ^ 1; }
 
 // Sizes the call's HSP set: the smallest power of two >= 2 * hits (at least
-// 1024), at most `max_slots` (a power of two), and marks every slot empty.
-__global__ void sa_k_hash_init(SaHashSet hs, SaCounters* ctr, unsigned long long max_slots) {
+// 1024), at most `max_slots` (a power of two, the whole table).  With `full`
+// every slot of the table is marked empty; otherwise the table is known to be
+// empty already (the previous call's compaction emptied the slots it used).
+__global__ void sa_k_hash_init(SaHashSet hs, SaCounters* ctr, unsigned long long max_slots, int full) {
     unsigned long long want = 2 * ctr->num_hits;
     if (want < 1024) want = 1024;
     unsigned long long slots = 1;
     while (slots < want && slots < max_slots) slots <<= 1;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctr->hash_mask = slots - 1;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < 2 * slots;
+    if (!full) return;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < 2 * max_slots;
          i += (unsigned long long)gridDim.x * blockDim.x)
         hs.keys[i] = ~0ull;
 }
 
-// Distinct HSPs out of the set into rec/scope (any order: the sort that
-// follows is total).  More distinct HSPs than `cap` is a capacity error.
+// Distinct HSPs out of the set into rec/scope, in claim order (the sort that
+// follows is total), emptying their slots.  *n_out = slots claimed; more than
+// `cap` is a capacity error (sa_k_dedup_prep).
 __global__ void __launch_bounds__(256)
 sa_k_hash_compact(SaHashSet hs, SaCounters* ctr, SaRec* rec, uint32_t* scope, uint64_t cap, unsigned long long* n_out) {
-    const unsigned long long slots = ctr->hash_mask + 1;
-    const int lane = threadIdx.x & 31;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < slots; base += stride) {
-        const unsigned long long s = base + threadIdx.x;
-        unsigned long long k0 = ~0ull, k1 = ~0ull;
-        if (s < slots) {
-            k0 = hs.keys[2 * s];
-            k1 = hs.keys[2 * s + 1];
-        }
-        const bool occ = k0 != ~0ull;
-        const uint32_t m = __ballot_sync(0xffffffffu, occ);
-        if (!m) continue;
-        unsigned long long at = 0;
-        if (lane == __ffs(m) - 1) at = atomicAdd(n_out, (unsigned long long)__popc(m));
-        at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
-        if (occ) {
-            const unsigned long long i = at + __popc(m & sa_lanemask_lt());
-            if (i < cap) {
-                SaRec r;
-                r.ref_start = (uint32_t)k0;
-                r.query_start = (uint32_t)(k1 >> 32);
-                r.len = (uint32_t)k1;
-                r.score = hs.score[s];
-                rec[i] = r;
-                scope[i] = (uint32_t)(k0 >> 32);
-            } else {
-                atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_SURV_OVERFLOW);
-            }
-        }
+    const unsigned long long used = ctr->hash_used;
+    unsigned long long n = used < hs.used_cap ? used : hs.used_cap;
+    if (n > cap) n = cap;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = used;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long h = hs.used[i];
+        const ulonglong2 k = *reinterpret_cast<const ulonglong2*>(hs.keys + 2 * h);
+        SaRec r;
+        r.ref_start = (uint32_t)k.x;
+        r.query_start = (uint32_t)(k.y >> 32);
+        r.len = (uint32_t)k.y;
+        r.score = hs.score[h];
+        rec[i] = r;
+        scope[i] = (uint32_t)(k.x >> 32);
+        *reinterpret_cast<ulonglong2*>(hs.keys + 2 * h) = make_ulonglong2(~0ull, ~0ull);
     }
 }
 
@@ -269,8 +259,13 @@ __global__ void sa_k_dedup_prep(SaCounters* ctr, uint64_t cap, unsigned long lon
 void sa_launch_hash_init(SaWork& w, cudaStream_t st) {
     unsigned long long max_slots = 1;
     while (max_slots * 2 <= 2 * w.surv_cap) max_slots <<= 1;
-    sa_k_hash_init<<<148 * 8, 256, 0, st>>>(w.hset, w.ctr, max_slots);
+    sa_k_hash_init<<<148 * 8, 256, 0, st>>>(w.hset, w.ctr, max_slots, w.hash_clean ? 0 : 1);
     sa_note_launch();
+    w.hash_clean = false;  // until the host has seen this call complete
+}
+
+void sa_note_hash_state(SaWork& w, const SaCounters& c) {
+    w.hash_clean = c.error == 0 && c.hash_used <= w.hset.used_cap && c.hash_used <= w.surv_cap;
 }
 
 __global__ void sa_k_copy_u64(unsigned long long* dst, const unsigned long long* src) { *dst = *src; }

@@ -186,3 +186,42 @@ def test_repeat_masker_self_alignment(built, exclude):
             compare_segments(got, want, f"rm rev={rev} exclude={exclude}")
     finally:
         sf.set_rm_exclude_diagonal(False)
+
+
+def test_hsp_set_reused_after_overflow(setup):
+    """The HSP set is emptied by each call's compaction and cleared in full
+    only after a call that left it dirty: a call with more distinct HSPs than
+    the workspace holds fails with SA_ERR_CAPACITY, and the next call on the
+    same workspace still matches the oracle."""
+    import os
+    from segalign_b200 import SegAlignError
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    seeds = host_seeds(w.query, 0, CHUNK)
+    want_big, _ = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    cap = 16
+    assert len(want_big) - 1 > cap
+    small = seeds[:4000]
+    want_small, _ = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], small, False)
+    assert 0 < len(want_small) - 1 <= cap
+    saved = {k: os.environ.get(k) for k in ("SA_SURV_CAP", "SA_SLOTS_PER_GPU")}
+    os.environ["SA_SURV_CAP"] = str(cap)
+    os.environ["SA_SLOTS_PER_GPU"] = "1"
+    try:
+        sf.generate_shape_pos("12of19")
+        sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
+        sf.send_ref_write_request(w.target)
+        sf.generate_seed_pos_table(None, 1, 19, 12)
+        sf.send_query_write_request(w.query, 0)
+        compare_segments(sf.seed_and_filter(small, False, 0), want_small, "before overflow")
+        with pytest.raises(SegAlignError) as ei:
+            sf.seed_and_filter(seeds, False, 0)
+        assert ei.value.code == -8  # SA_ERR_CAPACITY
+        for _ in range(2):
+            compare_segments(sf.seed_and_filter(small, False, 0), want_small, "after overflow")
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+        sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
