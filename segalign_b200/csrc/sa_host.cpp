@@ -23,27 +23,82 @@ struct HostShape {
     int kmer_size = 12;
     int pos[32] = {0, 1, 2, 4, 7, 8, 11, 13, 15, 16, 17, 18};
     int transition = 0;
+    // Key extraction from a rolling window of 2-bit codes (newest base in the
+    // low bits): key = OR over b of part[b][byte b of the window].
+    uint32_t part[8][256];
+    int nbytes = 5;
 };
 HostShape g_shape;
 
-inline int nt_valid(char ch, uint32_t* v) {
-    switch (ch) {
-        case 'A': *v = 0; return 1;
-        case 'C': *v = 1; return 1;
-        case 'G': *v = 2; return 1;
-        case 'T': *v = 3; return 1;
-        default: return 0;  // lowercase, N, '&', IUPAC: invalid (common/ntcoding.cpp:10-19)
+// Code of each character: 0..3 for A, C, G, T; 4 for every other character
+// (lowercase, N, '&', IUPAC: invalid in a seed, common/ntcoding.cpp:10-19).
+struct CodeTable {
+    uint8_t c[256];
+    CodeTable() {
+        std::memset(c, 4, sizeof c);
+        c[(uint8_t)'A'] = 0;
+        c[(uint8_t)'C'] = 1;
+        c[(uint8_t)'G'] = 2;
+        c[(uint8_t)'T'] = 3;
     }
+};
+const CodeTable g_codes;
+
+// Key of the window whose first base is at window offset 0: shape position
+// p_i (i = 0..K-1, the first one most significant, common/ntcoding.cpp:43-61)
+// lies 2 * (S - 1 - p_i) bits up the window; byte b of the window contributes
+// the key bits of the shape positions it holds.
+void build_parts(HostShape& h) {
+    const int S = h.seed_size, K = h.kmer_size;
+    h.nbytes = (2 * S + 7) / 8;
+    for (int b = 0; b < 8; ++b)
+        for (int v = 0; v < 256; ++v) {
+            uint32_t key = 0;
+            for (int i = 0; i < K; ++i) {
+                const int bit = 2 * (S - 1 - h.pos[i]);  // position of the base's code in the window
+                if (bit / 8 != b) continue;
+                const uint32_t code = (uint32_t)(v >> (bit % 8)) & 3u;
+                key |= code << (2 * (K - 1 - i));
+            }
+            h.part[b][v] = key;
+        }
 }
 
-// common/ntcoding.cpp:43-61
-inline uint32_t kmer_at(const char* s, uint64_t p) {
-    uint32_t nt[32];
-    for (int i = 0; i < g_shape.seed_size; ++i)
-        if (!nt_valid(s[p + i], &nt[i])) return 1u << 31;
-    uint32_t k = 0;
-    for (int i = 0; i < g_shape.kmer_size; ++i) k = (k << 2) + nt[g_shape.pos[i]];
-    return k;
+struct PartsInit {
+    PartsInit() { build_parts(g_shape); }
+} g_parts_init;
+
+// Seed words of positions [j0, j1): the first `cap` go to out (out may be
+// NULL with cap 0); returns the count.  One pass: rolling window of 2-bit
+// codes and the position of the last invalid base.
+uint64_t chunk_seeds(const HostShape& h, const char* text, uint32_t j0, uint32_t j1, uint64_t* out, uint64_t cap) {
+    const int S = h.seed_size, K = h.kmer_size;
+    const uint64_t wmask = (S >= 32) ? ~0ull : ((1ull << (2 * S)) - 1);
+    uint64_t w = 0, n = 0;
+    int64_t last_bad = (int64_t)j0 - 1;
+    // prime the window with bases j0 .. j0+S-2
+    for (int i = 0; i + 1 < S; ++i) {
+        const uint32_t c = g_codes.c[(uint8_t)text[j0 + i]];
+        if (c > 3) last_bad = (int64_t)j0 + i;
+        w = ((w << 2) | (c & 3u)) & wmask;
+    }
+    for (uint32_t j = j0; j < j1; ++j) {
+        const uint64_t p = (uint64_t)j + (uint64_t)(S - 1);  // newest base of window j
+        const uint32_t c = g_codes.c[(uint8_t)text[p]];
+        if (c > 3) last_bad = (int64_t)p;
+        w = ((w << 2) | (c & 3u)) & wmask;
+        if (last_bad >= (int64_t)j) continue;  // window has a non-ACGT base
+        uint32_t key = 0;
+        for (int b = 0; b < h.nbytes; ++b) key |= h.part[b][(w >> (8 * b)) & 0xff];
+        if (n < cap) out[n] = ((uint64_t)key << 32) + j;
+        ++n;
+        if (h.transition)
+            for (int t = 0; t < K; ++t) {
+                if (n < cap) out[n] = ((uint64_t)(key ^ (2u << (2 * t))) << 32) + j;
+                ++n;
+            }
+    }
+    return n;
 }
 
 }  // namespace
@@ -58,32 +113,28 @@ int sa_host_set_shape(const char* shape, int transition) {
         pat = name;
         for (auto& c : pat) c = (c == '1' || c == 'T') ? 'T' : '0';
     }
+    HostShape h;
     int k = 0;
     for (size_t i = 0; i < pat.size() && k < 32; ++i)
-        if (pat[i] == 'T') g_shape.pos[k++] = (int)i;
+        if (pat[i] == 'T') h.pos[k++] = (int)i;
     if (k > 15 || k <= 3 || pat.size() > 32) return SA_ERR_ARG;
-    g_shape.kmer_size = k;
-    g_shape.seed_size = (int)pat.size();
-    g_shape.transition = transition ? 1 : 0;
+    h.kmer_size = k;
+    h.seed_size = (int)pat.size();
+    h.transition = transition ? 1 : 0;
+    if (h.seed_size != g_shape.seed_size || h.kmer_size != g_shape.kmer_size || h.transition != g_shape.transition ||
+        !std::equal(h.pos, h.pos + k, g_shape.pos)) {
+        build_parts(h);
+        g_shape = h;
+    }
     return k;
 }
 
 // src/seeder.cpp:57-74: for j in [j0, j1): word (key << 32) + j, followed by
 // the transition variants key ^ (2 << 2t), t = 0..K-1, when transitions are on.
+// With out == NULL (or cap too small) only the count is returned.
 uint64_t sa_host_chunk_seeds(const char* text, uint32_t j0, uint32_t j1, uint64_t* out, uint64_t cap) {
-    uint64_t n = 0;
-    for (uint32_t j = j0; j < j1; ++j) {
-        uint32_t k = kmer_at(text, j);
-        if (k == (1u << 31)) continue;
-        if (n < cap) out[n] = ((uint64_t)k << 32) + j;
-        ++n;
-        if (g_shape.transition)
-            for (int t = 0; t < g_shape.kmer_size; ++t) {
-                if (n < cap) out[n] = ((uint64_t)(k ^ (2u << (2 * t))) << 32) + j;
-                ++n;
-            }
-    }
-    return n;
+    if (j1 <= j0) return 0;
+    return chunk_seeds(g_shape, text, j0, j1, out, out ? cap : 0);
 }
 
 // common/ntcoding.cpp:63-105; characters other than ACGTacgtnN& are skipped.
@@ -202,10 +253,10 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
             if (c >= calls.size()) break;
             const Call& cl = calls[c];
             const char* txt = cl.strand ? rctext.data() : query;
-            uint64_t need = sa_host_chunk_seeds(txt, cl.j0, cl.j1, nullptr, 0);
+            const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
+            seeds.resize((uint64_t)(cl.j1 - cl.j0) * per);
+            const uint64_t need = chunk_seeds(g_shape, txt, cl.j0, cl.j1, seeds.data(), seeds.size());
             if (need == 0) continue;  // src/seeder.cpp:190
-            seeds.resize(need);
-            sa_host_chunk_seeds(txt, cl.j0, cl.j1, seeds.data(), need);
             sa_segment* out = nullptr;
             uint64_t ol = 0;
             int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, cfg->buffer, &out, &ol);
