@@ -29,6 +29,10 @@ static std::atomic<unsigned long long> g_launches{0};
 static std::atomic<int> g_timing{0};
 
 void sa_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// Generation of everything a captured call graph bakes in (tuning, timing,
+// parameters, resident target and table); bumped by every change of them.
+static std::atomic<uint64_t> g_graph_gen{1};
+static void invalidate_graphs() { g_graph_gen.fetch_add(1); }
 
 void sa_set_error(int, const char* fmt, ...) {
     char buf[512];
@@ -98,6 +102,11 @@ struct Slot {
     SaRec* h_out = nullptr;
     uint64_t h_out_cap = 0;
     cudaEvent_t ev[6] = {};
+    // CUDA graph of the per-call device chain (run_chain), valid for graph_key
+    cudaGraphExec_t graph = nullptr;
+    uint64_t graph_key = 0;
+    uint64_t graph_kernels = 0;
+    bool graph_off = false;  // capture failed once: launch directly
 };
 
 // Phase timing with CUDA events on the slot stream (enabled by sa_set_timing).
@@ -225,6 +234,7 @@ int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed*
 void free_slot(Slot* s) {
     if (!s) return;
     cudaSetDevice(s->dev_idx >= 0 ? G().devs[s->dev_idx].dev : 0);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
     if (s->arena) cudaFree(s->arena);
     if (s->stream) cudaStreamDestroy(s->stream);
     if (s->h_ctr) cudaFreeHost(s->h_ctr);
@@ -361,6 +371,86 @@ uint64_t max_hits_now() {
 
 // One SeedAndFilter call on a slot: seeds -> hits -> X-drop -> dedup -> host.
 // mode 0 = plain, 1 = repeat masker.
+// Device work of one plain (mode 0) or rm (mode 1) call once its seed words
+// are on the device: descriptor uploads from the slot's pinned buffers,
+// counters reset, lookup, extension, dedup and the counters' copy back.
+// Every size is read on the device, so one capture serves every call.
+int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
+    Global& g = G();
+    DevState& d = g.devs[s->dev_idx];
+    SaWork& w = s->w;
+    cudaStream_t st = s->stream;
+    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
+    SA_CUDA_OK(cudaMemcpyAsync(w.desc, s->h_desc, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.units, s->h_units, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
+    SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
+    sa_launch_lookup_seeds(w, d.index, (uint32_t)d.nbuckets, g.params, Gr, st);
+    sa_launch_hash_init(w, false, st);
+    tm.mark(1);
+    SaExtendArgs xa;
+    xa.ref = d.ref.data;
+    xa.ref_len = (uint32_t)d.ref.len;
+    xa.pos_table = d.pos;
+    xa.seed_size = (uint32_t)g.params.seed_size;
+    xa.xdrop = g.params.xdrop;
+    xa.hspthresh = g.params.hspthresh;
+    xa.noentropy = g.params.noentropy;
+    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(2);
+    sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
+    tm.mark(3);
+    sa_launch_dedup(w, mode, 0, Gr, st);
+    tm.mark(4);
+    SA_CUDA_OK(cudaGetLastError());
+    SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
+    return SA_OK;
+}
+
+bool graphs_enabled() {
+    static const bool on = env_u64("SA_GRAPHS", 1) != 0;
+    return on;
+}
+
+// Runs the call chain: replays the slot's CUDA graph, capturing it first when
+// the chain changed (mode, or anything invalidate_graphs covers).
+int run_chain(Slot* s, int mode, PhaseTimer& tm) {
+    // phase timing (a diagnostic mode) records events between the kernels: direct launches
+    if (!graphs_enabled() || s->graph_off || tm.on) return launch_call_chain(s, mode, tm);
+    Global& g = G();
+    cudaStream_t st = s->stream;
+    const uint64_t key = (g_graph_gen.load() << 1) | (uint64_t)mode;
+    if (!s->graph || s->graph_key != key) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        sa_prepare_extend_lane(g.params, g.tuning);  // kernel attributes are not set during capture
+        const unsigned long long l0 = g_launches.load();
+        SA_CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int r = launch_call_chain(s, mode, tm);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        const unsigned long long captured = g_launches.load() - l0;
+        g_launches.fetch_sub(captured);  // counted again at each replay
+        cudaError_t ei = cudaErrorUnknown;
+        if (r == SA_OK && e == cudaSuccess && graph) ei = cudaGraphInstantiate(&s->graph, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            // capture not possible here: direct launches from now on
+            s->graph = nullptr;
+            s->graph_off = true;
+            cudaGetLastError();
+            return launch_call_chain(s, mode, tm);
+        }
+        s->graph_key = key;
+        s->graph_kernels = captured;
+    }
+    SA_CUDA_OK(cudaGraphLaunch(s->graph, st));
+    g_launches.fetch_add(s->graph_kernels);
+    return SA_OK;
+}
+
+// One SeedAndFilter call on a slot: seeds -> hits -> X-drop -> dedup -> host.
+// mode 0 = plain, 1 = repeat masker.
 int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& q, int mode, uint32_t rm_lo,
              uint32_t rm_hi, sa_segment** out, uint64_t* out_len) {
     Global& g = G();
@@ -368,7 +458,6 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     SaWork& w = s->w;
     cudaStream_t st = s->stream;
     SA_CUDA_OK(cudaSetDevice(d.dev));
-    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
     // descriptor, unit, scope flags
     SaCallDesc* hd = s->h_desc;
     hd->num_seeds = n;
@@ -387,29 +476,9 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     PhaseTimer tm(s);
     tm.mark(0);
     SA_CUDA_OK(cudaMemcpyAsync(w.seeds, seeds, 8ull * n, cudaMemcpyHostToDevice, st));
-    SA_CUDA_OK(cudaMemcpyAsync(w.desc, hd, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
-    SA_CUDA_OK(cudaMemcpyAsync(w.units, u, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
-    SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
-    SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
-    sa_launch_lookup_seeds(w, d.index, (uint32_t)d.nbuckets, g.params, Gr, st);
-    sa_launch_hash_init(w, st);
-    tm.mark(1);
-    SaExtendArgs xa;
-    xa.ref = d.ref.data;
-    xa.ref_len = (uint32_t)d.ref.len;
-    xa.pos_table = d.pos;
-    xa.seed_size = (uint32_t)g.params.seed_size;
-    xa.xdrop = g.params.xdrop;
-    xa.hspthresh = g.params.hspthresh;
-    xa.noentropy = g.params.noentropy;
-    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st);
-    tm.mark(2);
-    sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
-    tm.mark(3);
-    sa_launch_dedup(w, mode, 0, Gr, st);
-    tm.mark(4);
-    SA_CUDA_OK(cudaGetLastError());
-    SA_CUDA_OK(cudaMemcpyAsync(s->h_ctr, w.ctr, sizeof(SaCounters), cudaMemcpyDeviceToHost, st));
+    if (!w.hash_clean) sa_launch_hash_clear(w, st);
+    w.hash_clean = false;  // until this call is seen to complete
+    SA_TRY(run_chain(s, mode, tm));
     SA_CUDA_OK(cudaStreamSynchronize(st));
     SaCounters c = *s->h_ctr;
     sa_note_hash_state(w, c);
@@ -552,7 +621,9 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     SA_CUDA_OK(cudaMemsetAsync(w.scope_flags, 0, 4 * n, st));
     SA_CUDA_OK(cudaMemsetAsync(w.ctr, 0, sizeof(SaCounters), st));
     sa_launch_lookup_batch(w, d.index, (uint32_t)d.nbuckets, n, g.params, Gr, st);
-    sa_launch_hash_init(w, st);
+    if (!w.hash_clean) sa_launch_hash_clear(w, st);
+    w.hash_clean = false;  // until this group is seen to complete
+    sa_launch_hash_init(w, false, st);
     tm.mark(1);
     SaExtendArgs xa;
     xa.ref = d.ref.data;
@@ -746,6 +817,7 @@ int sa_generate_shape_pos(const char* shape) {
 
 // common/seed_filter_interface.cu:82-101
 int sa_send_ref_write_request(const char* seq, size_t start_addr, uint32_t len) {
+    invalidate_graphs();
     Global& g = G();
     if (!g.interface_ready) {
         sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
@@ -762,6 +834,7 @@ int sa_send_ref_write_request(const char* seq, size_t start_addr, uint32_t len) 
 
 // common/seed_filter_interface.cu:103-113
 int sa_clear_ref(void) {
+    invalidate_graphs();
     Global& g = G();
     for (auto& d : g.devs) {
         cudaSetDevice(d.dev);
@@ -845,6 +918,7 @@ static int build_table_on(DevState& d, const Packed& ref, uint32_t step) {
 // common/seed_pos_table.cu:49-109
 int sa_generate_seed_pos_table(const char* ref_str, size_t start_addr, uint32_t ref_length, uint32_t step,
                                int shape_size, int kmer_size) {
+    invalidate_graphs();
     Global& g = G();
     if (!g.interface_ready) {
         sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
@@ -875,6 +949,7 @@ int sa_generate_seed_pos_table(const char* ref_str, size_t start_addr, uint32_t 
 // common/seed_pos_table.cu:33-47
 int sa_send_seed_pos_table(const uint32_t* index_table, uint32_t index_table_size, const uint32_t* pos_table,
                            uint32_t num_index) {
+    invalidate_graphs();
     Global& g = G();
     if (!g.interface_ready) return SA_ERR_STATE;
     if (!index_table || (num_index && !pos_table)) return SA_ERR_ARG;
@@ -921,6 +996,7 @@ int sa_get_seed_pos_table(uint32_t* index_table, uint64_t index_cap, uint32_t* p
 // src/seed_filter.cu:780-847
 int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_size, const int* sub_mat, int xdrop,
                             int hspthresh, int noentropy) {
+    invalidate_graphs();
     Global& g = G();
     if (!g.interface_ready) {
         sa_set_error(SA_ERR_STATE, "sa_initialize_interface() has not been called");
@@ -1031,6 +1107,7 @@ int sa_clear_query(uint32_t buffer) {
 
 // repeat_masker_src/seed_filter.cu:925-935
 int sa_rm_send_query_write_request(void) {
+    invalidate_graphs();
     Global& g = G();
     for (auto& d : g.devs) {
         if (!d.ref.data) {
@@ -1183,6 +1260,7 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
 void sa_free_segments(sa_segment* p) { free(p); }
 
 int sa_set_timing(int on) {
+    invalidate_graphs();
     g_timing = on ? 1 : 0;
     return SA_OK;
 }
@@ -1243,16 +1321,19 @@ int sa_resident_view(uint32_t buffer, SaResidentView* v) {
 extern "C" {
 
 int sa_set_max_hits(uint64_t max_hits) {
+    invalidate_graphs();
     G().max_hits_override = max_hits;
     return SA_OK;
 }
 
 int sa_set_rm_exclude_diagonal(int on) {
+    invalidate_graphs();
     G().rm_exclude_diag = on ? 1 : 0;
     return SA_OK;
 }
 
 int sa_set_tuning_param(const char* name, int value) {
+    invalidate_graphs();
     if (!name) return SA_ERR_ARG;
     SaTuning& t = G().tuning;
     const std::string n = name;
@@ -1294,6 +1375,7 @@ int sa_get_tuning_param(const char* name) {
 }
 
 int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits) {
+    invalidate_graphs();
     SaTuning& t = G().tuning;
     if (lane_cap >= 0 && (lane_cap % 8 || lane_cap < 8)) {
         sa_set_error(SA_ERR_ARG, "lane_cap must be a positive multiple of 8 (got %d)", lane_cap);

@@ -24,6 +24,7 @@
 // (SaHashSet), which the dedup stage compacts and sorts.
 #include <algorithm>
 #include <climits>
+#include <mutex>
 
 #include "sa_launch.h"
 #include "sa_radix.cuh"
@@ -784,8 +785,8 @@ static bool sa_lane_fast_form(const SaParams& p, int step) {
 
 template <int C, int STEP, bool EXACT>
 static void sa_lane_launch(const SaExtK& a, const SaParams& p, int grid, size_t smem, cudaStream_t st) {
-    cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    sa_k_extend_lane<C, STEP, EXACT><<<grid, 256, smem, st>>>(a, p);
+    if (grid > 0) sa_k_extend_lane<C, STEP, EXACT><<<grid, 256, smem, st>>>(a, p);
+    else cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 template <int C>
@@ -803,8 +804,30 @@ static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool 
     }
 }
 
+// Allows every lane-kernel instance the largest tile's shared memory, once
+// per device (kernel attributes cannot be set while a stream is captured).
+void sa_prepare_extend_lane(const SaParams& p, const SaTuning& t) {
+    (void)t;
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    const size_t smem = sa_lane_smem(1024);
+    SaExtK none{};
+    for (int step : {8, 16, 32})
+        for (bool exact : {false, true}) {
+            sa_lane_dispatch<2>(none, p, step, exact, 0, smem, 0);
+            sa_lane_dispatch<3>(none, p, step, exact, 0, smem, 0);
+            sa_lane_dispatch<4>(none, p, step, exact, 0, smem, 0);
+        }
+    done[dev] = true;
+}
+
 void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
                            cudaStream_t st) {
+    sa_prepare_extend_lane(p, t);
     // Register budget follows the CTAs per SM: 4 -> <= 64 registers, 3 -> <= 85, 2 -> <= 128.
     const SaExtK a = sa_ext_args(w, x, t);
     const int grid = num_sms * t.ext_ctas_per_sm;

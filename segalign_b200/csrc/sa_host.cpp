@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -138,27 +139,44 @@ uint64_t sa_host_chunk_seeds(const char* text, uint32_t j0, uint32_t j1, uint64_
 }
 
 // common/ntcoding.cpp:63-105; characters other than ACGTacgtnN& are skipped.
+// Large inputs are split into blocks on several threads: each block's count
+// of kept characters gives, by a suffix sum, where its output starts.
 uint64_t sa_host_revcomp(char* dst, const char* src, uint64_t len) {
-    uint64_t r = 0;
-    for (uint64_t i = len; i > 0; --i) {
-        char c = src[i - 1], o;
-        switch (c) {
-            case 'a': o = 't'; break;
-            case 'A': o = 'T'; break;
-            case 'c': o = 'g'; break;
-            case 'C': o = 'G'; break;
-            case 'g': o = 'c'; break;
-            case 'G': o = 'C'; break;
-            case 't': o = 'a'; break;
-            case 'T': o = 'A'; break;
-            case 'n': o = 'n'; break;
-            case 'N': o = 'N'; break;
-            case '&': o = '&'; break;
-            default: continue;
+    static const struct CompTable {
+        char c[256];
+        CompTable() {
+            std::memset(c, 0, sizeof c);
+            const char* from = "aAcCgGtTnN&";
+            const char* to = "tTgGcCaAnN&";
+            for (int i = 0; from[i]; ++i) c[(uint8_t)from[i]] = to[i];
         }
-        dst[r++] = o;
-    }
-    return r;
+    } comp;
+    unsigned hw = std::thread::hardware_concurrency();
+    const int nb = len >= (1u << 22) ? (int)std::min<unsigned>(16, hw ? hw : 1) : 1;
+    std::vector<uint64_t> lo(nb + 1), cnt(nb, 0), start(nb + 1, 0);
+    for (int b = 0; b <= nb; ++b) lo[b] = len * (uint64_t)b / (uint64_t)nb;
+    auto count = [&](int b) {
+        uint64_t k = 0;
+        for (uint64_t i = lo[b]; i < lo[b + 1]; ++i) k += comp.c[(uint8_t)src[i]] != 0;
+        cnt[b] = k;
+    };
+    auto write = [&](int b) {
+        char* o = dst + start[b + 1];  // kept characters of the blocks after b come first
+        for (uint64_t i = lo[b + 1]; i > lo[b]; --i) {
+            const char c = comp.c[(uint8_t)src[i - 1]];
+            if (c) *o++ = c;
+        }
+    };
+    auto run = [&](auto&& f) {
+        if (nb == 1) return f(0);
+        std::vector<std::thread> th;
+        for (int b = 0; b < nb; ++b) th.emplace_back(f, b);
+        for (auto& t : th) t.join();
+    };
+    run(count);
+    for (int b = nb - 1; b >= 0; --b) start[b] = start[b + 1] + cnt[b];  // kept in blocks b..nb-1
+    run(write);
+    return start[0];
 }
 
 // src/main.cpp:180-261 (no --scoring file): HOXD70 plus the lowercase, N,
@@ -220,10 +238,12 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
         return SA_ERR_ARG;
     auto t0 = std::chrono::steady_clock::now();
     if (query_len < (uint32_t)g_shape.seed_size) return SA_ERR_ARG;
-    std::vector<char> rctext(query_len);
+    std::unique_ptr<char[]> rcbuf;
     if (cfg->strand & 2) {
-        if (sa_host_revcomp(rctext.data(), query, query_len) != query_len) return SA_ERR_ARG;
+        rcbuf.reset(new char[query_len]);
+        if (sa_host_revcomp(rcbuf.get(), query, query_len) != query_len) return SA_ERR_ARG;
     }
+    const char* rctext = rcbuf.get();
     const uint32_t qlen_s = query_len - (uint32_t)g_shape.seed_size;
     struct Call {
         int strand;
@@ -252,7 +272,7 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
             uint64_t c = next.fetch_add(1);
             if (c >= calls.size()) break;
             const Call& cl = calls[c];
-            const char* txt = cl.strand ? rctext.data() : query;
+            const char* txt = cl.strand ? rctext : query;
             const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
             seeds.resize((uint64_t)(cl.j1 - cl.j0) * per);
             const uint64_t need = chunk_seeds(g_shape, txt, cl.j0, cl.j1, seeds.data(), seeds.size());

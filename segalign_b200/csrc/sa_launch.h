@@ -150,7 +150,12 @@ void sa_launch_extend_warp(SaWork& w, const SaExtendArgs& a, const SaParams& p, 
 
 // ---- sa_sort.cu ----
 // Sizes the call's HSP set from its hit count (<= 2 * surv_cap slots) and empties it.
-void sa_launch_hash_init(SaWork& w, cudaStream_t st);
+// Sizes the call's HSP set (device side, from the hit count); `full` also
+// empties every slot.  sa_launch_hash_clear only empties every slot.
+void sa_launch_hash_init(SaWork& w, bool full, cudaStream_t st);
+void sa_launch_hash_clear(SaWork& w, cudaStream_t st);
+// Kernel attributes of the lane kernel, set once per device outside stream capture.
+void sa_prepare_extend_lane(const SaParams& p, const SaTuning& t);
 // After the host has read a call's counters: whether the HSP set was left empty.
 void sa_note_hash_state(SaWork& w, const SaCounters& c);
 // mode 0 = plain dedup; 1 = rm (adds diagonal sort/unique and final sort).

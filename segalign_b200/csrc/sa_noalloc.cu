@@ -183,7 +183,9 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, flags, sizeof flags, cudaMemcpyHostToDevice, st));
     const int G = std::min(v.tuning.range_ctas, SA_MAX_CTAS);
     sa_launch_lookup_seeds(w, v.index, (uint32_t)v.nbuckets, v.params, G, st);
-    sa_launch_hash_init(w, st);
+    if (!w.hash_clean) sa_launch_hash_clear(w, st);
+    w.hash_clean = false;
+    sa_launch_hash_init(w, false, st);
     SaExtendArgs xa;
     xa.ref = v.ref;
     xa.ref_len = v.ref_len;

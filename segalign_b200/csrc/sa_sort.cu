@@ -256,12 +256,26 @@ __global__ void sa_k_dedup_prep(SaCounters* ctr, uint64_t cap, unsigned long lon
     st[0] = 0;
 }
 
-void sa_launch_hash_init(SaWork& w, cudaStream_t st) {
+static unsigned long long sa_hash_max_slots(const SaWork& w) {
     unsigned long long max_slots = 1;
     while (max_slots * 2 <= 2 * w.surv_cap) max_slots <<= 1;
-    sa_k_hash_init<<<148 * 8, 256, 0, st>>>(w.hset, w.ctr, max_slots, w.hash_clean ? 0 : 1);
+    return max_slots;
+}
+
+void sa_launch_hash_init(SaWork& w, bool full, cudaStream_t st) {
+    sa_k_hash_init<<<148 * 8, 256, 0, st>>>(w.hset, w.ctr, sa_hash_max_slots(w), full ? 1 : 0);
     sa_note_launch();
-    w.hash_clean = false;  // until the host has seen this call complete
+}
+
+__global__ void sa_k_hash_clear(unsigned long long* keys, unsigned long long n) {
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        keys[i] = ~0ull;
+}
+
+void sa_launch_hash_clear(SaWork& w, cudaStream_t st) {
+    sa_k_hash_clear<<<148 * 8, 256, 0, st>>>(w.hset.keys, 2 * sa_hash_max_slots(w));
+    sa_note_launch();
 }
 
 void sa_note_hash_state(SaWork& w, const SaCounters& c) {

@@ -57,9 +57,12 @@ def test_host_seeder_matches_oracle(built, shape, transition):
     assert np.array_equal(got, want)
 
 
-def test_host_revcomp_matches_oracle(built):
+@pytest.mark.parametrize("size", [10000, 5_000_003])
+def test_host_revcomp_matches_oracle(built, size):
+    """Small inputs take one pass; inputs of 4 Mi characters or more are split
+    into blocks on several threads (skipped characters shift the blocks)."""
     rng = np.random.default_rng(3)
-    t = rng.choice(np.frombuffer(b"ACGTacgtNn&RY", dtype=np.uint8), size=10000).tobytes()
+    t = rng.choice(np.frombuffer(b"ACGTacgtNn&RY", dtype=np.uint8), size=size).tobytes()
     assert sa.host_revcomp(t) == oracle.revcomp_text(t)
 
 
