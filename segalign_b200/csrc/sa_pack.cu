@@ -31,21 +31,42 @@ sa_k_scan_partials(unsigned long long* a, unsigned long long* b, int G, unsigned
 }
 
 __global__ void __launch_bounds__(1024)
-sa_k_radix_scan(unsigned int* hist, int G, const int* in_buf, int pass) {
+sa_k_radix_scan(unsigned int* hist, int G, const int* in_buf, int pass, const unsigned long long* d_n) {
     if (in_buf && in_buf[pass] < 0) return;
+    constexpr int PER = 8, TILE = 1024 * PER;
+    __shared__ unsigned int tile[TILE];
     __shared__ unsigned int ws[33];
     const int t = threadIdx.x;
-    const uint64_t n = (uint64_t)256 * G;
-    const uint64_t per = (n + 1023) / 1024;
-    const uint64_t a = (uint64_t)t * per, b = a + per < n ? a + per : n;
-    unsigned int s = 0;
-    for (uint64_t i = a; i < b; ++i) s += hist[i];
-    unsigned int tot;
-    unsigned int run = sa_block_excl_sum<unsigned int, 1024>(s, ws, &tot);
-    for (uint64_t i = a; i < b; ++i) {
-        unsigned int v = hist[i];
-        hist[i] = run;
-        run += v;
+    const uint32_t n = 256u * sa_radix_active(*d_n, (uint32_t)G);
+    unsigned int carry = 0;
+    for (uint32_t base = 0; base < n; base += TILE) {
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t i = base + k * 1024 + t;
+            tile[k * 1024 + t] = i < n ? hist[i] : 0u;
+        }
+        __syncthreads();
+        unsigned int v[PER], s = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            v[k] = tile[t * PER + k];
+            s += v[k];
+        }
+        unsigned int tot;
+        unsigned int run = sa_block_excl_sum<unsigned int, 1024>(s, ws, &tot) + carry;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            tile[t * PER + k] = run;
+            run += v[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const uint32_t i = base + k * 1024 + t;
+            if (i < n) hist[i] = tile[k * 1024 + t];
+        }
+        carry += tot;
+        __syncthreads();
     }
 }
 
@@ -281,7 +302,7 @@ void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint3
     for (int p = 0; p < passes; ++p) {
         sa_k_radix_up<SaKvOps><<<G, SA_RADIX_BLOCK, 0, st>>>(c, p, ctl, cta_hist);
         sa_note_launch();
-        sa_k_radix_scan<<<1, 1024, 0, st>>>(cta_hist, G, in_buf, p);
+        sa_k_radix_scan<<<1, 1024, 0, st>>>(cta_hist, G, in_buf, p, d_n);
         sa_note_launch();
         sa_k_radix_down<SaKvOps><<<G, SA_RADIX_BLOCK, 0, st>>>(c, p, ctl, cta_hist);
         sa_note_launch();

@@ -4,10 +4,12 @@
 //
 // Every kernel here is range-partitioned: CTA c of a G-CTA grid owns items
 // [n*c/G, n*(c+1)/G), with n read from device memory, so a whole call can be
-// launched without host round trips.  One pass = up-sweep (per-CTA digit
-// histogram), a single-CTA exclusive scan of the bin-major histogram, and a
-// stable down-sweep scatter that ranks equal digits inside a warp with
-// __match_any_sync and across warps with a per-round shared-memory prefix.
+// launched without host round trips.  The sort passes use only the first
+// A = min(G, ceil(n / SA_RADIX_MIN_ITEMS)) CTAs, so small sorts scan small
+// histograms.  One pass = up-sweep (per-CTA digit histogram), a single-CTA
+// exclusive scan of the bin-major histogram [256][A], and a stable down-sweep
+// scatter that ranks equal digits inside a warp with __match_any_sync and
+// across warps with a per-round shared-memory prefix.
 // A pass whose input buffer is recorded as -1 is skipped (all items share
 // that digit), which is how the fixed-layout HSP keys avoid scattering
 // constant bytes.
@@ -16,11 +18,29 @@
 #include "sa_internal.cuh"
 
 #define SA_RADIX_BLOCK 256
+#define SA_RADIX_MIN_ITEMS 512  // items per active CTA of a sort pass (at least)
 
 __device__ __forceinline__ void sa_cta_range(uint64_t n, uint64_t& a, uint64_t& b) {
     const uint64_t G = gridDim.x, c = blockIdx.x;
     a = (n * c) / G;
     b = (n * (c + 1)) / G;
+}
+
+// Active CTAs of a sort pass over n items on a G-CTA grid.
+__host__ __device__ __forceinline__ uint32_t sa_radix_active(uint64_t n, uint32_t G) {
+    const uint64_t want = (n + SA_RADIX_MIN_ITEMS - 1) / SA_RADIX_MIN_ITEMS;
+    return want == 0 ? 1u : (want < G ? (uint32_t)want : G);
+}
+
+// Range of CTA blockIdx.x among the A active CTAs (empty for the others).
+__device__ __forceinline__ void sa_radix_range(uint64_t n, uint32_t A, uint64_t& a, uint64_t& b) {
+    const uint64_t c = blockIdx.x;
+    if (c >= A) {
+        a = b = 0;
+        return;
+    }
+    a = (n * c) / A;
+    b = (n * (c + 1)) / A;
 }
 
 // Inclusive warp scan (sum).
@@ -62,8 +82,10 @@ __device__ __forceinline__ T sa_block_excl_sum(T v, T* ws, T* total) {
 __global__ void sa_k_scan_partials(unsigned long long* a, unsigned long long* b, int G,
                                    unsigned long long* ta, unsigned long long* tb);
 
-// Exclusive scan of the bin-major histogram [256][G] in place (one CTA of 1024).
-__global__ void sa_k_radix_scan(unsigned int* hist, int G, const int* in_buf, int pass);
+// Exclusive scan of the bin-major histogram [256][A] in place (one CTA of
+// 1024), A = sa_radix_active(*d_n, G).
+__global__ void sa_k_radix_scan(unsigned int* hist, int G, const int* in_buf, int pass,
+                                const unsigned long long* d_n);
 
 struct SaRadixCtl {
     const unsigned long long* d_n;  // item count
@@ -79,15 +101,18 @@ __global__ void __launch_bounds__(SA_RADIX_BLOCK)
 sa_k_radix_up(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, unsigned int* hist) {
     const int buf = ctl.in_buf[pass];
     if (buf < 0) return;
+    const uint64_t n = *ctl.d_n;
+    const uint32_t A = sa_radix_active(n, gridDim.x);
+    if (blockIdx.x >= A) return;
     __shared__ unsigned int h[256];
     const int t = threadIdx.x;
     h[t] = 0;
     __syncthreads();
     uint64_t a, b;
-    sa_cta_range(*ctl.d_n, a, b);
+    sa_radix_range(n, A, a, b);
     for (uint64_t i = a + t; i < b; i += SA_RADIX_BLOCK) atomicAdd(&h[Ops::digit(ctx, buf, i, pass)], 1u);
     __syncthreads();
-    hist[(uint64_t)t * gridDim.x + blockIdx.x] = h[t];
+    hist[(uint64_t)t * A + blockIdx.x] = h[t];
 }
 
 template <class Ops>
@@ -95,15 +120,18 @@ __global__ void __launch_bounds__(SA_RADIX_BLOCK)
 sa_k_radix_down(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, const unsigned int* hist) {
     const int buf = ctl.in_buf[pass];
     if (buf < 0) return;
+    const uint64_t n = *ctl.d_n;
+    const uint32_t A = sa_radix_active(n, gridDim.x);
+    if (blockIdx.x >= A) return;
     __shared__ unsigned int offs[256];
     __shared__ unsigned int wcnt[SA_RADIX_BLOCK / 32][256];
     const int t = threadIdx.x, warp = t >> 5;
-    offs[t] = hist[(uint64_t)t * gridDim.x + blockIdx.x];
+    offs[t] = hist[(uint64_t)t * A + blockIdx.x];
 #pragma unroll
     for (int w = 0; w < SA_RADIX_BLOCK / 32; ++w) wcnt[w][t] = 0;
     __syncthreads();
     uint64_t a, b;
-    sa_cta_range(*ctl.d_n, a, b);
+    sa_radix_range(n, A, a, b);
     const uint32_t lt = sa_lanemask_lt();
     for (uint64_t base = a; base < b; base += SA_RADIX_BLOCK) {
         const uint64_t i = base + t;

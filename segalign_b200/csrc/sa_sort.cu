@@ -122,7 +122,7 @@ static void sa_radix_sort_recs(SaWork& w, const SaSortSpec& spec, const unsigned
     for (int p = 0; p < spec.npass; ++p) {
         sa_k_radix_up<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
         sa_note_launch();
-        sa_k_radix_scan<<<1, 1024, 0, s>>>(w.sort_cta_hist, G, st + 1, p);
+        sa_k_radix_scan<<<1, 1024, 0, s>>>(w.sort_cta_hist, G, st + 1, p, d_n);
         sa_note_launch();
         sa_k_radix_down<SaRecOps><<<G, SA_RADIX_BLOCK, 0, s>>>(c, p, ctl, w.sort_cta_hist);
         sa_note_launch();
