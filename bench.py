@@ -72,6 +72,19 @@ def seeder_calls(query_len: int):
     return calls
 
 
+def lane_traffic(hits: float):
+    """DRAM bytes (read + write) of one lane-kernel launch, scaled by hits from
+    the ncu capture recorded in profiles/extend_lane_dram.json; (None, why) if absent."""
+    path = os.path.join(ROOT, "profiles", "extend_lane_dram.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        per_hit = float(d["dram_bytes"]) / float(d["hits"])
+    except (OSError, KeyError, ValueError, ZeroDivisionError):
+        return None, "no ncu capture recorded"
+    return per_hit * hits, f"ncu dram bytes per hit of {d['workload']} x this launch's hits"
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -239,7 +252,7 @@ def run_ours(args):
     sf = SeedFilter()
     sf.initialize_interface(1)
     sf.generate_shape_pos("12of19")
-    os.environ.setdefault("SA_SLOTS_PER_GPU", "4")
+    os.environ.setdefault("SA_SLOTS_PER_GPU", "8")  # concurrent plain calls per GPU (e2e leg)
     sf.initialize_processor(False, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
     sf.send_ref_write_request(w.target)
     t = time.perf_counter()
@@ -294,9 +307,10 @@ def run_ours(args):
     alg_bytes = 24.0 * nnz + 4.0 * hits + 24.0 * st_tiles + 16.0 * surv
     peak, peak_src = peaks()
     achieved = alg_bytes / (lane_ms_avg / 1000.0) / 1e9
+    traffic, traffic_src = lane_traffic(hits)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "sa_k_extend_lane", "peak_source": peak_src,
-                "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg}
+                "traffic": traffic, "traffic_source": traffic_src, "kernel": "sa_k_extend_lane",
+                "peak_source": peak_src, "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -323,13 +337,14 @@ def run_ours(args):
     if not args.no_e2e:
         k_e2e = args.e2e_steps or max(1, min(args.steps, 3))
         sf.set_timing(False)
-        sf.seeder_run(w.query, buffer=0, strand=3, num_threads=8, interval_size=INTERVAL, chunk_size=CHUNK,
+        e2e_threads = min(16, os.cpu_count() or 8)
+        sf.seeder_run(w.query, buffer=0, strand=3, num_threads=e2e_threads, interval_size=INTERVAL, chunk_size=CHUNK,
                       interval_overlap=OVERLAP)
         barrier()
         t0 = time.perf_counter()
         for _ in range(k_e2e):
-            fw, rc, sst = sf.seeder_run(w.query, buffer=0, strand=3, num_threads=8, interval_size=INTERVAL,
-                                        chunk_size=CHUNK, interval_overlap=OVERLAP)
+            fw, rc, sst = sf.seeder_run(w.query, buffer=0, strand=3, num_threads=e2e_threads,
+                                        interval_size=INTERVAL, chunk_size=CHUNK, interval_overlap=OVERLAP)
         barrier()
         e2e_s = (time.perf_counter() - t0) / k_e2e
         e2e_s_max = allreduce(e2e_s, "max")
@@ -339,8 +354,8 @@ def run_ours(args):
         h2d = sst["num_seeds"] * 8 + sst["num_calls"] * (32 + 32 + 1024)
         d2h = (sst["num_hsps"] + sst["num_calls"]) * 16 + sst["num_calls"] * 128
         out["e2e"] = {"value": e2e_hits / e2e_s_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                      "d2h_bytes_per_step": int(d2h), "path": "sa_seed_and_filter per 250 kbp unit from 8 host "
-                      "threads (C++ seeder), host wall time", "steps": k_e2e}
+                      "d2h_bytes_per_step": int(d2h), "path": f"sa_seed_and_filter per 250 kbp unit from "
+                      f"{e2e_threads} host threads (C++ seeder), host wall time", "steps": k_e2e}
         # batched with host buffers: query text up, HSP lists down
         sf.set_timing(True)
         barrier()
