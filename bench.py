@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=48, help="requests per load in the serving leg")
     return ap.parse_args()
 
 
@@ -180,6 +182,80 @@ def cpu_sample(w, max_chunks: int, threads: int):
                                  chunk_size=CHUNK, interval_overlap=OVERLAP, max_chunks=max_chunks)
     dt = time.perf_counter() - t
     return dict(seconds=dt, hits=st["num_hits"], hsps=st["num_hsps"], table_s=table_s, fw=fw, rc=rc, stats=st)
+
+
+def serve_requests(target: bytes, n: int, seed: int):
+    """Request texts of the serving workload: lengths log-uniform in
+    [10 kbp, 20 Mbp]; 30% of each request's bases are target blocks of
+    1-50 kbp with 20% substitutions, the rest i.i.d. bases at GC 36%."""
+    rng = np.random.default_rng(seed)
+    tgt = np.frombuffer(target, dtype=np.uint8)
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    out = []
+    for _ in range(n):
+        L = int(np.exp(rng.uniform(np.log(1e4), np.log(2e7))))
+        parts, have = [], 0
+        while have < L:
+            b = int(min(L - have, rng.integers(1_000, 50_001)))
+            if rng.random() < 0.3:
+                a = int(rng.integers(0, len(tgt) - b))
+                blk = tgt[a:a + b].copy()
+                m = rng.random(b) < 0.2
+                blk[m] = acgt[rng.integers(0, 4, int(m.sum()))]
+            else:
+                blk = acgt[rng.choice(4, size=b, p=[0.32, 0.18, 0.18, 0.32])]
+            parts.append(blk)
+            have += b
+        out.append(np.concatenate(parts).tobytes())
+    return out
+
+
+def run_serving(sf, target: bytes, n_req: int) -> dict:
+    """Serving leg: capacity from a closed-loop burst, then Poisson arrivals at
+    0.5x, 1x and 2x of it; latency = submission -> HSP lists on the host."""
+    reqs = serve_requests(target, n_req, seed=105)
+    sf.serve_start(interval_size=INTERVAL, interval_overlap=OVERLAP, chunk_size=CHUNK, strands=3)
+    try:
+        alone = {}
+        for k in range(4):  # a sample run alone, to compare with the same requests in the mix
+            alone[k] = sf.serve_wait(sf.serve_submit(reqs[k]))[:2]
+        # capacity: everything submitted at once
+        ids = [sf.serve_submit(q) for q in reqs]
+        st = [sf.serve_wait(r)[2] for r in ids]
+        span = max(x["done_s"] for x in st) - min(x["submit_s"] for x in st)
+        cap = len(reqs) / span
+        rates = []
+        exact = True
+        for load in (0.5, 1.0, 2.0):
+            rng = np.random.default_rng(int(load * 100))
+            gaps = rng.exponential(1.0 / (load * cap), size=len(reqs))
+            ids = []
+            t0 = time.perf_counter()
+            t_next = 0.0
+            for q, g in zip(reqs, gaps):
+                t_next += g
+                d = t_next - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                ids.append(sf.serve_submit(q))
+            res = [sf.serve_wait(r) for r in ids]
+            st = [x[2] for x in res]
+            for k, (fw, rc) in alone.items():
+                exact = exact and np.array_equal(res[k][0].view(np.uint32), fw.view(np.uint32)) and \
+                    np.array_equal(res[k][1].view(np.uint32), rc.view(np.uint32))
+            lat = np.array([x["done_s"] - x["submit_s"] for x in st]) * 1000.0
+            wall = max(x["done_s"] for x in st) - min(x["submit_s"] for x in st)
+            rates.append({"load": load, "offered_rps": load * cap, "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+                          "extensions_per_s": sum(x["num_hits"] for x in st) / wall,
+                          "hsps_per_s": sum(x["num_hsps"] for x in st) / wall,
+                          "mean_passes_per_request": float(np.mean([x["num_passes"] for x in st]))})
+    finally:
+        sf.serve_stop()
+    return {"workload": f"{n_req} requests per load, lengths log-uniform 10 kbp-20 Mbp (mean "
+                        f"{np.mean([len(q) for q in reqs]) / 1e6:.2f} Mbp), 30% target blocks at 20% divergence, "
+                        "both strands, against the resident genome-scale target table",
+            "capacity_rps": cap, "loads": rates, "bit_exact_alone_vs_mix": bool(exact)}
 
 
 def run_reference(args):
@@ -375,6 +451,11 @@ def run_ours(args):
             len(bf) == len(fw) and len(br) == len(rc) and np.array_equal(bf.view(np.uint32), fw.view(np.uint32))
             and np.array_equal(br.view(np.uint32), rc.view(np.uint32)))
         out["batched_vs_plain"] = out["value"] / out["e2e"]["value"]
+
+    # ---- serving form (one GPU): Poisson request stream over the resident table ----
+    if world == 1 and not args.no_serve:
+        sf.set_timing(False)
+        out["serving"] = run_serving(sf, w.target, args.serve_requests)
 
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only) ----
     if rank == 0 and world == 1 and not args.no_cpu:

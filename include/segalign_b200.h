@@ -171,6 +171,52 @@ typedef struct {
 int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment** out, uint64_t* out_len,
                              uint64_t* offsets);
 
+/* ---- serving form (no reference counterpart) ----
+ * A request loop over the resident target and seed table.  A request is one
+ * query sequence; it is cut into units exactly as the seeder cuts a query
+ * block (src/main.cpp:373-386 intervals, src/seeder.cpp:47-121 chunks and
+ * strands), so its result equals sa_seeder_run() on that query alone: one
+ * HSP list per strand, the units' lists concatenated in interval/chunk order
+ * (no per-unit headers).  Requests are admitted while their device buffers
+ * fit in a budget of free HBM taken at sa_serve_start (minus hbm_reserve);
+ * admitted requests' units are batched into device passes as they arrive, so
+ * a request that arrives while others are on the GPU joins the next pass and
+ * its buffers are built while the current pass runs. */
+typedef struct {
+    uint32_t interval_size;    /* query positions per interval; 0 = 10,000,000 */
+    uint32_t interval_overlap; /* positions shared with the next interval      */
+    uint32_t chunk_size;       /* positions per unit; 0 = the WGA chunk        */
+    int32_t strands;           /* 1 = plus, 2 = minus, 3 = both                */
+    uint64_t pass_slots;       /* seed slots per device pass; 0 = 2^25         */
+    uint64_t hbm_reserve;      /* free HBM admission leaves unused; 0 = 2 GiB  */
+} sa_serve_cfg;
+
+typedef struct {
+    double submit_s;           /* seconds since sa_serve_start: submitted      */
+    double admit_s;            /* device buffers built                         */
+    double done_s;             /* HSP lists complete on the host               */
+    uint64_t num_units;
+    uint64_t num_passes;       /* device passes the request took part in       */
+    uint64_t num_hits;         /* ungapped extensions                          */
+    uint64_t num_hsps;
+    uint64_t device_bytes;     /* device memory the request held               */
+} sa_serve_request_stats;
+
+#define SA_PENDING 1           /* sa_serve_wait: not finished within the timeout */
+
+/* Starts the request loop (one at a time per process); needs a resident
+ * target and seed table and an initialised processor. */
+int sa_serve_start(const sa_serve_cfg* cfg);
+/* Queues a copy of query[0, len); *request_id identifies it. */
+int sa_serve_submit(const char* query, uint32_t len, uint64_t* request_id);
+/* Waits up to timeout_ms (< 0: no limit) for a request.  SA_OK: *fw / *rc
+ * hold its plus / minus HSP lists (free with sa_free_segments) and the
+ * request is forgotten; SA_PENDING: not finished yet; < 0: it failed. */
+int sa_serve_wait(uint64_t request_id, int timeout_ms, sa_segment** fw, uint64_t* fw_len, sa_segment** rc,
+                  uint64_t* rc_len, sa_serve_request_stats* stats);
+/* Stops the loop; unfinished requests fail with SA_ERR_STATE. */
+int sa_serve_stop(void);
+
 /* ---- results, configuration, diagnostics (no reference counterpart) ---- */
 
 void sa_free_segments(sa_segment* segments);

@@ -48,6 +48,7 @@ EXPORTS = [
     "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
     "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
     "sa_set_tuning_param", "sa_get_tuning_param",
+    "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop",
 ]
 
 
@@ -74,6 +75,22 @@ class SeederCfg(C.Structure):
 class Unit(C.Structure):
     """sa_unit: seed positions [start, end) of query buffer `buffer` on strand `rev`."""
     _fields_ = [("buffer", C.c_uint32), ("rev", C.c_int32), ("start", C.c_uint32), ("end", C.c_uint32)]
+
+
+class ServeCfg(C.Structure):
+    """sa_serve_cfg: unit cutting, strands, seed slots per device pass, HBM left unused by admission."""
+    _fields_ = [("interval_size", C.c_uint32), ("interval_overlap", C.c_uint32), ("chunk_size", C.c_uint32),
+                ("strands", C.c_int32), ("pass_slots", C.c_uint64), ("hbm_reserve", C.c_uint64)]
+
+
+class ServeStats(C.Structure):
+    """sa_serve_request_stats: times in seconds since sa_serve_start."""
+    _fields_ = [("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("num_units", C.c_uint64), ("num_passes", C.c_uint64), ("num_hits", C.c_uint64),
+                ("num_hsps", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
+SA_PENDING = 1
 
 
 class SeederStats(C.Structure):
@@ -133,6 +150,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_seed_and_filter_noalloc": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, _P(C.c_uint8),
                                                      C.c_uint64, u64p]),
             "sa_kernel_launches": (C.c_uint64, []),
+            "sa_serve_start": (C.c_int, [_P(ServeCfg)]),
+            "sa_serve_submit": (C.c_int, [C.c_char_p, C.c_uint32, u64p]),
+            "sa_serve_wait": (C.c_int, [C.c_uint64, C.c_int, segpp, u64p, segpp, u64p, _P(ServeStats)]),
+            "sa_serve_stop": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -345,6 +366,37 @@ class SeedFilter:
         st = CallStats()
         self.lib.sa_last_call_stats(C.byref(st))
         return {k: getattr(st, k) for k, _ in CallStats._fields_ if k != "pad"}
+
+    # ---- serving form ----
+    def serve_start(self, interval_size: int = 10_000_000, interval_overlap: int = 0, chunk_size: int = 0,
+                    strands: int = 3, pass_slots: int = 0, hbm_reserve: int = 0) -> None:
+        """Starts the request loop over the resident target (sa_serve_start)."""
+        cfg = ServeCfg(interval_size, interval_overlap, chunk_size, strands, pass_slots, hbm_reserve)
+        self._chk(self.lib.sa_serve_start(C.byref(cfg)), "serve_start")
+
+    def serve_submit(self, query) -> int:
+        """Queues one query sequence; returns its request id."""
+        q = _bytes(query)
+        rid = C.c_uint64()
+        self._chk(self.lib.sa_serve_submit(q, len(q), C.byref(rid)), "serve_submit")
+        return rid.value
+
+    def serve_wait(self, request_id: int, timeout_ms: int = -1):
+        """(plus HSPs, minus HSPs, stats) of a request, or None if it is not
+        finished within timeout_ms; raises SegAlignError if it failed."""
+        fw, fl, rc, rl = _P(C.c_uint8)(), C.c_uint64(), _P(C.c_uint8)(), C.c_uint64()
+        st = ServeStats()
+        r = self.lib.sa_serve_wait(request_id, timeout_ms, C.byref(fw), C.byref(fl), C.byref(rc), C.byref(rl),
+                                   C.byref(st))
+        if r == SA_PENDING:
+            return None
+        self._chk(r, "serve_wait")
+        f = _take_segments(self.lib, fw, fl.value)
+        g = _take_segments(self.lib, rc, rl.value)
+        return f, g, {k: getattr(st, k) for k, _ in ServeStats._fields_}
+
+    def serve_stop(self) -> None:
+        self._chk(self.lib.sa_serve_stop(), "serve_stop")
 
     def seeder_run(self, query, buffer: int = 0, strand: int = 3, num_threads: int = 4,
                    interval_size: int = 10_000_000, chunk_size: int = 250_000, interval_overlap: int = 0,

@@ -1313,6 +1313,7 @@ int sa_resident_view(uint32_t buffer, SaResidentView* v) {
     v->q_len = (uint32_t)d.qf[buffer].len;
     v->max_seeds = g.max_seeds;
     v->max_hits = max_hits_now();
+    v->wga_chunk = g.wga_chunk;
     v->params = g.params;
     v->tuning = g.tuning;
     return SA_OK;

@@ -180,6 +180,7 @@ struct SaResidentView {
     uint32_t q_len;
     uint64_t max_seeds;
     uint64_t max_hits;
+    uint32_t wga_chunk;           // InitializeProcessor's WGA_CHUNK
     SaParams params;
     SaTuning tuning;
 };

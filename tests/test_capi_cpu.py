@@ -99,3 +99,17 @@ def test_tuning_validation(built):
     assert lib.sa_set_tuning(-1, -1, -1, 2048) == -1  # shared-memory tiles hold at most 1024 hits
     assert lib.sa_get_tuning_param(b"tile_hits") == 1024
     assert lib.sa_set_tuning(4096, 256, 3, 160) == 0
+
+
+def test_serve_calls_without_a_running_loop(built):
+    """Serving calls report SA_ERR_STATE until sa_serve_start succeeds; stop is harmless."""
+    import ctypes as C
+    lib = sa.load_library()
+    rid = C.c_uint64()
+    assert lib.sa_serve_submit(b"ACGTACGT", 8, C.byref(rid)) == -2
+    fw, rc = C.POINTER(C.c_uint8)(), C.POINTER(C.c_uint8)()
+    n1, n2 = C.c_uint64(), C.c_uint64()
+    assert lib.sa_serve_wait(1, 0, C.byref(fw), C.byref(n1), C.byref(rc), C.byref(n2), None) == -2
+    assert lib.sa_serve_stop() == 0
+    if not os.path.exists("/dev/nvidia0"):
+        assert lib.sa_serve_start(None) == -2  # no interface, target or table
