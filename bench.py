@@ -210,6 +210,46 @@ def serve_requests(target: bytes, n: int, seed: int):
     return out
 
 
+def distinct_rows(lists) -> np.ndarray:
+    """Distinct HSP records (16-byte rows) of a list of HSP arrays, sorted."""
+    a = np.concatenate([np.asarray(x).view(np.uint32).reshape(-1, 4) for x in lists]) if lists else \
+        np.zeros((0, 4), dtype=np.uint32)
+    k = a.view(np.uint64).reshape(-1, 2)
+    order = np.lexsort((k[:, 1], k[:, 0]))
+    k = k[order]
+    keep = np.ones(len(k), dtype=bool)
+    keep[1:] = (k[1:, 0] != k[:-1, 0]) | (k[1:, 1] != k[:-1, 1])
+    return k[keep]
+
+
+def run_uneven(sf, query_len: int, chunked_outs, chunked_units) -> dict:
+    """Batched form over uneven query windows (log-uniform 50 kbp-10 Mbp, both
+    strands, seeds 103/104): device time, and its distinct HSPs per strand
+    against the 250 kbp-chunk run's (chunking only adds duplicates)."""
+    from segalign_b200.synth import loguniform_chunks
+    L = query_len - SEED_SIZE
+    units = [(0, r, int(a), int(b)) for r in (0, 1) for a, b in loguniform_chunks(103 + r, L, 5e4, 1e7)]
+    sf.set_timing(True)
+    sf.seed_and_filter_batch(units, keep_on_device=True)  # warm
+    ms = []
+    for _ in range(3):
+        sf.seed_and_filter_batch(units, keep_on_device=True)
+        ms.append(sf.last_call_stats()["ms_total"])
+    st = sf.last_call_stats()
+    outs = sf.seed_and_filter_batch(units)
+    exact = True
+    for r in (0, 1):
+        got = distinct_rows([o[1:] for u, o in zip(units, outs) if u[1] == r])
+        want = distinct_rows([o[1:] for u, o in zip(chunked_units, chunked_outs) if u[1] == r])
+        exact = exact and got.shape == want.shape and np.array_equal(got, want)
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        tuned = sf.autotune(units, cache_path=os.path.join(d, "tune.jsonl"), quick=True, repeats=1)
+    return {"units": len(units), "extensions_per_step": st["num_hits"], "ms_per_step": min(ms),
+            "value": st["num_hits"] / (min(ms) / 1000.0), "hsps_per_step": st["num_hsps"],
+            "bit_exact_distinct_vs_250kbp_chunks": bool(exact), "autotune_quick": tuned}
+
+
 def run_serving(sf, target: bytes, n_req: int) -> dict:
     """Serving leg: capacity from a closed-loop burst, then Poisson arrivals at
     0.5x, 1x and 2x of it; latency = submission -> HSP lists on the host."""
@@ -451,6 +491,11 @@ def run_ours(args):
             len(bf) == len(fw) and len(br) == len(rc) and np.array_equal(bf.view(np.uint32), fw.view(np.uint32))
             and np.array_equal(br.view(np.uint32), rc.view(np.uint32)))
         out["batched_vs_plain"] = out["value"] / out["e2e"]["value"]
+
+    # ---- batched form over uneven windows, distinct HSPs vs the chunked run ----
+    if not args.no_e2e:
+        out["batched_uneven"] = run_uneven(sf, len(w.query), outs, units)
+        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=32, range_ctas=296)
 
     # ---- serving form (one GPU): Poisson request stream over the resident table ----
     if world == 1 and not args.no_serve:

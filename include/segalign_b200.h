@@ -262,6 +262,35 @@ const char* sa_last_error(void);
  * hits per warp tile.  -1 keeps a value. */
 int sa_set_tuning(int lane_cap, int ext_block, int ext_ctas_per_sm, int tile_hits);
 
+/* Phase timing state set by sa_set_timing. */
+int sa_get_timing(void);
+
+/* Autotuner (no reference counterpart).  Times the batched path on `units`
+ * under candidate settings of the named tuning parameters (coordinate
+ * descent from the current setting; each candidate must reproduce the
+ * starting setting's HSP lists exactly, else it is rejected), applies the
+ * fastest and records it in cache_path (JSON lines keyed by GPU name and
+ * workload signature).  With a cache hit and refresh == 0 the cached setting
+ * is applied without timing anything. */
+typedef struct {
+    const char* cache_path;  /* NULL: no cache                          */
+    int32_t repeats;         /* timed runs per candidate (best); 0 = 2   */
+    int32_t quick;           /* 1: fewer candidates, one round           */
+    int32_t refresh;         /* 1: ignore a cached entry                 */
+    int32_t pad;
+} sa_autotune_cfg;
+
+typedef struct {
+    int32_t ext_ctas_per_sm, step_bases, tile_hits, lane_cap, range_ctas;
+    int32_t candidates;      /* settings timed                           */
+    int32_t rejected;        /* settings that failed or changed results  */
+    int32_t from_cache;
+    double ms_start;         /* device ms of the batch at the start       */
+    double ms_best;          /* device ms with the chosen setting         */
+} sa_autotune_result;
+
+int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* cfg, sa_autotune_result* out);
+
 /* Named tuning parameters: "lane_cap", "ext_ctas_per_sm" (2..4), "tile_hits" (32..1024),
  * "step_bases" (8, 16 or 32 bases scored per lane step), "range_ctas" (CTAs of the
  * lookup/sort kernels).  Results never depend on them.  Returns SA_OK or

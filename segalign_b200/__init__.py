@@ -48,7 +48,7 @@ EXPORTS = [
     "sa_host_set_shape", "sa_host_chunk_seeds", "sa_host_revcomp", "sa_build_sub_mat", "sa_seeder_run",
     "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
     "sa_set_tuning_param", "sa_get_tuning_param",
-    "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop",
+    "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
 ]
 
 
@@ -91,6 +91,18 @@ class ServeStats(C.Structure):
 
 
 SA_PENDING = 1
+
+
+class AutotuneCfg(C.Structure):
+    _fields_ = [("cache_path", C.c_char_p), ("repeats", C.c_int32), ("quick", C.c_int32), ("refresh", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class AutotuneResult(C.Structure):
+    _fields_ = [("ext_ctas_per_sm", C.c_int32), ("step_bases", C.c_int32), ("tile_hits", C.c_int32),
+                ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("candidates", C.c_int32),
+                ("rejected", C.c_int32), ("from_cache", C.c_int32), ("ms_start", C.c_double),
+                ("ms_best", C.c_double)]
 
 
 class SeederStats(C.Structure):
@@ -154,6 +166,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_serve_submit": (C.c_int, [C.c_char_p, C.c_uint32, u64p]),
             "sa_serve_wait": (C.c_int, [C.c_uint64, C.c_int, segpp, u64p, segpp, u64p, _P(ServeStats)]),
             "sa_serve_stop": (C.c_int, []),
+            "sa_autotune": (C.c_int, [_P(Unit), C.c_uint32, _P(AutotuneCfg), _P(AutotuneResult)]),
+            "sa_get_timing": (C.c_int, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -325,6 +339,15 @@ class SeedFilter:
                   "SeedAndFilterBatch")
         allsegs = _take_segments(self.lib, ptr, n.value)
         return [allsegs[int(offs[i]):int(offs[i + 1])] for i in range(len(units))]
+
+    def autotune(self, units, cache_path: str | None = None, repeats: int = 0, quick: bool = False,
+                 refresh: bool = False) -> dict:
+        """Picks the fastest tuning for a batch of units (sa_autotune) and applies it."""
+        arr = (Unit * max(len(units), 1))(*[Unit(b, int(r), s, e) for (b, r, s, e) in units])
+        cfg = AutotuneCfg(cache_path.encode() if cache_path else None, repeats, int(quick), int(refresh), 0)
+        res = AutotuneResult()
+        self._chk(self.lib.sa_autotune(arr, len(units), C.byref(cfg), C.byref(res)), "autotune")
+        return {k: getattr(res, k) for k, _ in AutotuneResult._fields_}
 
     # ---- repeat_masker_src/seed_filter.cu ----
     def rm_send_query_write_request(self) -> None:

@@ -19,7 +19,7 @@ OBJ = os.path.join(HERE, "_obj")
 LIB = os.path.join(HERE, "libsegalign_b200.so")
 SYNTH = os.path.join(HERE, "libsa_synth.so")
 
-CU_SOURCES = ["sa_pack.cu", "sa_lookup.cu", "sa_extend.cu", "sa_sort.cu", "sa_api.cu", "sa_host.cpp", "sa_noalloc.cu", "sa_serve.cu"]
+CU_SOURCES = ["sa_pack.cu", "sa_lookup.cu", "sa_extend.cu", "sa_sort.cu", "sa_api.cu", "sa_host.cpp", "sa_noalloc.cu", "sa_serve.cu", "sa_tune.cu"]
 HEADERS = ["sa_internal.cuh", "sa_launch.h", "sa_radix.cuh"]
 
 NVCC_FLAGS = [

@@ -1265,6 +1265,8 @@ int sa_set_timing(int on) {
     return SA_OK;
 }
 
+int sa_get_timing(void) { return g_timing.load(); }
+
 uint64_t sa_kernel_launches(void) { return g_launches.load(); }
 
 }  // extern "C"

@@ -1,0 +1,209 @@
+// sa_tune.cu — in-library autotuner of the batched path's launch parameters.
+//
+// The kernels' results never depend on their tuning (every knob only changes
+// how work is spread over the GPU), so the tuner may pick any setting that is
+// fastest on a representative batch.  It times candidates by coordinate
+// descent from the current setting: one knob at a time over its candidate
+// values, keeping a change only when the batch's device time (lookup +
+// extension + dedup, CUDA events) drops, and checks that every candidate
+// reproduces the starting setting's HSP lists (a 64-bit hash of the whole
+// output).  The knobs stand for the choices the batched form exposes:
+//   ext_ctas_per_sm  lane-kernel CTAs per SM (registers per thread: 128/85/64)
+//   step_bases       bases a lane scores per step (the extension window)
+//   tile_hits        hits per warp tile held in shared memory
+//   lane_cap         bases a lane scans before a hit moves to a whole warp
+//   range_ctas       CTAs of the lookup, compaction and sort kernels
+// Results are cached per GPU name and workload signature in a JSON-lines
+// file, so a later run applies them without a sweep.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/segalign_b200.h"
+#include "sa_launch.h"
+
+namespace {
+
+struct Knob {
+    const char* name;
+    std::vector<int> full, quick;
+};
+
+const Knob kKnobs[] = {
+    {"ext_ctas_per_sm", {2, 3, 4}, {2, 3}},
+    {"step_bases", {8, 16, 32}, {16, 32}},
+    {"tile_hits", {96, 128, 160, 224, 320}, {128, 160, 224}},
+    {"lane_cap", {1024, 2048, 4096, 8192}, {2048, 4096}},
+    {"range_ctas", {148, 296, 592}, {296}},
+};
+constexpr int kNumKnobs = sizeof(kKnobs) / sizeof(kKnobs[0]);
+
+uint64_t fnv1a(const void* p, size_t n, uint64_t h) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= b[i];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+// One timed run of the batch: device ms of its phases and the output hash.
+int run_once(const sa_unit* units, uint32_t n, double* ms, uint64_t* hash) {
+    std::vector<uint64_t> offsets(n + 1);
+    sa_segment* out = nullptr;
+    uint64_t len = 0;
+    int r = sa_seed_and_filter_batch(units, n, &out, &len, offsets.data());
+    if (r != SA_OK) return r;
+    *hash = fnv1a(out, len * sizeof(sa_segment), 0xcbf29ce484222325ull);
+    sa_free_segments(out);
+    sa_call_stats st;
+    sa_last_call_stats(&st);
+    *ms = st.ms_lookup + st.ms_extend_lane + st.ms_extend_warp + st.ms_dedup;
+    return SA_OK;
+}
+
+int best_of(const sa_unit* units, uint32_t n, int repeats, double* ms, uint64_t* hash) {
+    double best = 1e300;
+    for (int i = 0; i < repeats; ++i) {
+        double t = 0;
+        int r = run_once(units, n, &t, hash);
+        if (r != SA_OK) return r;
+        best = t < best ? t : best;
+    }
+    *ms = best;
+    return SA_OK;
+}
+
+std::string signature(const sa_unit* units, uint32_t n) {
+    SaResidentView v{};
+    sa_resident_view(0, &v);
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, v.dev);
+    uint64_t positions = 0, minus = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        positions += units[i].end - units[i].start;
+        minus += units[i].rev ? 1 : 0;
+    }
+    std::ostringstream k;
+    k << prop.name << "|sms=" << prop.multiProcessorCount << "|target=" << v.ref_len << "|units=" << n
+      << "|minus=" << minus << "|positions=" << positions << "|xdrop=" << v.params.xdrop
+      << "|transition=" << v.params.transition << "|seed=" << v.params.seed_size;
+    return k.str();
+}
+
+// Cache line: {"key": "...", "ext_ctas_per_sm": 3, ..., "ms": 1.0}
+bool cache_lookup(const char* path, const std::string& key, int* values) {
+    if (!path) return false;
+    std::ifstream f(path);
+    std::string line;
+    const std::string tag = "\"key\": \"" + key + "\"";
+    while (std::getline(f, line)) {
+        if (line.find(tag) == std::string::npos) continue;
+        for (int i = 0; i < kNumKnobs; ++i) {
+            const std::string field = std::string("\"") + kKnobs[i].name + "\": ";
+            const size_t at = line.find(field);
+            if (at == std::string::npos) return false;
+            values[i] = std::atoi(line.c_str() + at + field.size());
+        }
+        return true;
+    }
+    return false;
+}
+
+void cache_store(const char* path, const std::string& key, const int* values, double ms) {
+    if (!path) return;
+    std::vector<std::string> keep;
+    {
+        std::ifstream f(path);
+        std::string line;
+        const std::string tag = "\"key\": \"" + key + "\"";
+        while (std::getline(f, line))
+            if (!line.empty() && line.find(tag) == std::string::npos) keep.push_back(line);
+    }
+    std::ostringstream e;
+    e << "{\"key\": \"" << key << "\"";
+    for (int i = 0; i < kNumKnobs; ++i) e << ", \"" << kKnobs[i].name << "\": " << values[i];
+    e << ", \"ms\": " << ms << "}";
+    keep.push_back(e.str());
+    std::ofstream o(path, std::ios::trunc);
+    for (auto& l : keep) o << l << "\n";
+}
+
+int apply(const int* values) {
+    for (int i = 0; i < kNumKnobs; ++i) {
+        const int r = sa_set_tuning_param(kKnobs[i].name, values[i]);
+        if (r != SA_OK) return r;
+    }
+    return SA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* cfg, sa_autotune_result* out) {
+    if (!units || !n_units || !out) return SA_ERR_ARG;
+    const sa_autotune_cfg c = cfg ? *cfg : sa_autotune_cfg{};
+    const int repeats = c.repeats > 0 ? c.repeats : 2;
+    const int rounds = c.quick ? 1 : 2;
+    std::memset(out, 0, sizeof *out);
+    int cur[kNumKnobs];
+    for (int i = 0; i < kNumKnobs; ++i) cur[i] = sa_get_tuning_param(kKnobs[i].name);
+    const std::string key = signature(units, n_units);
+    const int timing_was = sa_get_timing();
+    int cached[kNumKnobs];
+    if (!c.refresh && cache_lookup(c.cache_path, key, cached)) {
+        int r = apply(cached);
+        if (r != SA_OK) return r;
+        std::memcpy(cur, cached, sizeof cur);
+        out->from_cache = 1;
+    } else {
+        sa_set_timing(1);
+        double best_ms = 0;
+        uint64_t want = 0;
+        int r = best_of(units, n_units, repeats, &best_ms, &want);
+        if (r != SA_OK) {
+            sa_set_timing(timing_was);
+            return r;
+        }
+        out->ms_start = best_ms;
+        for (int round = 0; round < rounds; ++round)
+            for (int k = 0; k < kNumKnobs; ++k) {
+                const std::vector<int>& cand = c.quick ? kKnobs[k].quick : kKnobs[k].full;
+                int best_v = cur[k];
+                for (int v : cand) {
+                    if (v == cur[k]) continue;
+                    if (sa_set_tuning_param(kKnobs[k].name, v) != SA_OK) continue;
+                    double ms = 0;
+                    uint64_t h = 0;
+                    r = best_of(units, n_units, repeats, &ms, &h);
+                    ++out->candidates;
+                    if (r != SA_OK || h != want) {
+                        // a setting that fails or changes results is never kept
+                        ++out->rejected;
+                        continue;
+                    }
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best_v = v;
+                    }
+                }
+                cur[k] = best_v;
+                sa_set_tuning_param(kKnobs[k].name, cur[k]);
+            }
+        sa_set_timing(timing_was);
+        out->ms_best = best_ms;
+        cache_store(c.cache_path, key, cur, best_ms);
+    }
+    out->ext_ctas_per_sm = cur[0];
+    out->step_bases = cur[1];
+    out->tile_hits = cur[2];
+    out->lane_cap = cur[3];
+    out->range_ctas = cur[4];
+    return SA_OK;
+}
+
+}  // extern "C"

@@ -113,3 +113,14 @@ def test_serve_calls_without_a_running_loop(built):
     assert lib.sa_serve_stop() == 0
     if not os.path.exists("/dev/nvidia0"):
         assert lib.sa_serve_start(None) == -2  # no interface, target or table
+
+
+def test_autotune_needs_a_processor(built):
+    import ctypes as C
+    lib = sa.load_library()
+    if os.path.exists("/dev/nvidia0"):
+        pytest.skip("a GPU is present")
+    u = (sa.Unit * 1)(sa.Unit(0, 0, 0, 100))
+    res = sa.AutotuneResult()
+    assert lib.sa_autotune(u, 1, None, C.byref(res)) == -2  # SA_ERR_STATE
+    assert lib.sa_autotune(None, 0, None, C.byref(res)) == -1
