@@ -494,8 +494,9 @@ def run_ours(args):
 
     # ---- batched form over uneven windows, distinct HSPs vs the chunked run ----
     if not args.no_e2e:
+        saved = sf.get_tuning()
         out["batched_uneven"] = run_uneven(sf, len(w.query), outs, units)
-        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=32, range_ctas=296)
+        sf.set_tuning(**saved)
 
     # ---- serving form (one GPU): Poisson request stream over the resident table ----
     if world == 1 and not args.no_serve:

@@ -152,7 +152,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{4096, 256, 3, 256, 296, 160, 32};
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;

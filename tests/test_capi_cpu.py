@@ -98,7 +98,7 @@ def test_tuning_validation(built):
     assert lib.sa_set_tuning(512, 256, 3, 1024) == 0
     assert lib.sa_set_tuning(-1, -1, -1, 2048) == -1  # shared-memory tiles hold at most 1024 hits
     assert lib.sa_get_tuning_param(b"tile_hits") == 1024
-    assert lib.sa_set_tuning(4096, 256, 3, 160) == 0
+    assert lib.sa_set_tuning(8192, 256, 3, 160) == 0
 
 
 def test_serve_calls_without_a_running_loop(built):

@@ -116,12 +116,13 @@ def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
     w, p, sf = setup["w"], setup["p"], setup["sf"]
     seeds = host_seeds(w.query, 250_000, 500_000)
     want, st = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    saved = sf.get_tuning()
     sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile, step_bases=step)
     try:
         compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas} step={step}")
         assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
-        sf.set_tuning(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=32)
+        sf.set_tuning(**saved)
 
 
 def test_host_table_upload(setup):

@@ -8,9 +8,6 @@ from tests.helpers import compare_segments, small_workload
 
 pytestmark = pytest.mark.gpu
 
-DEFAULT = dict(lane_cap=4096, ext_ctas_per_sm=3, tile_hits=160, step_bases=32, range_ctas=296)
-
-
 @pytest.fixture(scope="module")
 def sf(built):
     w = small_workload()
@@ -21,12 +18,13 @@ def sf(built):
     s.send_ref_write_request(w.target)
     s.generate_seed_pos_table(None, 1, 19, 12)
     s.send_query_write_request(w.query, 0)
-    s.set_tuning(**DEFAULT)
+    saved = s.get_tuning()
     yield s
-    s.set_tuning(**DEFAULT)
+    s.set_tuning(**saved)
 
 
 def test_autotune_keeps_results_and_caches(sf, tmp_path):
+    DEFAULT = sf.get_tuning()
     L = 1_000_000 - 19
     units = [(0, r, a, min(a + 125_000, L)) for r in (0, 1) for a in range(0, L, 125_000)]
     want = sf.seed_and_filter_batch(units)
