@@ -50,12 +50,18 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = named sizes)")
-    ap.add_argument("--cpu-chunks", type=int, default=64, help="units in the bounded CPU sample")
+    ap.add_argument("--cpu-chunks", type=int, default=None,
+                    help="units in the bounded CPU sample (default 64; 2 for --workload large)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
-    ap.add_argument("--serve-requests", type=int, default=48, help="requests per load in the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=None,
+                    help="requests per load in the serving leg (default 48; 16 for --workload large)")
+    ap.add_argument("--workload", choices=["genome", "large"], default="genome",
+                    help="genome: 100 Mbp x 108 Mbp (the headline); large: 600 Mbp x 600 Mbp with transitions, "
+                         "a query sample of --query-sample bases against the whole target")
+    ap.add_argument("--query-sample", type=int, default=12_000_000, help="query bases used by --workload large")
     return ap.parse_args()
 
 
@@ -74,16 +80,17 @@ def seeder_calls(query_len: int):
     return calls
 
 
-def lane_traffic(hits: float):
+def lane_traffic(hits: float, workload: str):
     """DRAM bytes (read + write) of one lane-kernel launch, scaled by hits from
-    the ncu capture recorded in profiles/extend_lane_dram.json; (None, why) if absent."""
+    the ncu capture of this workload recorded in profiles/extend_lane_dram.json;
+    (None, why) if there is none."""
     path = os.path.join(ROOT, "profiles", "extend_lane_dram.json")
     try:
         with open(path) as f:
-            d = json.load(f)
+            d = json.load(f)[workload]
         per_hit = float(d["dram_bytes"]) / float(d["hits"])
-    except (OSError, KeyError, ValueError, ZeroDivisionError):
-        return None, "no ncu capture recorded"
+    except (OSError, KeyError, ValueError, ZeroDivisionError, TypeError):
+        return None, f"no ncu capture recorded for the {workload} workload"
     return per_hit * hits, f"ncu dram bytes per hit of {d['workload']} x this launch's hits"
 
 
@@ -167,10 +174,10 @@ def gpu_index(local_rank: int) -> int:
 _TABLES = {}
 
 
-def cpu_sample(w, max_chunks: int, threads: int):
+def cpu_sample(w, max_chunks: int, threads: int, transition: bool = False):
     import oracle
 
-    p = oracle.params()
+    p = oracle.params(transition=transition)
     t = time.perf_counter()
     key = id(w)
     if key not in _TABLES:
@@ -250,7 +257,7 @@ def run_uneven(sf, query_len: int, chunked_outs, chunked_units) -> dict:
             "bit_exact_distinct_vs_250kbp_chunks": bool(exact), "autotune_quick": tuned}
 
 
-def run_serving(sf, target: bytes, n_req: int) -> dict:
+def run_serving(sf, target: bytes, n_req: int, table: str) -> dict:
     """Serving leg: capacity from a closed-loop burst, then Poisson arrivals at
     0.5x, 1x and 2x of it; latency = submission -> HSP lists on the host."""
     reqs = serve_requests(target, n_req, seed=105)
@@ -294,34 +301,48 @@ def run_serving(sf, target: bytes, n_req: int) -> dict:
         sf.serve_stop()
     return {"workload": f"{n_req} requests per load, lengths log-uniform 10 kbp-20 Mbp (mean "
                         f"{np.mean([len(q) for q in reqs]) / 1e6:.2f} Mbp), 30% target blocks at 20% divergence, "
-                        "both strands, against the resident genome-scale target table",
+                        f"both strands, against the resident {table}",
             "capacity_rps": cap, "loads": rates, "bit_exact_alone_vs_mix": bool(exact)}
+
+
+def make_workload(args, rank: int):
+    """(workload, transition, description) of --workload; ranks get their own seeds."""
+    from segalign_b200 import synth
+
+    if args.workload == "large":
+        w = synth.make(4, seed=104 + 1000 * rank, scale=args.scale)
+        w = synth.Workload(w.target, w.query[: args.query_sample], w.target_chr, w.query_chr)
+        desc = (f"large: 600 Mbp target (12 chr) x the first {len(w.query) / 1e6:.0f} Mbp of a 600 Mbp query, "
+                "GC 41%, 45% repeats, 12of19 with one transition, HOXD70, xdrop 910, hspthresh 3000, entropy, "
+                "both strands, 10 Mbp intervals + 50 kbp overlap, 250 kbp units")
+        return w, True, desc
+    w = synth.make(2, seed=102 + 1000 * rank, scale=args.scale)
+    desc = ("genome scale: 100 Mbp target (6 chr) x 108 Mbp query, GC 36%, 12of19, HOXD70, xdrop 910, "
+            "hspthresh 3000, entropy, both strands, 10 Mbp intervals + 50 kbp overlap, 250 kbp units")
+    return w, False, desc
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from segalign_b200 import synth
-
-    w = synth.make(2, seed=102, scale=args.scale)
+    w, transition, desc = make_workload(args, 0)
     threads = os.cpu_count() or 1
     vals = []
     last = None
     for k in range(args.warmup + args.steps):
-        r = cpu_sample(w, args.cpu_chunks, threads)
+        r = cpu_sample(w, args.cpu_chunks, threads, transition)
         if k >= args.warmup:
             vals.append(r["hits"] / r["seconds"])
         last = r
     v = float(statistics.median(vals)) if vals else 0.0
     sample = (f"first {args.cpu_chunks} SeedAndFilter units (250 kbp, seeder order: interval 0 plus strand, then "
-              f"minus) of the genome-scale workload; {last['hits']} extensions per step")
+              f"minus) of the {args.workload} workload; {last['hits']} extensions per step")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * last["seconds"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "genome scale 100 Mbp (6 chr) x 108 Mbp, 12of19, xdrop 910, hspthresh 3000, both "
-                               "strands, 250 kbp units", "sample_units": args.cpu_chunks},
+        "config": {"workload": desc, "sample_units": args.cpu_chunks},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "hsps_per_s": last["hsps"] / last["seconds"],
@@ -364,12 +385,12 @@ def run_ours(args):
         return float(t.item())
 
     # weak scaling: each rank its own genome pair of the same shape
-    w = synth.make(2, seed=102 + 1000 * rank, scale=args.scale)
+    w, transition, desc = make_workload(args, rank)
     sf = SeedFilter()
     sf.initialize_interface(1)
     sf.generate_shape_pos("12of19")
     os.environ.setdefault("SA_SLOTS_PER_GPU", "8")  # concurrent plain calls per GPU (e2e leg)
-    sf.initialize_processor(False, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
+    sf.initialize_processor(transition, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
     sf.send_ref_write_request(w.target)
     t = time.perf_counter()
     sf.generate_seed_pos_table(None, 1, SEED_SIZE, 12)
@@ -423,7 +444,7 @@ def run_ours(args):
     alg_bytes = 24.0 * nnz + 4.0 * hits + 24.0 * st_tiles + 16.0 * surv
     peak, peak_src = peaks()
     achieved = alg_bytes / (lane_ms_avg / 1000.0) / 1e9
-    traffic, traffic_src = lane_traffic(hits)
+    traffic, traffic_src = lane_traffic(hits, args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_source": traffic_src, "kernel": "sa_k_extend_lane",
                 "peak_source": peak_src, "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg}
@@ -432,9 +453,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic",
-        "config": {"workload": "genome scale: 100 Mbp target (6 chr) x 108 Mbp query, GC 36%, 12of19, HOXD70, "
-                               "xdrop 910, hspthresh 3000, entropy, both strands, 10 Mbp intervals + 50 kbp overlap, "
-                               "250 kbp units", "path": "batched, device-resident", "units": len(units),
+        "config": {"workload": desc, "path": "batched, device-resident", "units": len(units),
                    "target_bp": len(w.target), "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)",
                    "scale": args.scale},
         "hsps_per_s": hsps_all / (ms_step_max / 1000.0),
@@ -455,12 +474,13 @@ def run_ours(args):
         sf.set_timing(False)
         e2e_threads = min(16, os.cpu_count() or 8)
         sf.seeder_run(w.query, buffer=0, strand=3, num_threads=e2e_threads, interval_size=INTERVAL, chunk_size=CHUNK,
-                      interval_overlap=OVERLAP)
+                      interval_overlap=OVERLAP, transition=transition)
         barrier()
         t0 = time.perf_counter()
         for _ in range(k_e2e):
             fw, rc, sst = sf.seeder_run(w.query, buffer=0, strand=3, num_threads=e2e_threads,
-                                        interval_size=INTERVAL, chunk_size=CHUNK, interval_overlap=OVERLAP)
+                                        interval_size=INTERVAL, chunk_size=CHUNK, interval_overlap=OVERLAP,
+                                        transition=transition)
         barrier()
         e2e_s = (time.perf_counter() - t0) / k_e2e
         e2e_s_max = allreduce(e2e_s, "max")
@@ -501,12 +521,15 @@ def run_ours(args):
     # ---- serving form (one GPU): Poisson request stream over the resident table ----
     if world == 1 and not args.no_serve:
         sf.set_timing(False)
-        out["serving"] = run_serving(sf, w.target, args.serve_requests)
+        n_req = args.serve_requests or (16 if args.workload == "large" else 48)
+        table = ("600 Mbp target table (transitions on)" if args.workload == "large"
+                 else "100 Mbp genome-scale target table")
+        out["serving"] = run_serving(sf, w.target, n_req, table)
 
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only) ----
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        r = cpu_sample(w, args.cpu_chunks, threads)
+        r = cpu_sample(w, args.cpu_chunks, threads, transition)
         cpu_v = r["hits"] / r["seconds"]
         out["cpu_baseline"] = {"value": cpu_v, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"first {args.cpu_chunks} 250 kbp units of the same workload "
@@ -533,6 +556,8 @@ def run_ours(args):
 
 def main():
     args = parse_args()
+    if args.cpu_chunks is None:
+        args.cpu_chunks = 2 if args.workload == "large" else 64
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -156,6 +156,16 @@ def test_transitions_small(built):
         got = sf.seed_and_filter(seeds, False, 1)
         want, _ = oracle.seed_and_filter(p, R, QC, idx, pos, seeds, False)
         compare_segments(got, want, f"transition chunk {j0}")
+    # batched units (13 seed slots per position, device seeding) equal the per-call results, both strands
+    QR = host_revcomp(Q)
+    units, plain = [], []
+    for rev, text in ((0, Q), (1, QR)):
+        for j0 in range(0, len(Q) - 19, 50_000):
+            j1 = min(j0 + 50_000, len(Q) - 19)
+            units.append((1, rev, j0, j1))
+            plain.append(sf.seed_and_filter(host_seeds(text, j0, j1, transition=True), bool(rev), 1))
+    for u, (g, x) in enumerate(zip(sf.seed_and_filter_batch(units), plain)):
+        compare_segments(g, x, f"batched transition unit {units[u]}")
 
 
 @pytest.mark.parametrize("exclude", [False, True])
