@@ -54,6 +54,50 @@ typedef struct {
 int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query_block, uint32_t query_len, sa_segment** fw,
                   uint64_t* fw_len, sa_segment** rc, uint64_t* rc_len, sa_seeder_stats* stats);
 
+/* Repeat-masker self-alignment driver over a whole sequence
+ * (repeat_masker_src/main.cpp:318-426 blocks and intervals with neighbour
+ * windows; repeat_masker_src/seeder.cpp:40-186 per-interval chunks on both
+ * strands through the rm SeedAndFilter, uint8 coverage of the HSPs' query
+ * ranges, runs with coverage >= M).  For every block it sends the block as the
+ * resident target (SendRefWriteRequest, rm SendQueryWriteRequest,
+ * GenerateSeedPosTable), so it replaces any resident target.  Runs are
+ * block-relative, in interval order; a run still open at the block end is not
+ * reported, as in the reference. */
+typedef struct {
+    uint32_t lastz_interval_size;  /* 0 = 10,000,000 (repeat_masker_src/graph.h:11) */
+    uint32_t seq_block_size;       /* 0 = 1e9 rounded down to a multiple of the interval */
+    float prop_neigh_interval;     /* 0 = 0.2                                  */
+    uint32_t M;                    /* 0 = 1: minimum coverage of a reported run */
+    uint32_t chunk_size;           /* 0 = the WGA chunk of InitializeProcessor  */
+    int32_t strand;                /* 1 plus, 2 minus, 3 both (0 = both)        */
+    int32_t num_threads;           /* intervals processed concurrently          */
+    uint32_t max_intervals;        /* 0 = every interval; else the first ones   */
+    uint32_t step;                 /* seed table step; 0 = 1                    */
+    uint32_t pad;
+} sa_rm_seeder_cfg;
+
+typedef struct {
+    uint32_t block;        /* block index                                 */
+    uint32_t interval;     /* interval index over all blocks              */
+    uint32_t query_start;  /* block-relative start of the run             */
+    uint32_t len;
+} sa_rm_run;
+
+typedef struct {
+    uint64_t num_seeds;
+    uint64_t num_hits;       /* hits looked up (every window)              */
+    uint64_t num_hsps;
+    uint64_t num_calls;
+    uint64_t num_intervals;
+    uint64_t num_blocks;
+    double seconds;
+} sa_rm_seeder_stats;
+
+int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_len, sa_rm_run** runs,
+                     uint64_t* n_runs, sa_rm_seeder_stats* stats);
+/* Frees the runs array of sa_rm_seeder_run. */
+void sa_free_rm_runs(sa_rm_run* runs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,8 @@ def lib() -> C.CDLL:
                                      _P(HitResult)]),
             "or_pipeline": (C.c_int, [_P(Params), _P(PipelineCfg), C.c_char_p, C.c_uint32, C.c_char_p, C.c_uint32,
                                       u32p, u32p, segpp, u64p, segpp, u64p, _P(Stats)]),
+            "or_rm_plan": (C.c_uint64, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, u32p,
+                                        C.c_uint64]),
             "or_rm_intervals": (C.c_uint64, [_P(SEGSTRUCT := C.c_uint8), C.c_uint64, C.c_uint32, C.c_uint32, u32p,
                                              u32p, C.c_uint64, u8p]),
         }
@@ -230,3 +232,12 @@ def rm_intervals(hsps: np.ndarray, block_len: int, M: int):
     L.or_rm_intervals(h.ctypes.data_as(_P(C.c_uint8)), len(h), block_len, M, st.ctypes.data_as(_P(C.c_uint32)),
                       ln.ctypes.data_as(_P(C.c_uint32)), n, cnt.ctypes.data_as(_P(C.c_uint8)))
     return st[:n], ln[:n]
+
+
+def rm_plan(seq_len: int, interval_size: int, block_size: int, prop_neigh: float, seed_size: int = 19) -> np.ndarray:
+    """repeat_masker_src/main.cpp:319-428 -> rows (block, block_start, block_len, start, end, ref_start, ref_end)."""
+    L = lib()
+    n = L.or_rm_plan(seq_len, interval_size, block_size, prop_neigh, seed_size, None, 0)
+    out = np.zeros((max(n, 1), 7), dtype=np.uint32)
+    L.or_rm_plan(seq_len, interval_size, block_size, prop_neigh, seed_size, out.ctypes.data_as(_P(C.c_uint32)), n)
+    return out[:n]

@@ -685,6 +685,58 @@ int or_pipeline(const or_params* p, const or_pipeline_cfg* cfg, const char* ref_
     return 0;
 }
 
+// repeat_masker_src/main.cpp:319-428.  Interval counts use float ceil as the
+// reference does; all window arithmetic is uint32.
+uint64_t or_rm_plan(uint64_t seq_len, uint32_t interval_size, uint32_t block_size, float prop_neigh,
+                    uint32_t seed_size, uint32_t* out, uint64_t cap) {
+    const uint32_t total = (uint32_t)std::ceil((float)seq_len / interval_size);
+    const uint32_t neigh = (uint32_t)std::ceil((float)prop_neigh * total);
+    const uint32_t left_iv = (uint32_t)std::ceil((float)(neigh - 1) / 2);
+    const uint32_t right_iv = neigh - 1 - left_iv;
+    const uint32_t left_overlap = left_iv * interval_size;
+    const uint32_t right_overlap = right_iv * interval_size;
+    const uint32_t max_len = left_overlap + interval_size + right_overlap;
+    uint64_t k = 0;
+    uint32_t block = 0;
+    for (uint64_t l = 0; l < seq_len; l += block_size, ++block) {
+        uint64_t bstart = (l < left_overlap) ? l : l - left_overlap;
+        uint32_t blen;
+        if (l + block_size + right_overlap > seq_len) blen = (uint32_t)(seq_len - bstart);
+        else blen = (uint32_t)(l - bstart + block_size) + right_overlap;
+        uint32_t start_pos = (uint32_t)(l - bstart), end_pos;
+        if (blen < block_size) end_pos = start_pos + blen - (uint32_t)(l - bstart) - seed_size;
+        else end_pos = start_pos + block_size - seed_size;
+        while (start_pos < end_pos) {
+            const uint32_t is = start_pos, ie = std::min(end_pos, is + interval_size);
+            uint32_t rs, re;
+            const bool ll = is < left_overlap, rl = (ie + right_overlap) > blen;
+            if (ll) {
+                rs = 0;
+                re = rl ? blen : (max_len > blen ? blen : max_len);
+            } else if (rl) {
+                re = blen;
+                rs = blen < max_len ? 0 : blen - max_len;
+            } else {
+                rs = is - left_overlap;
+                re = ie + right_overlap;
+            }
+            if (k < cap) {
+                uint32_t* row = out + 7 * k;
+                row[0] = block;
+                row[1] = (uint32_t)bstart;
+                row[2] = blen;
+                row[3] = is;
+                row[4] = ie;
+                row[5] = rs;
+                row[6] = re;
+            }
+            ++k;
+            start_pos += interval_size;
+        }
+    }
+    return k;
+}
+
 // repeat_masker_src/seeder.cpp:151-186: uint8 coverage over [qs, qs+len) of
 // every HSP, then runs with count >= M; a run still open at the block end is
 // not emitted (the loop only closes runs in its else branch).

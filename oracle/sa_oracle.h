@@ -134,6 +134,13 @@ int or_pipeline(const or_params* p, const or_pipeline_cfg* cfg,
 uint64_t or_rm_intervals(const or_segment* hsps, uint64_t n, uint32_t block_len, uint32_t M,
                          uint32_t* starts, uint32_t* lens, uint64_t cap, uint8_t* scratch_counts);
 
+// repeat_masker_src/main.cpp:319-428: blocks (with neighbour overlap) and
+// intervals with their target windows.  Row i of out (cap rows): block,
+// block_start (low 32 bits), block_len, start, end, ref_start, ref_end.
+// Returns the number of intervals.
+uint64_t or_rm_plan(uint64_t seq_len, uint32_t interval_size, uint32_t block_size, float prop_neigh,
+                    uint32_t seed_size, uint32_t* out, uint64_t cap);
+
 #ifdef __cplusplus
 }
 #endif

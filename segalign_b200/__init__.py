@@ -49,6 +49,7 @@ EXPORTS = [
     "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
     "sa_set_tuning_param", "sa_get_tuning_param",
     "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
+    "sa_rm_seeder_run", "sa_free_rm_runs",
 ]
 
 
@@ -103,6 +104,22 @@ class AutotuneResult(C.Structure):
                 ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("candidates", C.c_int32),
                 ("rejected", C.c_int32), ("from_cache", C.c_int32), ("ms_start", C.c_double),
                 ("ms_best", C.c_double)]
+
+
+class RmSeederCfg(C.Structure):
+    _fields_ = [("lastz_interval_size", C.c_uint32), ("seq_block_size", C.c_uint32),
+                ("prop_neigh_interval", C.c_float), ("M", C.c_uint32), ("chunk_size", C.c_uint32),
+                ("strand", C.c_int32), ("num_threads", C.c_int32), ("max_intervals", C.c_uint32),
+                ("step", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class RmSeederStats(C.Structure):
+    _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
+                ("num_calls", C.c_uint64), ("num_intervals", C.c_uint64), ("num_blocks", C.c_uint64),
+                ("seconds", C.c_double)]
+
+
+RM_RUN_DTYPE = np.dtype([("block", "<u4"), ("interval", "<u4"), ("query_start", "<u4"), ("len", "<u4")])
 
 
 class SeederStats(C.Structure):
@@ -168,6 +185,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_serve_stop": (C.c_int, []),
             "sa_autotune": (C.c_int, [_P(Unit), C.c_uint32, _P(AutotuneCfg), _P(AutotuneResult)]),
             "sa_get_timing": (C.c_int, []),
+            "sa_rm_seeder_run": (C.c_int, [_P(RmSeederCfg), C.c_char_p, C.c_uint64, _P(_P(C.c_uint8)), u64p,
+                                           _P(RmSeederStats)]),
+            "sa_free_rm_runs": (None, [_P(C.c_uint8)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -348,6 +368,25 @@ class SeedFilter:
         res = AutotuneResult()
         self._chk(self.lib.sa_autotune(arr, len(units), C.byref(cfg), C.byref(res)), "autotune")
         return {k: getattr(res, k) for k, _ in AutotuneResult._fields_}
+
+    def rm_seeder_run(self, seq, lastz_interval_size: int = 0, seq_block_size: int = 0, prop: float = 0.0,
+                      M: int = 0, chunk_size: int = 0, strand: int = 3, num_threads: int = 4,
+                      max_intervals: int = 0, step: int = 1, shape: str = "12of19", transition: bool = False):
+        """Repeat-masker self-alignment over a whole sequence (sa_rm_seeder_run):
+        (runs as RM_RUN_DTYPE records, stats)."""
+        q = _bytes(seq)
+        self.lib.sa_host_set_shape(shape.encode(), int(transition))
+        cfg = RmSeederCfg(lastz_interval_size, seq_block_size, prop, M, chunk_size, strand, num_threads,
+                          max_intervals, step, 0)
+        ptr, n, st = _P(C.c_uint8)(), C.c_uint64(), RmSeederStats()
+        self._chk(self.lib.sa_rm_seeder_run(C.byref(cfg), q, len(q), C.byref(ptr), C.byref(n), C.byref(st)),
+                  "rm_seeder_run")
+        try:
+            runs = np.frombuffer(bytes(C.cast(ptr, _P(C.c_uint8 * (16 * n.value))).contents), dtype=RM_RUN_DTYPE).copy() \
+                if n.value else np.zeros(0, dtype=RM_RUN_DTYPE)
+        finally:
+            self.lib.sa_free_rm_runs(ptr)
+        return runs, {k: getattr(st, k) for k, _ in RmSeederStats._fields_}
 
     # ---- repeat_masker_src/seed_filter.cu ----
     def rm_send_query_write_request(self) -> None:

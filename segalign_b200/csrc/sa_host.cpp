@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -316,6 +317,193 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
         stats->num_hits = nhits;
         stats->num_hsps = nhsps;
         stats->num_calls = calls.size();
+        stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return SA_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct RmInterval {
+    uint32_t block, start, end, ref_start, ref_end;
+};
+
+// Runs of coverage >= M over [0, block_len) for one interval's HSPs, with the
+// per-position uint8 counts of repeat_masker_src/seeder.cpp:151-186 (counts
+// wrap at 256) taken from a sweep over the sorted ends of the HSPs' query
+// ranges instead of a block-length array.  A run still open at block_len is
+// not reported, as the reference loop only closes runs in its else branch.
+void coverage_runs(std::vector<std::pair<uint32_t, int>>& ev, uint32_t block_len, uint32_t M, uint32_t block,
+                   uint32_t interval, std::vector<sa_rm_run>& out) {
+    std::sort(ev.begin(), ev.end());
+    int64_t count = 0;
+    bool run = false;
+    uint32_t run_start = 0;
+    size_t k = 0;
+    uint32_t pos = 0;
+    while (pos < block_len) {
+        while (k < ev.size() && ev[k].first <= pos) count += ev[k++].second;
+        const uint32_t next = k < ev.size() ? std::min(ev[k].first, block_len) : block_len;
+        const bool in = (uint32_t)(count & 255) >= M;
+        if (in && !run) {
+            run = true;
+            run_start = pos;
+        } else if (!in && run) {
+            run = false;
+            out.push_back({block, interval, run_start, pos - run_start});
+        }
+        pos = next;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void sa_free_rm_runs(sa_rm_run* runs) { free(runs); }
+
+int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_len, sa_rm_run** runs,
+                     uint64_t* n_runs, sa_rm_seeder_stats* stats) {
+    if (!cfg || !seq || !runs || !n_runs || seq_len == 0 || seq_len > 0xffffffffull) return SA_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    const uint32_t isz = cfg->lastz_interval_size ? cfg->lastz_interval_size : 10000000u;
+    uint32_t bsz = cfg->seq_block_size;
+    if (!bsz) bsz = 1000000000u - 1000000000u % isz;  // repeat_masker_src/main.cpp:255-258
+    const float prop = cfg->prop_neigh_interval > 0 ? cfg->prop_neigh_interval : 0.2f;
+    const uint32_t M = cfg->M ? cfg->M : 1;
+    const uint32_t chunk = cfg->chunk_size ? cfg->chunk_size : 250000u;
+    const int strand = cfg->strand ? cfg->strand : 3;
+    const uint32_t step = cfg->step ? cfg->step : 1;
+    const uint32_t S = (uint32_t)g_shape.seed_size;
+    // intervals and neighbour windows (repeat_masker_src/main.cpp:319-428)
+    uint32_t total_iv = (uint32_t)std::ceil((float)seq_len / isz);
+    const uint32_t num_neigh = (uint32_t)std::ceil(prop * total_iv);
+    const uint32_t left_iv = (uint32_t)std::ceil((float)(num_neigh - 1) / 2);
+    const uint32_t right_iv = num_neigh - 1 - left_iv;
+    const uint32_t left_ov = left_iv * isz, right_ov = right_iv * isz;
+    const uint32_t max_iv_len = left_ov + isz + right_ov;
+    std::vector<uint64_t> bstart;
+    std::vector<uint32_t> blen;
+    std::vector<RmInterval> ivs;
+    for (uint64_t l = 0; l < seq_len; l += bsz) {
+        const uint64_t b0 = l < left_ov ? l : l - left_ov;
+        const uint32_t bl = (l + bsz + right_ov > seq_len) ? (uint32_t)(seq_len - b0)
+                                                             : (uint32_t)(l - b0 + bsz) + right_ov;
+        const uint32_t blk = (uint32_t)bstart.size();
+        bstart.push_back(b0);
+        blen.push_back(bl);
+        uint32_t start_pos = (uint32_t)(l - b0), end_pos;
+        if (bl < bsz) end_pos = start_pos + bl - (uint32_t)(l - b0) - S;
+        else end_pos = start_pos + bsz - S;
+        while (start_pos < end_pos) {
+            RmInterval iv{blk, start_pos, std::min(end_pos, start_pos + isz), 0, 0};
+            const bool lim_l = iv.start < left_ov, lim_r = iv.end + right_ov > bl;
+            if (lim_l) {
+                iv.ref_start = 0;
+                iv.ref_end = lim_r ? bl : (max_iv_len > bl ? bl : max_iv_len);
+            } else if (lim_r) {
+                iv.ref_end = bl;
+                iv.ref_start = bl < max_iv_len ? 0 : bl - max_iv_len;
+            } else {
+                iv.ref_start = iv.start - left_ov;
+                iv.ref_end = iv.end + right_ov;
+            }
+            ivs.push_back(iv);
+            start_pos += isz;
+        }
+    }
+    if (cfg->max_intervals && ivs.size() > cfg->max_intervals) ivs.resize(cfg->max_intervals);
+    // reverse complement of the whole sequence, padded past its end with N
+    // (minus-strand seeds near a block end read past it, as in the reference)
+    std::unique_ptr<char[]> rc(new char[seq_len + 64]);
+    if (sa_host_revcomp(rc.get(), seq, seq_len) != seq_len) return SA_ERR_ARG;
+    std::memset(rc.get() + seq_len, 'N', 64);
+    std::vector<std::vector<sa_rm_run>> out(ivs.size());
+    std::atomic<uint64_t> nseeds{0}, nhits{0}, nhsps{0}, ncalls{0};
+    std::atomic<int> err{0};
+    const int nt = std::max(1, cfg->num_threads);
+    size_t first = 0;
+    uint32_t blocks_run = 0;
+    while (first < ivs.size() && !err) {
+        const uint32_t blk = ivs[first].block;
+        size_t last = first;
+        while (last < ivs.size() && ivs[last].block == blk) ++last;
+        const uint64_t b0 = bstart[blk];
+        const uint32_t bl = blen[blk];
+        int r = sa_send_ref_write_request(seq, b0, bl);
+        if (r == SA_OK) r = sa_rm_send_query_write_request();
+        if (r == SA_OK) r = sa_generate_seed_pos_table(seq, b0, bl, step, (int)S, g_shape.kmer_size);
+        if (r != SA_OK) return r;
+        ++blocks_run;
+        const char* text = seq + b0;
+        const char* rctext = rc.get() + (seq_len - b0 - bl);  // repeat_masker_src/seeder.cpp:49
+        std::atomic<size_t> next{first};
+        auto worker = [&]() {
+            const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
+            std::vector<uint64_t> seeds;
+            std::vector<std::pair<uint32_t, int>> ev;
+            while (!err) {
+                const size_t k = next.fetch_add(1);
+                if (k >= last) break;
+                const RmInterval& iv = ivs[k];
+                const uint32_t end_rc = bl - 1 - iv.start;
+                ev.clear();
+                auto call = [&](const char* t, uint32_t a, uint32_t b, int rev) -> int {
+                    if (b <= a) return SA_OK;
+                    seeds.resize((uint64_t)(b - a) * per);
+                    const uint64_t n = chunk_seeds(g_shape, t, a, b, seeds.data(), seeds.size());
+                    if (!n) return SA_OK;
+                    sa_segment* o = nullptr;
+                    uint64_t ol = 0;
+                    const int rr = sa_rm_seed_and_filter(seeds.data(), (uint32_t)n, rev, iv.ref_start, iv.ref_end, &o, &ol);
+                    if (rr != SA_OK) return rr;
+                    nseeds += n;
+                    nhits += (uint32_t)o[0].score;
+                    nhsps += ol - 1;
+                    ++ncalls;
+                    for (uint64_t h = 1; h < ol; ++h) {
+                        ev.emplace_back(o[h].query_start, 1);
+                        ev.emplace_back(o[h].query_start + o[h].len, -1);
+                    }
+                    sa_free_segments(o);
+                    return SA_OK;
+                };
+                for (uint32_t i = iv.start; i < iv.end && !err; i += chunk) {
+                    const uint32_t e = std::min(i + chunk, iv.end);
+                    int rr = SA_OK;
+                    if (strand & 1) rr = call(text, i, e, 0);
+                    if (rr == SA_OK && (strand & 2)) {
+                        const uint32_t ms = bl - 1 - e;  // repeat_masker_src/seeder.cpp:115-117
+                        rr = call(rctext, ms, std::min(ms + chunk, end_rc), 1);
+                    }
+                    if (rr != SA_OK) err = rr;
+                }
+                if (!err) coverage_runs(ev, bl, M, blk, (uint32_t)k, out[k]);
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t) th.emplace_back(worker);
+        for (auto& t : th) t.join();
+        first = last;
+    }
+    if (err) return err;
+    uint64_t total = 0;
+    for (auto& v : out) total += v.size();
+    *runs = (sa_rm_run*)malloc(sizeof(sa_rm_run) * (total ? total : 1));
+    if (!*runs) return SA_ERR_NOMEM;
+    uint64_t at = 0;
+    for (auto& v : out)
+        for (auto& x : v) (*runs)[at++] = x;
+    *n_runs = total;
+    if (stats) {
+        stats->num_seeds = nseeds;
+        stats->num_hits = nhits;
+        stats->num_hsps = nhsps;
+        stats->num_calls = ncalls;
+        stats->num_intervals = ivs.size();
+        stats->num_blocks = blocks_run;
         stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
     return SA_OK;

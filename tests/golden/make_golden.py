@@ -5,7 +5,8 @@ produced by the oracle (oracle/sa_oracle.cpp, a restatement of the reference
 semantics) on seeded inputs and committed; the hand-derived known-answer
 tests live in tests/test_oracle_kat.py.  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --rm-only  # the repeat-masker runs only (slow: oracle)
 """
 from __future__ import annotations
 
@@ -93,7 +94,63 @@ def small_calls():
     return out, calls
 
 
+# Repeat-masker self-alignment fixture: a repeat-rich 1.8 Mbp sequence (the
+# large workload's generator at scale 0.003, seed 11) in two blocks.
+RM = dict(scale=0.003, seed=11, interval_size=300_000, block_size=1_200_000, prop=0.2, chunk=100_000)
+RM_CASES = [(1, True), (2, False)]  # (M, diagonal excluded)
+
+
+def rm_runs(seq: bytes, M: int, exclude: bool) -> np.ndarray:
+    """The oracle's repeat-masker pipeline: block/interval plan
+    (repeat_masker_src/main.cpp:319-428), rm SeedAndFilter per chunk and strand
+    (repeat_masker_src/seeder.cpp:40-149), uint8 coverage runs (:151-186).
+    Rows: block, interval, block-relative start, length."""
+    isz, bsz, prop, ch = RM["interval_size"], RM["block_size"], RM["prop"], RM["chunk"]
+    p = oracle.params(rm_exclude_diag=exclude)
+    plan = oracle.rm_plan(len(seq), isz, bsz, prop)
+    rc_all = oracle.revcomp_text(seq) + b"N" * 64  # minus-strand seeds near a block end read past it
+    runs, tables = [], {}
+    for k, (blk, b0, bl, s, e, rs, re_) in enumerate(plan.tolist()):
+        block = seq[b0:b0 + bl]
+        if blk not in tables:
+            R = oracle.encode(block)
+            tables[blk] = (oracle.build_table(block, p), R, oracle.rc_codes(R))
+        (idx, pos), R, RC = tables[blk]
+        rct = rc_all[len(seq) - b0 - bl:]
+        hsps = []
+        for i in range(s, e, ch):
+            ee = min(i + ch, e)
+            sd = oracle.chunk_seeds(block, i, ee, p)
+            if len(sd):
+                hsps.append(oracle.seed_and_filter(p, R, R, idx, pos, sd, False, 1, rs, re_)[0][1:])
+            ms = bl - 1 - ee
+            me = min(ms + ch, bl - 1 - s)
+            if me > ms:
+                sd = oracle.chunk_seeds(rct, ms, me, p)
+                if len(sd):
+                    hsps.append(oracle.seed_and_filter(p, R, RC, idx, pos, sd, True, 1, rs, re_)[0][1:])
+        h = np.concatenate(hsps) if hsps else np.zeros(0, dtype=oracle.SEGMENT_DTYPE)
+        st, ln = oracle.rm_intervals(h, bl, M)
+        runs += [(blk, k, int(a), int(b)) for a, b in zip(st, ln)]
+    return np.array(runs, dtype=np.uint32).reshape(-1, 4)
+
+
+def rm_fixture():
+    seq = synth.make(4, seed=RM["seed"], scale=RM["scale"]).target
+    arrays = {f"M{M}_exclude{int(ex)}": rm_runs(seq, M, ex) for M, ex in RM_CASES}
+    np.savez_compressed(os.path.join(HERE, "rm_runs.npz"), **arrays)
+    with open(os.path.join(HERE, "rm_runs.json"), "w") as f:
+        json.dump({**RM, "seq_len": len(seq), "cases": [list(c) for c in RM_CASES]}, f, indent=1)
+    print("wrote rm runs", {k: len(v) for k, v in arrays.items()})
+
+
 def main():
+    if "--rm-only" not in sys.argv:
+        small_fixtures()
+    rm_fixture()
+
+
+def small_fixtures():
     rng = np.random.default_rng(20261203)
     with open(os.path.join(HERE, "kat_cases.json"), "w") as f:
         json.dump(kat_cases(rng), f, indent=0)
