@@ -62,6 +62,8 @@ def parse_args():
                     help="genome: 100 Mbp x 108 Mbp (the headline); large: 600 Mbp x 600 Mbp with transitions, "
                          "a query sample of --query-sample bases against the whole target")
     ap.add_argument("--query-sample", type=int, default=12_000_000, help="query bases used by --workload large")
+    ap.add_argument("--rm-intervals", type=int, default=4,
+                    help="--workload large: repeat-masker intervals run on the 600 Mbp target (0 = skip)")
     return ap.parse_args()
 
 
@@ -545,6 +547,21 @@ def run_ours(args):
                 len(gf) == len(r["fw"]) and len(gr) == len(r["rc"])
                 and np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32))
                 and np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))
+
+    # ---- repeat-masker self-alignment of the large target (last: it re-sends the target) ----
+    if args.workload == "large" and args.rm_intervals and world == 1:
+        sf.set_rm_exclude_diagonal(True)
+        try:
+            runs, rst = sf.rm_seeder_run(w.target, strand=3, num_threads=16, max_intervals=args.rm_intervals,
+                                         transition=transition)
+        finally:
+            sf.set_rm_exclude_diagonal(False)
+        out["rm_self_alignment"] = {
+            "workload": f"first {rst['num_intervals']} of the 10 Mbp intervals of the 600 Mbp target against "
+                        "their neighbour windows (proportion 0.2), both strands, transitions, diagonal excluded, M 1",
+            "seconds": rst["seconds"], "hits": rst["num_hits"], "hits_per_s": rst["num_hits"] / rst["seconds"],
+            "hsps": rst["num_hsps"], "calls": rst["num_calls"], "runs": int(len(runs)),
+            "covered_bases": int(runs["len"].sum()) if len(runs) else 0}
 
     if rank == 0:
         print(json.dumps(out), flush=True)
