@@ -98,6 +98,37 @@ int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_
 /* Frees the runs array of sa_rm_seeder_run. */
 void sa_free_rm_runs(sa_rm_run* runs);
 
+/* Chromosome table of a concatenated sequence text: chromosome i is
+ * starts[i] .. starts[i] + lens[i] (global positions, ascending). */
+typedef struct {
+    const char* const* names;
+    const uint64_t* starts;
+    const uint32_t* lens;
+    uint32_t count;
+    uint32_t pad;
+} sa_chrom_table;
+
+/* Segment writer, src/segment_printer.cpp:51-147: the lastz --segments lines
+ * of one SeedAndFilter interval's HSP lists, "rchr rstart rend qchr qstart
+ * qend +|- score" with 1-based starts and chromosome-relative coordinates.
+ * Plus-strand lines follow fw in order; minus-strand lines follow rc in
+ * reverse order, with query chromosomes placed in the reverse complement of
+ * the query block (start 2*block_start + block_len - start - len).  `query`
+ * is the whole query's table; the block is [query_block_start,
+ * query_block_start + query_block_len).  Texts are malloc'd (sa_free_text). */
+int sa_format_segments(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                       uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
+                       const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len, char** minus_text,
+                       uint64_t* minus_len);
+
+/* Interval writer of the repeat masker, repeat_masker_src/segment_printer.cpp:24-62:
+ * "chr start end" per run (start 0-based, end = start + len + 1 as the
+ * reference prints it), and an end-of-file marker line when markend. */
+int sa_format_rm_intervals(const sa_chrom_table* chroms, uint64_t block_start, const sa_rm_run* runs, uint64_t n,
+                           int markend, char** text, uint64_t* len);
+
+void sa_free_text(char* text);
+
 #ifdef __cplusplus
 }
 #endif

@@ -241,3 +241,48 @@ def rm_plan(seq_len: int, interval_size: int, block_size: int, prop_neigh: float
     out = np.zeros((max(n, 1), 7), dtype=np.uint32)
     L.or_rm_plan(seq_len, interval_size, block_size, prop_neigh, seed_size, out.ctypes.data_as(_P(C.c_uint32)), n)
     return out[:n]
+
+
+def _chrom_index(starts, x):
+    import bisect
+    return max(bisect.bisect_right(starts, x) - 1, 0)
+
+
+def format_segments(ref_chroms, r_block_start, q_chroms, q_block_start, q_block_len, fw, rc):
+    """src/segment_printer.cpp:51-147 (the .segments lines; the lastz command
+    lines are out of scope).  Chromosome tables: [(name, global start, len)].
+    The reference caches the current query chromosome, which picks the same
+    chromosome as its upper_bound lookup for every position inside one."""
+    rstarts = [c[1] for c in ref_chroms]
+    qstarts = [c[1] for c in q_chroms]
+    block = [c for c in q_chroms if q_block_start <= c[1] < q_block_start + q_block_len]
+    # src/main.cpp:355-362: rc table = the block's chromosomes in reverse order
+    rct = [(n, 2 * q_block_start + q_block_len - st - ln, ln) for (n, st, ln) in reversed(block)]
+    rcstarts = [c[1] for c in rct]
+
+    def lines(hsps, table, starts, strand):
+        out = []
+        for e in hsps:
+            sr = int(e["ref_start"]) + r_block_start
+            rn, rs, _ = ref_chroms[_chrom_index(rstarts, sr)]
+            sq = q_block_start + int(e["query_start"])
+            qn, qs, _ = table[_chrom_index(starts, sq)]
+            ln = int(e["len"])
+            out.append(f"{rn}\t{sr + 1 - rs}\t{sr + ln + 1 - rs}\t{qn}\t{sq + 1 - qs}\t{sq + ln + 1 - qs}\t{strand}\t"
+                       f"{int(e['score'])}\n")
+        return "".join(out)
+
+    return lines(fw, q_chroms, qstarts, "+"), lines(list(rc)[::-1], rct, rcstarts, "-")
+
+
+def format_rm_intervals(chroms, block_start, runs, markend=False):
+    """repeat_masker_src/segment_printer.cpp:24-62."""
+    starts = [c[1] for c in chroms]
+    out = []
+    for r in runs:
+        sq = block_start + int(r["query_start"])
+        n, st, _ = chroms[_chrom_index(starts, sq)]
+        out.append(f"{n}\t{sq - st}\t{sq + int(r['len']) + 1 - st}\n")
+    if out and markend:
+        out.append("# segalign_repeat_masker end-of-file\n")
+    return "".join(out)

@@ -49,7 +49,7 @@ EXPORTS = [
     "sa_seed_and_filter_batch", "sa_set_timing", "sa_kernel_launches", "sa_seed_and_filter_noalloc",
     "sa_set_tuning_param", "sa_get_tuning_param",
     "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
-    "sa_rm_seeder_run", "sa_free_rm_runs",
+    "sa_rm_seeder_run", "sa_free_rm_runs", "sa_format_segments", "sa_format_rm_intervals", "sa_free_text",
 ]
 
 
@@ -117,6 +117,19 @@ class RmSeederStats(C.Structure):
     _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
                 ("num_calls", C.c_uint64), ("num_intervals", C.c_uint64), ("num_blocks", C.c_uint64),
                 ("seconds", C.c_double)]
+
+
+class ChromTable(C.Structure):
+    _fields_ = [("names", C.POINTER(C.c_char_p)), ("starts", C.POINTER(C.c_uint64)), ("lens", C.POINTER(C.c_uint32)),
+                ("count", C.c_uint32), ("pad", C.c_uint32)]
+
+
+def _chrom_table(chroms):
+    """[(name, global start, length), ...] -> (ChromTable, kept buffers)."""
+    names = (C.c_char_p * len(chroms))(*[c[0].encode() for c in chroms])
+    starts = (C.c_uint64 * len(chroms))(*[int(c[1]) for c in chroms])
+    lens = (C.c_uint32 * len(chroms))(*[int(c[2]) for c in chroms])
+    return ChromTable(names, starts, lens, len(chroms), 0), (names, starts, lens)
 
 
 RM_RUN_DTYPE = np.dtype([("block", "<u4"), ("interval", "<u4"), ("query_start", "<u4"), ("len", "<u4")])
@@ -188,6 +201,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_rm_seeder_run": (C.c_int, [_P(RmSeederCfg), C.c_char_p, C.c_uint64, _P(_P(C.c_uint8)), u64p,
                                            _P(RmSeederStats)]),
             "sa_free_rm_runs": (None, [_P(C.c_uint8)]),
+            "sa_format_segments": (C.c_int, [_P(ChromTable), C.c_uint64, _P(ChromTable), C.c_uint64, C.c_uint32,
+                                             _P(C.c_uint8), C.c_uint64, _P(C.c_uint8), C.c_uint64,
+                                             _P(C.c_void_p), u64p, _P(C.c_void_p), u64p]),
+            "sa_format_rm_intervals": (C.c_int, [_P(ChromTable), C.c_uint64, _P(C.c_uint8), C.c_uint64, C.c_int,
+                                                 _P(C.c_void_p), u64p]),
+            "sa_free_text": (None, [C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -474,3 +493,42 @@ class SeedFilter:
         f = _take_segments(self.lib, fw, fl.value)
         r = _take_segments(self.lib, rc, rl.value)
         return f, r, {k: getattr(st, k) for k, _ in SeederStats._fields_}
+
+
+def _take_text(lib, ptr: C.c_void_p, n: int) -> str:
+    try:
+        return C.string_at(ptr, n).decode() if n else ""
+    finally:
+        lib.sa_free_text(ptr)
+
+
+def format_segments(ref_chroms, ref_block_start: int, query_chroms, query_block_start: int, query_block_len: int,
+                    fw: np.ndarray, rc: np.ndarray):
+    """lastz --segments lines of one interval's HSP lists (sa_format_segments):
+    (plus-strand text, minus-strand text).  Chromosome tables are
+    [(name, global start, length), ...]."""
+    lib = load_library()
+    rt, keep1 = _chrom_table(ref_chroms)
+    qt, keep2 = _chrom_table(query_chroms)
+    f = np.ascontiguousarray(fw, dtype=SEGMENT_DTYPE)
+    r = np.ascontiguousarray(rc, dtype=SEGMENT_DTYPE)
+    pt, pl, mt, ml = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_uint64()
+    st = lib.sa_format_segments(C.byref(rt), ref_block_start, C.byref(qt), query_block_start, query_block_len,
+                                f.ctypes.data_as(_P(C.c_uint8)), len(f), r.ctypes.data_as(_P(C.c_uint8)), len(r),
+                                C.byref(pt), C.byref(pl), C.byref(mt), C.byref(ml))
+    if st != 0:
+        raise SegAlignError(st, "format_segments", "")
+    return _take_text(lib, pt, pl.value), _take_text(lib, mt, ml.value)
+
+
+def format_rm_intervals(chroms, block_start: int, runs: np.ndarray, markend: bool = False) -> str:
+    """Repeat-masker interval lines of one interval's runs (sa_format_rm_intervals)."""
+    lib = load_library()
+    ct, keep = _chrom_table(chroms)
+    r = np.ascontiguousarray(runs, dtype=RM_RUN_DTYPE)
+    t, n = C.c_void_p(), C.c_uint64()
+    st = lib.sa_format_rm_intervals(C.byref(ct), block_start, r.ctypes.data_as(_P(C.c_uint8)), len(r), int(markend),
+                                    C.byref(t), C.byref(n))
+    if st != 0:
+        raise SegAlignError(st, "format_rm_intervals", "")
+    return _take_text(lib, t, n.value)

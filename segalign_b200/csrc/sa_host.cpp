@@ -326,6 +326,111 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
 
 namespace {
 
+// Index of the chromosome holding global position x: the last with start <= x
+// (std::upper_bound - 1, as src/segment_printer.cpp does); 0 before the first.
+uint32_t chrom_of(const uint64_t* starts, uint32_t n, uint64_t x) {
+    const uint64_t* it = std::upper_bound(starts, starts + n, x);
+    return it == starts ? 0u : (uint32_t)(it - starts - 1);
+}
+
+char* dup_text(const std::string& t, uint64_t* len) {
+    char* p = (char*)malloc(t.size() + 1);
+    if (!p) return nullptr;
+    std::memcpy(p, t.data(), t.size());
+    p[t.size()] = 0;
+    *len = t.size();
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+void sa_free_text(char* text) { free(text); }
+
+int sa_format_segments(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                       uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
+                       const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len, char** minus_text,
+                       uint64_t* minus_len) {
+    if (!ref || !query || !ref->count || !query->count || (n_fw && !fw) || (n_rc && !rc) || !plus_text ||
+        !plus_len || !minus_text || !minus_len)
+        return SA_ERR_ARG;
+    // reverse-complement chromosome table of the block (src/main.cpp:355-362):
+    // the block's chromosomes in reverse order
+    std::vector<uint64_t> rs;
+    std::vector<uint32_t> rl, ri;
+    for (uint32_t i = query->count; i-- > 0;) {
+        const uint64_t st = query->starts[i];
+        if (st < query_block_start || st >= query_block_start + query_block_len) continue;
+        rs.push_back(2 * query_block_start + query_block_len - st - query->lens[i]);
+        rl.push_back(query->lens[i]);
+        ri.push_back(i);
+    }
+    if (rs.empty()) return SA_ERR_ARG;
+    // "rchr rstart rend qchr " of one HSP
+    auto ref_part = [&](std::string& out, const sa_segment& e, const char* qname) {
+        const uint64_t sr = e.ref_start + ref_block_start;
+        const uint32_t r = chrom_of(ref->starts, ref->count, sr);
+        char buf[64];
+        out += ref->names[r];
+        std::snprintf(buf, sizeof buf, "\t%llu\t%llu\t", (unsigned long long)(sr + 1 - ref->starts[r]),
+                      (unsigned long long)(sr + e.len + 1 - ref->starts[r]));
+        out += buf;
+        out += qname;
+    };
+    std::string plus, minus;
+    for (uint64_t k = 0; k < n_fw; ++k) {
+        const sa_segment& e = fw[k];
+        const uint64_t sq = query_block_start + e.query_start;
+        const uint32_t q = chrom_of(query->starts, query->count, sq);
+        ref_part(plus, e, query->names[q]);
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "\t%llu\t%llu\t+\t%d\n", (unsigned long long)(sq + 1 - query->starts[q]),
+                      (unsigned long long)(sq + e.len + 1 - query->starts[q]), e.score);
+        plus += buf;
+    }
+    for (uint64_t k = n_rc; k-- > 0;) {
+        const sa_segment& e = rc[k];
+        const uint64_t sq = query_block_start + e.query_start;
+        const uint32_t j = chrom_of(rs.data(), (uint32_t)rs.size(), sq);
+        ref_part(minus, e, query->names[ri[j]]);
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "\t%llu\t%llu\t-\t%d\n", (unsigned long long)(sq + 1 - rs[j]),
+                      (unsigned long long)(sq + e.len + 1 - rs[j]), e.score);
+        minus += buf;
+    }
+    *plus_text = dup_text(plus, plus_len);
+    *minus_text = dup_text(minus, minus_len);
+    if (!*plus_text || !*minus_text) {
+        free(*plus_text);
+        free(*minus_text);
+        return SA_ERR_NOMEM;
+    }
+    return SA_OK;
+}
+
+int sa_format_rm_intervals(const sa_chrom_table* chroms, uint64_t block_start, const sa_rm_run* runs, uint64_t n,
+                           int markend, char** text, uint64_t* len) {
+    if (!chroms || !chroms->count || (n && !runs) || !text || !len) return SA_ERR_ARG;
+    std::string out;
+    char buf[64];
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint64_t sq = block_start + runs[k].query_start;
+        const uint32_t c = chrom_of(chroms->starts, chroms->count, sq);
+        out += chroms->names[c];
+        std::snprintf(buf, sizeof buf, "\t%llu\t%llu\n", (unsigned long long)(sq - chroms->starts[c]),
+                      (unsigned long long)(sq + runs[k].len + 1 - chroms->starts[c]));
+        out += buf;
+    }
+    if (n && markend) out += "# segalign_repeat_masker end-of-file\n";
+    *text = dup_text(out, len);
+    return *text ? SA_OK : SA_ERR_NOMEM;
+}
+
+}  // extern "C"
+
+namespace {
+
 struct RmInterval {
     uint32_t block, start, end, ref_start, ref_end;
 };

@@ -124,3 +124,49 @@ def test_autotune_needs_a_processor(built):
     res = sa.AutotuneResult()
     assert lib.sa_autotune(u, 1, None, C.byref(res)) == -2  # SA_ERR_STATE
     assert lib.sa_autotune(None, 0, None, C.byref(res)) == -1
+
+
+def _random_chroms(rng, n, first=0):
+    chroms, at = [], first
+    for i in range(n):
+        ln = int(rng.integers(1_000, 50_000))
+        chroms.append((f"chr{i + 1}", at, ln))
+        at += ln + 1  # '&' separator
+    return chroms, at - 1
+
+
+def test_segment_writer_matches_oracle(built):
+    """.segments lines (src/segment_printer.cpp:51-147) from the C++ writer
+    equal the oracle's restatement, for a query block in the middle of a
+    multi-chromosome query and HSPs spread over its chromosomes."""
+    rng = np.random.default_rng(5)
+    ref, rlen = _random_chroms(rng, 7)
+    query, qlen = _random_chroms(rng, 9)
+    qb0 = query[3][1]
+    qblen = query[7][1] + query[7][2] - qb0
+    rb0 = ref[1][1]
+
+    def hsps(n):
+        a = np.zeros(n, dtype=sa.SEGMENT_DTYPE)
+        a["ref_start"] = rng.integers(0, rlen - rb0 - 400, n)
+        a["query_start"] = rng.integers(0, qblen - 400, n)
+        a["len"] = rng.integers(1, 300, n)
+        a["score"] = rng.integers(3000, 20000, n)
+        return a
+
+    fw, rc = hsps(300), hsps(200)
+    got = sa.format_segments(ref, rb0, query, qb0, qblen, fw, rc)
+    want = oracle.format_segments(ref, rb0, query, qb0, qblen, fw, rc)
+    assert got == want
+    assert got[0].count("\n") == 300 and got[1].count("\n") == 200 and "\t-\t" in got[1]
+
+
+def test_rm_interval_writer_matches_oracle(built):
+    rng = np.random.default_rng(6)
+    chroms, total = _random_chroms(rng, 5)
+    runs = np.zeros(50, dtype=sa.RM_RUN_DTYPE)
+    runs["query_start"] = np.sort(rng.integers(0, total - 600, 50))
+    runs["len"] = rng.integers(1, 500, 50)
+    for markend in (False, True):
+        assert sa.format_rm_intervals(chroms, 0, runs, markend) == oracle.format_rm_intervals(chroms, 0, runs, markend)
+    assert sa.format_rm_intervals(chroms, 0, runs[:0], True) == ""
