@@ -307,6 +307,28 @@ def run_serving(sf, target: bytes, n_req: int, table: str) -> dict:
             "capacity_rps": cap, "loads": rates, "bit_exact_alone_vs_mix": bool(exact)}
 
 
+def allreduce_value(x: float, op: str, dist=None, device: str = "cuda") -> float:
+    """One scalar reduced over the ranks ("max" or "sum"); the value itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_figures(ms_step: float, hits: float, hsps: float, dist=None, device: str = "cuda") -> dict:
+    """Whole-job figures of a weak-scaled step: every rank runs its own
+    workload, so the step lasts as long as the slowest rank and the work of
+    all ranks adds up."""
+    ms = allreduce_value(ms_step, "max", dist, device)
+    h = allreduce_value(hits, "sum", dist, device)
+    hs = allreduce_value(hsps, "sum", dist, device)
+    return {"ms_per_step": ms, "extensions": h, "hsps": hs, "value": h / (ms / 1000.0),
+            "hsps_per_s": hs / (ms / 1000.0)}
+
+
 def make_workload(args, rank: int):
     """(workload, transition, description) of --workload; ranks get their own seeds."""
     from segalign_b200 import synth
@@ -380,11 +402,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def allreduce(x: float, op: str) -> float:
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
-        return float(t.item())
+        return allreduce_value(x, op, dist)
 
     # weak scaling: each rank its own genome pair of the same shape
     w, transition, desc = make_workload(args, rank)
@@ -432,10 +450,8 @@ def run_ours(args):
         wall_s = time.perf_counter() - t0
     launches = sf.kernel_launches() - l0
     ms_step = sum(dev_ms) / len(dev_ms)
-    ms_step_max = allreduce(ms_step, "max")
-    hits_all = allreduce(float(hits), "sum")
-    hsps_all = allreduce(float(hsps), "sum")
-    value = hits_all / (ms_step_max / 1000.0)
+    job = job_figures(ms_step, float(hits), float(hsps), dist)
+    ms_step_max, hits_all, hsps_all, value = job["ms_per_step"], job["extensions"], job["hsps"], job["value"]
 
     # roofline of the dominant kernel (lane-per-hit X-drop): algorithmic bytes
     # = 24 B per hit-bearing seed (E, lo, j, scope, unit) + 4 B per hit (pos)
