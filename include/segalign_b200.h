@@ -281,7 +281,7 @@ typedef struct {
 } sa_autotune_cfg;
 
 typedef struct {
-    int32_t ext_ctas_per_sm, step_bases, tile_hits, lane_cap, range_ctas;
+    int32_t ext_ctas_per_sm, step_bases, tile_hits, lane_cap, range_ctas, substeps;
     int32_t candidates;      /* settings timed                           */
     int32_t rejected;        /* settings that failed or changed results  */
     int32_t from_cache;
@@ -292,6 +292,7 @@ typedef struct {
 int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* cfg, sa_autotune_result* out);
 
 /* Named tuning parameters: "lane_cap", "ext_ctas_per_sm" (2..4), "tile_hits" (32..1024),
+ * "substeps" (1..8 steps a lane may take per iteration of the lane kernel),
  * "step_bases" (8, 16 or 32 bases scored per lane step), "range_ctas" (CTAs of the
  * lookup/sort kernels).  Results never depend on them.  Returns SA_OK or
  * SA_ERR_ARG; sa_get_tuning_param returns the current value. */

@@ -101,7 +101,7 @@ class AutotuneCfg(C.Structure):
 
 class AutotuneResult(C.Structure):
     _fields_ = [("ext_ctas_per_sm", C.c_int32), ("step_bases", C.c_int32), ("tile_hits", C.c_int32),
-                ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("candidates", C.c_int32),
+                ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("substeps", C.c_int32), ("candidates", C.c_int32),
                 ("rejected", C.c_int32), ("from_cache", C.c_int32), ("ms_start", C.c_double),
                 ("ms_best", C.c_double)]
 
@@ -434,7 +434,7 @@ class SeedFilter:
         self._chk(self.lib.sa_set_tuning(lane_cap, ext_block, ext_ctas_per_sm, tile_hits), "set_tuning")
 
     def get_tuning(self) -> dict:
-        names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas")
+        names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas", "substeps")
         return {n: int(self.lib.sa_get_tuning_param(n.encode())) for n in names}
 
     def set_timing(self, on: bool) -> None:

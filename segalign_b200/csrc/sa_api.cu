@@ -152,7 +152,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 1};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -1356,9 +1356,12 @@ int sa_set_tuning_param(const char* name, int value) {
         t.range_ctas = value;
         return SA_OK;
     }
-    if (n == "long_ctas_per_sm") {
-        if (value < 1 || value > 8) return SA_ERR_ARG;
-        t.long_block = 256;
+    if (n == "substeps") {
+        if (value < 1 || value > 8) {
+            sa_set_error(SA_ERR_ARG, "substeps must be 1..8 (got %d)", value);
+            return SA_ERR_ARG;
+        }
+        t.substeps = value;
         return SA_OK;
     }
     sa_set_error(SA_ERR_ARG, "unknown tuning parameter %s", name);
@@ -1373,6 +1376,7 @@ int sa_get_tuning_param(const char* name) {
     if (n == "ext_ctas_per_sm") return t.ext_ctas_per_sm;
     if (n == "tile_hits") return t.tile_hits;
     if (n == "step_bases") return t.step_bases;
+    if (n == "substeps") return t.substeps;
     if (n == "range_ctas") return t.range_ctas;
     return SA_ERR_ARG;
 }

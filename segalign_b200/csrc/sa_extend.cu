@@ -46,6 +46,7 @@ struct SaExtK {
     int32_t xdrop, hspthresh, noentropy;
     uint32_t lane_cap;
     uint32_t tile_hits;
+    uint32_t substeps;  // steps per lane-kernel iteration (at most)
 };
 
 // Reverse the order of the 8 nibbles of a word.
@@ -409,91 +410,102 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         }
         const bool done = !__any_sync(SA_FULL, has) && exhausted && tile_pos >= tile_n;
 
-        // ---- one STEP-base step per busy lane ----
+        // ---- up to `substeps` STEP-base steps per busy lane: the lanes still
+        // scanning go on while any lane of the warp does; a lane stops for
+        // this iteration when its direction ends or it goes to the long queue ----
         bool finished = false, to_long = false;
         int Lpos = 0, total = 0;
-        if (has) {
-            uint32_t rwin[NW], qwin[NW];
-#pragma unroll
-            for (int j = 0; j < NW; ++j) {
-                rwin[j] = __funnelshift_r(w_r[j], w_r[j + 1], sh_r);
-                qwin[j] = __funnelshift_r(w_q[j], w_q[j + 1], sh_q);
-            }
-            w_r[0] = w_r[NW];
-            w_q[0] = w_q[NW];
-#pragma unroll
-            for (int j = 1; j <= NW; ++j) {
-                w_r[j] = __ldg(pr + j - 1);
-                w_q[j] = __ldg(pq + j - 1);
-            }
-            pr += NW;
-            pq += NW;
-            const bool edge = o + STEP > avail;
-            bool stop = false;
-            uint32_t lo, hi;
-            if (EXACT) {
-                bool alive = true;
-                int pk = 0;
-                const int best_in = best;
-                if (!edge) {
-#pragma unroll
-                    for (int j = 0; j < NW; ++j) {
-                        sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_exact<false>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
+        bool scanning = has;
+#pragma unroll 1
+        for (uint32_t sub = 0; sub < a.substeps; ++sub) {
+            if (!__any_sync(SA_FULL, scanning)) break;
+            if (scanning) {
+                uint32_t rwin[NW], qwin[NW];
+    #pragma unroll
+                for (int j = 0; j < NW; ++j) {
+                    rwin[j] = __funnelshift_r(w_r[j], w_r[j + 1], sh_r);
+                    qwin[j] = __funnelshift_r(w_q[j], w_q[j + 1], sh_q);
+                }
+                w_r[0] = w_r[NW];
+                w_q[0] = w_q[NW];
+    #pragma unroll
+                for (int j = 1; j <= NW; ++j) {
+                    w_r[j] = __ldg(pr + j - 1);
+                    w_q[j] = __ldg(pq + j - 1);
+                }
+                pr += NW;
+                pq += NW;
+                const bool edge = o + STEP > avail;
+                bool stop = false;
+                uint32_t lo, hi;
+                if (EXACT) {
+                    bool alive = true;
+                    int pk = 0;
+                    const int best_in = best;
+                    if (!edge) {
+    #pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            sa_merge8(rwin[j], qwin[j], lo, hi);
+                            sa_window_exact<false>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
+                        }
+                    } else {
+    #pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            sa_merge8(rwin[j], qwin[j], lo, hi);
+                            sa_window_exact<true>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
+                        }
                     }
+                    if (best != best_in) bpos = (int)o + pk;
+                    stop = !alive;
                 } else {
-#pragma unroll
-                    for (int j = 0; j < NW; ++j) {
-                        sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_exact<true>(tblb, lo, hi, 8 * j, o + 8 * j, avail, a.xdrop, S, best, pk, alive);
+                    int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
+                    if (!edge) {
+    #pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            sa_merge8(rwin[j], qwin[j], lo, hi);
+                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
+                        }
+                    } else {
+    #pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            sa_merge8(rwin[j], qwin[j], lo, hi);
+                            // a base past the sequence end scores -(xdrop + 1)
+                            sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
+                                                     a.xdrop, Pk, B, at, stop);
+                        }
+                    }
+                    const int low = at & (SCALE - 1);
+                    if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
+                    const int best_in = best;
+                    best = best_in + (at >> SH);
+                    S = best_in + (Pk >> SH);  // exact after a full step without a stop
+                }
+                if (stop) {
+                    // Steps start at multiples of STEP (8, 16 or 32), so the stop offset
+                    // lies in 32-base tile o >> 5 whichever base of the step it is.
+                    tiles += (o >> 5) + 1;
+                    if (dir == 0) {
+                        Rbest = best;
+                        Rpos = best > 0 ? bpos : -1;  // -1 when no positive score
+                        dir = 1;
+                        setup = true;
+                    } else {
+                        finished = true;
+                    }
+                    scanning = false;
+                } else {
+                    o += STEP;
+                    if (o >= a.lane_cap && !nocap) {
+                        to_long = true;
+                        scanning = false;
                     }
                 }
-                if (best != best_in) bpos = (int)o + pk;
-                stop = !alive;
-            } else {
-                int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
-                if (!edge) {
-#pragma unroll
-                    for (int j = 0; j < NW; ++j) {
-                        sa_merge8(rwin[j], qwin[j], lo, hi);
-                        sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < NW; ++j) {
-                        sa_merge8(rwin[j], qwin[j], lo, hi);
-                        // a base past the sequence end scores -(xdrop + 1)
-                        sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
-                                                 a.xdrop, Pk, B, at, stop);
-                    }
+                if (finished) {
+                    Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
+                    total = Rbest + best;
+                    tiles_acc += tiles;
+                    has = false;
                 }
-                const int low = at & (SCALE - 1);
-                if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
-                const int best_in = best;
-                best = best_in + (at >> SH);
-                S = best_in + (Pk >> SH);  // exact after a full step without a stop
-            }
-            if (stop) {
-                // Steps start at multiples of STEP (8, 16 or 32), so the stop offset
-                // lies in 32-base tile o >> 5 whichever base of the step it is.
-                tiles += (o >> 5) + 1;
-                if (dir == 0) {
-                    Rbest = best;
-                    Rpos = best > 0 ? bpos : -1;  // -1 when no positive score
-                    dir = 1;
-                    setup = true;
-                } else {
-                    finished = true;
-                }
-            } else {
-                o += STEP;
-                if (o >= a.lane_cap && !nocap) to_long = true;
-            }
-            if (finished) {
-                Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
-                total = Rbest + best;
-                tiles_acc += tiles;
-                has = false;
             }
         }
 
@@ -765,6 +777,7 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.noentropy = x.noentropy;
     a.lane_cap = (uint32_t)t.lane_cap;
     a.tile_hits = (uint32_t)t.tile_hits;
+    a.substeps = (uint32_t)t.substeps;
     return a;
 }
 

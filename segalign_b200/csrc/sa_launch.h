@@ -108,7 +108,8 @@ struct SaTuning {
     int long_block;      // threads per CTA of the warp-per-hit kernel
     int range_ctas;      // CTAs of the range-partitioned kernels
     int tile_hits;       // hits per warp tile
-    int step_bases;      // bases a lane scores per step of the lane-per-hit kernel (8 or 16)
+    int step_bases;      // bases a lane scores per step of the lane-per-hit kernel (8, 16 or 32)
+    int substeps;        // steps a lane may take per iteration of the lane-per-hit kernel
 };
 
 // ---- sa_pack.cu ----

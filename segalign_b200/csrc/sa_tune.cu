@@ -13,6 +13,7 @@
 //   tile_hits        hits per warp tile held in shared memory
 //   lane_cap         bases a lane scans before a hit moves to a whole warp
 //   range_ctas       CTAs of the lookup, compaction and sort kernels
+//   substeps         steps a lane may take per lane-kernel iteration
 // Results are cached per GPU name and workload signature in a JSON-lines
 // file, so a later run applies them without a sweep.
 #include <cstdio>
@@ -38,6 +39,7 @@ const Knob kKnobs[] = {
     {"tile_hits", {96, 128, 160, 224, 320}, {128, 160, 224}},
     {"lane_cap", {1024, 2048, 4096, 8192}, {2048, 4096}},
     {"range_ctas", {148, 296, 592}, {296}},
+    {"substeps", {1, 2, 3, 4}, {1, 2}},
 };
 constexpr int kNumKnobs = sizeof(kKnobs) / sizeof(kKnobs[0]);
 
@@ -203,6 +205,7 @@ int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* c
     out->tile_hits = cur[2];
     out->lane_cap = cur[3];
     out->range_ctas = cur[4];
+    out->substeps = cur[5];
     return SA_OK;
 }
 

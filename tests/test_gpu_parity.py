@@ -108,18 +108,20 @@ def test_max_hits_iterations(setup, max_hits):
         sf.set_max_hits(0)
 
 
-@pytest.mark.parametrize("lane_cap,ctas,tile,step", [(8, 2, 64, 8), (16, 4, 1024, 16), (32, 4, 1024, 8),
-                                                     (64, 3, 100, 16), (512, 3, 1024, 8), (4096, 3, 256, 16),
-                                                     (512, 2, 1024, 16), (32, 3, 160, 32), (4096, 2, 64, 32)])
-def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step):
+@pytest.mark.parametrize("lane_cap,ctas,tile,step,sub", [(8, 2, 64, 8, 1), (16, 4, 1024, 16, 3), (32, 4, 1024, 8, 2),
+                                                         (64, 3, 100, 16, 1), (512, 3, 1024, 8, 4), (4096, 3, 256, 16, 2),
+                                                         (512, 2, 1024, 16, 8), (32, 3, 160, 32, 3), (4096, 2, 64, 32, 1),
+                                                         (8192, 3, 160, 32, 4)])
+def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step, sub):
     """Every tuning gives the same HSPs and extends every hit exactly once (tile counts)."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
     seeds = host_seeds(w.query, 250_000, 500_000)
     want, st = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
     saved = sf.get_tuning()
-    sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile, step_bases=step)
+    sf.set_tuning(lane_cap=lane_cap, ext_ctas_per_sm=ctas, tile_hits=tile, step_bases=step, substeps=sub)
     try:
-        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"lane_cap={lane_cap} ctas={ctas} step={step}")
+        compare_segments(sf.seed_and_filter(seeds, False, 0), want,
+                         f"lane_cap={lane_cap} ctas={ctas} step={step} substeps={sub}")
         assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
         sf.set_tuning(**saved)
