@@ -49,6 +49,9 @@ typedef struct {
     uint64_t num_hsps;
     uint64_t num_calls;
     double seconds;
+    double seed_seconds;  /* summed over threads: host seeding           */
+    double call_seconds;  /* summed over threads: sa_seed_and_filter     */
+    double copy_seconds;  /* summed over threads and the final assembly: HSP copies */
 } sa_seeder_stats;
 
 int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query_block, uint32_t query_len, sa_segment** fw,

@@ -23,6 +23,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import threading
+import weakref
 
 import numpy as np
 
@@ -137,7 +138,8 @@ RM_RUN_DTYPE = np.dtype([("block", "<u4"), ("interval", "<u4"), ("query_start", 
 
 class SeederStats(C.Structure):
     _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
-                ("num_calls", C.c_uint64), ("seconds", C.c_double)]
+                ("num_calls", C.c_uint64), ("seconds", C.c_double), ("seed_seconds", C.c_double),
+                ("call_seconds", C.c_double), ("copy_seconds", C.c_double)]
 
 
 _lib = None
@@ -260,13 +262,14 @@ def host_revcomp(text: bytes) -> bytes:
 
 
 def _take_segments(lib, ptr, n) -> np.ndarray:
-    try:
-        if n == 0:
-            return np.zeros(0, dtype=SEGMENT_DTYPE)
-        buf = C.cast(ptr, _P(C.c_uint8 * (16 * n))).contents
-        return np.frombuffer(bytes(buf), dtype=SEGMENT_DTYPE).copy()
-    finally:
+    """The library's malloc'd HSP array as a numpy array, without a copy: the
+    buffer is freed (sa_free_segments) when the array is garbage-collected."""
+    if n == 0:
         lib.sa_free_segments(ptr)
+        return np.zeros(0, dtype=SEGMENT_DTYPE)
+    raw = np.ctypeslib.as_array(C.cast(ptr, _P(C.c_uint8)), shape=(16 * n,))
+    weakref.finalize(raw, lib.sa_free_segments, C.cast(ptr, _P(C.c_uint8)))
+    return raw.view(SEGMENT_DTYPE)
 
 
 class SeedFilter:

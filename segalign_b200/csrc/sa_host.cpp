@@ -264,9 +264,19 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
         }
     }
     if (cfg->max_chunks && calls.size() > cfg->max_chunks) calls.resize(cfg->max_chunks);
-    std::vector<std::vector<sa_segment>> res(calls.size());
+    // each call's output array (header + HSPs), kept until the final assembly
+    struct CallOut {
+        sa_segment* p = nullptr;
+        uint64_t n = 0;  // HSPs (without the header)
+    };
+    std::vector<CallOut> res(calls.size());
     std::atomic<uint64_t> next{0}, nseeds{0}, nhits{0}, nhsps{0};
+    std::atomic<uint64_t> ns_seed{0}, ns_call{0}, ns_copy{0};
     std::atomic<int> err{0};
+    using SClock = std::chrono::steady_clock;
+    auto ns_since = [](SClock::time_point t) {
+        return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(SClock::now() - t).count();
+    };
     auto worker = [&]() {
         std::vector<uint64_t> seeds;
         while (!err) {
@@ -275,12 +285,16 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
             const Call& cl = calls[c];
             const char* txt = cl.strand ? rctext : query;
             const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
+            auto t_seed = SClock::now();
             seeds.resize((uint64_t)(cl.j1 - cl.j0) * per);
             const uint64_t need = chunk_seeds(g_shape, txt, cl.j0, cl.j1, seeds.data(), seeds.size());
+            ns_seed += ns_since(t_seed);
             if (need == 0) continue;  // src/seeder.cpp:190
             sa_segment* out = nullptr;
             uint64_t ol = 0;
+            auto t_call = SClock::now();
             int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, cfg->buffer, &out, &ol);
+            ns_call += ns_since(t_call);
             if (r != SA_OK) {
                 err = r;
                 break;
@@ -290,25 +304,52 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
             nseeds += need;
             nhits += cs.num_hits;
             nhsps += ol - 1;
-            res[c].assign(out + 1, out + ol);
-            sa_free_segments(out);
+            res[c].p = out;
+            res[c].n = ol - 1;
         }
     };
     int nt = std::max(1, cfg->num_threads);
     std::vector<std::thread> th;
     for (int t = 0; t < nt; ++t) th.emplace_back(worker);
     for (auto& t : th) t.join();
-    if (err) return err;
+    auto t_asm = SClock::now();
+    auto free_all = [&]() {
+        for (auto& r : res) sa_free_segments(r.p);
+    };
+    if (err) {
+        free_all();
+        return err;
+    }
+    // per strand, the calls' HSP lists concatenated in call order: offsets
+    // first, then the copies spread over the worker threads
     uint64_t nf = 0, nr = 0;
-    for (size_t c = 0; c < calls.size(); ++c) (calls[c].strand ? nr : nf) += res[c].size();
+    std::vector<uint64_t> at(calls.size());
+    for (size_t c = 0; c < calls.size(); ++c) {
+        uint64_t& n = calls[c].strand ? nr : nf;
+        at[c] = n;
+        n += res[c].n;
+    }
     *fw = (sa_segment*)malloc(sizeof(sa_segment) * (nf ? nf : 1));
     *rc = (sa_segment*)malloc(sizeof(sa_segment) * (nr ? nr : 1));
-    if (!*fw || !*rc) return SA_ERR_NOMEM;
-    uint64_t a = 0, b = 0;
-    for (size_t c = 0; c < calls.size(); ++c) {
-        sa_segment* dst = calls[c].strand ? *rc + b : *fw + a;
-        if (!res[c].empty()) std::memcpy(dst, res[c].data(), res[c].size() * sizeof(sa_segment));
-        (calls[c].strand ? b : a) += res[c].size();
+    if (!*fw || !*rc) {
+        free(*fw);
+        free(*rc);
+        free_all();
+        return SA_ERR_NOMEM;
+    }
+    {
+        std::atomic<size_t> nc{0};
+        auto copier = [&]() {
+            for (size_t c; (c = nc.fetch_add(1)) < calls.size();) {
+                if (res[c].n)
+                    std::memcpy((calls[c].strand ? *rc : *fw) + at[c], res[c].p + 1, res[c].n * sizeof(sa_segment));
+                sa_free_segments(res[c].p);
+                res[c].p = nullptr;
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t) th.emplace_back(copier);
+        for (auto& t : th) t.join();
     }
     *fw_len = nf;
     *rc_len = nr;
@@ -318,6 +359,9 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
         stats->num_hsps = nhsps;
         stats->num_calls = calls.size();
         stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        stats->seed_seconds = ns_seed * 1e-9;
+        stats->call_seconds = ns_call * 1e-9;
+        stats->copy_seconds = ns_copy * 1e-9 + std::chrono::duration<double>(SClock::now() - t_asm).count();
     }
     return SA_OK;
 }
