@@ -15,6 +15,7 @@
 #include <deque>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/segalign_b200.h"
@@ -572,11 +573,19 @@ void drop_keys(DevState& d, uint32_t buffer) {
         }
 }
 
+// Receives one completed group: units [u0, u0 + n) of the run (in order),
+// their records back to back in recs (cnt[i] each) and hit counts.
+struct BatchSink {
+    virtual ~BatchSink() = default;
+    virtual int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) = 0;
+};
+
 struct BatchResult {
-    std::vector<std::vector<SaRec>> recs;  // per unit (body only)
+    std::vector<std::vector<SaRec>> recs;  // per unit (body only), unless sink is set
     std::vector<uint64_t> hits;            // per unit
     SaCounters tot{};
     sa_call_stats timing{};
+    BatchSink* sink = nullptr;  // records go here instead of recs
 };
 
 // Runs units [u0, u1) in one device pass.  Returns SA_ERR_CAPACITY when the
@@ -671,9 +680,10 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     tm.mark(5);
     SA_CUDA_OK(cudaStreamSynchronize(st));
     tm.collect(res.timing);
+    for (uint32_t i = 0; i < n; ++i) res.hits[u0 + i] = he[i] - hb[i];
+    if (want_out && res.sink) return res.sink->put(u0, n, s->h_out, cnt.data(), res.hits.data() + u0);
     uint64_t at = 0;
     for (uint32_t i = 0; i < n; ++i) {
-        res.hits[u0 + i] = he[i] - hb[i];
         if (want_out) res.recs[u0 + i].assign(s->h_out + at, s->h_out + at + cnt[i]);
         at += cnt[i];
     }
@@ -734,10 +744,97 @@ int run_resolved(const SaResolvedUnit* units, uint32_t n, bool want_out, BatchRe
             map[i] = (int64_t)live.size();
             live.push_back(units[i]);
         }
-    res.recs.resize(live.size());
+    if (!res.sink) res.recs.resize(live.size());
     res.hits.assign(live.size(), 0);
     return run_batch_range(d, d.batch, live.data(), 0, (uint32_t)live.size(), want_out, res);
 }
+
+// Output of sa_seed_and_filter_batch, written as groups complete: per unit a
+// header record {0, 0, HSP count, hit count} then its HSPs; a unit with an
+// empty window gets its header only.  One malloc'd block (grown by realloc,
+// which remaps rather than copies at these sizes), freed by sa_free_segments.
+struct SegmentWriter : BatchSink {
+    const uint64_t n_units;
+    uint64_t* offsets;
+    std::vector<uint32_t> orig;  // live unit -> unit index
+    sa_segment* o = nullptr;
+    uint64_t cap = 0, at = 0;
+    uint32_t next = 0;  // next unit to get a header
+
+    SegmentWriter(const sa_unit* units, uint32_t n, uint64_t* offs) : n_units(n), offsets(offs) {
+        for (uint32_t i = 0; i < n; ++i)
+            if (units[i].end > units[i].start) orig.push_back(i);
+    }
+    ~SegmentWriter() override { free(o); }
+
+    sa_segment* release() {
+        sa_segment* p = o;
+        o = nullptr;
+        return p;
+    }
+
+    int reserve(uint64_t need) {
+        if (need <= cap) return SA_OK;
+        uint64_t c = std::max<uint64_t>(need, cap + cap / 2);
+        void* p = realloc(o, sizeof(sa_segment) * c);
+        if (!p) {
+            sa_set_error(SA_ERR_NOMEM, "cannot hold %llu HSP records", (unsigned long long)c);
+            return SA_ERR_NOMEM;
+        }
+        o = (sa_segment*)p;
+        cap = c;
+        return SA_OK;
+    }
+
+    void header(uint32_t nb, uint64_t hits) {
+        offsets[next++] = at;
+        o[at++] = sa_segment{0, 0, nb, (int32_t)(uint32_t)hits};
+    }
+
+    int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) override {
+        if (!n) return SA_OK;
+        uint64_t body = 0;
+        for (uint32_t i = 0; i < n; ++i) body += cnt[i];
+        SA_TRY(reserve(at + body + (orig[u0 + n - 1] + 1 - next)));
+        std::vector<uint64_t> dst(n), src(n);
+        uint64_t s = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            while (next < orig[u0 + i]) header(0, 0);
+            header(cnt[i], hits[i]);
+            dst[i] = at;
+            src[i] = s;
+            at += cnt[i];
+            s += cnt[i];
+        }
+        // copy the bodies, units split over up to 8 threads by record count
+        auto copy = [&](uint32_t a, uint32_t b) {
+            for (uint32_t i = a; i < b; ++i)
+                if (cnt[i]) std::memcpy(o + dst[i], recs + src[i], cnt[i] * sizeof(sa_segment));
+        };
+        const uint64_t kPer = 2u << 20;  // records per thread, at least
+        const uint32_t nt = (uint32_t)std::min<uint64_t>({8, n, body / kPer});
+        if (nt < 2) {
+            copy(0, n);
+            return SA_OK;
+        }
+        std::vector<uint32_t> cut(nt + 1, n);
+        cut[0] = 0;
+        for (uint32_t i = 0, t = 1; i < n && t < nt; ++i)
+            if (src[i] + cnt[i] >= body * t / nt) cut[t++] = i + 1;
+        std::vector<std::thread> th;
+        for (uint32_t t = 1; t < nt; ++t) th.emplace_back(copy, cut[t], cut[t + 1]);
+        copy(cut[0], cut[1]);
+        for (auto& x : th) x.join();
+        return SA_OK;
+    }
+
+    int finish() {
+        SA_TRY(reserve(at + (n_units - next) + 1));
+        while (next < n_units) header(0, 0);
+        offsets[n_units] = at;
+        return SA_OK;
+    }
+};
 
 }  // namespace
 
@@ -1216,6 +1313,8 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
     }
     BatchResult res;
     std::vector<int64_t> map;
+    SegmentWriter wr(units, n_units, offsets);
+    if (out) res.sink = &wr;
     SA_TRY(run_resolved(ru.data(), n_units, out != nullptr, res, map));
     std::memset(&t_stats, 0, sizeof t_stats);
     t_stats.num_hits = res.tot.num_hits;
@@ -1233,27 +1332,9 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
     t_stats.ms_dedup = res.timing.ms_dedup;
     t_stats.ms_copy = res.timing.ms_copy;
     if (!out) return SA_OK;
-    uint64_t total = n_units;
-    for (auto& r : res.recs) total += r.size();
-    sa_segment* o = (sa_segment*)malloc(sizeof(sa_segment) * (total ? total : 1));
-    if (!o) return SA_ERR_NOMEM;
-    uint64_t at = 0;
-    for (uint32_t i = 0; i < n_units; ++i) {
-        offsets[i] = at;
-        const int64_t k = map[i];
-        const uint64_t nb = k >= 0 ? res.recs[k].size() : 0;
-        const uint64_t hits = k >= 0 ? res.hits[k] : 0;
-        o[at].ref_start = 0;
-        o[at].query_start = 0;
-        o[at].len = (uint32_t)nb;
-        o[at].score = (int32_t)(uint32_t)hits;
-        ++at;
-        if (nb) std::memcpy(o + at, res.recs[k].data(), nb * sizeof(sa_segment));
-        at += nb;
-    }
-    offsets[n_units] = at;
-    *out = o;
-    *out_len = at;
+    SA_TRY(wr.finish());
+    *out_len = wr.at;
+    *out = wr.release();
     return SA_OK;
 }
 
