@@ -573,19 +573,12 @@ void drop_keys(DevState& d, uint32_t buffer) {
         }
 }
 
-// Receives one completed group: units [u0, u0 + n) of the run (in order),
-// their records back to back in recs (cnt[i] each) and hit counts.
-struct BatchSink {
-    virtual ~BatchSink() = default;
-    virtual int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) = 0;
-};
-
 struct BatchResult {
     std::vector<std::vector<SaRec>> recs;  // per unit (body only), unless sink is set
     std::vector<uint64_t> hits;            // per unit
     SaCounters tot{};
     sa_call_stats timing{};
-    BatchSink* sink = nullptr;  // records go here instead of recs
+    SaBatchSink* sink = nullptr;  // records go here instead of recs
 };
 
 // Runs units [u0, u1) in one device pass.  Returns SA_ERR_CAPACITY when the
@@ -753,7 +746,7 @@ int run_resolved(const SaResolvedUnit* units, uint32_t n, bool want_out, BatchRe
 // header record {0, 0, HSP count, hit count} then its HSPs; a unit with an
 // empty window gets its header only.  One malloc'd block (grown by realloc,
 // which remaps rather than copies at these sizes), freed by sa_free_segments.
-struct SegmentWriter : BatchSink {
+struct SegmentWriter : SaBatchSink {
     const uint64_t n_units;
     uint64_t* offsets;
     std::vector<uint32_t> orig;  // live unit -> unit index
@@ -1358,15 +1351,16 @@ int sa_run_units(const SaResolvedUnit* units, uint32_t n, bool want_out, SaRunRe
     Global& g = G();
     std::lock_guard<std::mutex> lk(g.batch_mu);
     BatchResult res;
+    res.sink = out->sink;
     std::vector<int64_t> map;
     r = run_resolved(units, n, want_out, res, map);
     if (r != SA_OK) return r;
-    out->recs->assign(n, {});
+    if (!out->sink) out->recs->assign(n, {});
     out->hits->assign(n, 0);
     for (uint32_t i = 0; i < n; ++i)
         if (map[i] >= 0) {
             (*out->hits)[i] = res.hits[map[i]];
-            if (want_out) (*out->recs)[i] = std::move(res.recs[map[i]]);
+            if (want_out && !out->sink) (*out->recs)[i] = std::move(res.recs[map[i]]);
         }
     out->tot = res.tot;
     out->ms_total = res.timing.ms_total;

@@ -39,12 +39,22 @@ struct SaResolvedUnit {
     int32_t rev;
 };
 
+// Receives the output of one completed device group of a batched run:
+// units [u0, u0 + n) of the run's non-empty units, in order, their HSP
+// records back to back in recs (cnt[i] each) and their hit counts.  Groups
+// arrive in unit order.  recs is valid only during the call.
+struct SaBatchSink {
+    virtual ~SaBatchSink() = default;
+    virtual int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) = 0;
+};
+
 struct SaRunResult {
-    // per unit: HSP records (body) and hits
+    // per unit: HSP records (body) and hits; recs stays empty when sink is set
     std::vector<std::vector<SaRec>>* recs;
     std::vector<uint64_t>* hits;
     SaCounters tot;
     double ms_total, ms_lookup, ms_extend_lane, ms_extend_warp, ms_dedup, ms_copy;
+    SaBatchSink* sink;  // optional: records go here as groups complete
 };
 
 // Runs resolved units on GPU 0's batch workspace (one batch at a time).

@@ -15,8 +15,11 @@
 // cuts a query block (src/main.cpp:373-386, src/seeder.cpp:47-121), and the
 // batched path gives each unit the same HSP list as a plain SeedAndFilter
 // call, so a request's result does not depend on what it was batched with.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -37,9 +40,32 @@ struct ServeUnit {
     uint32_t j0, j1;
 };
 
+// One strand's HSP list of a request: a malloc'd array grown as the request's
+// units complete (in unit order), handed to the caller as is.
+struct SegBuf {
+    sa_segment* p = nullptr;
+    uint64_t n = 0, cap = 0;
+    SegBuf() = default;
+    SegBuf(const SegBuf&) = delete;
+    SegBuf& operator=(const SegBuf&) = delete;
+    ~SegBuf() { free(p); }
+    bool append(const SaRec* r, uint64_t k) {
+        if (n + k > cap) {
+            const uint64_t c = std::max<uint64_t>(n + k, std::max<uint64_t>(1024, cap + cap / 2));
+            void* q = realloc(p, c * sizeof(sa_segment));
+            if (!q) return false;
+            p = (sa_segment*)q;
+            cap = c;
+        }
+        if (k) std::memcpy(p + n, r, k * sizeof(sa_segment));
+        n += k;
+        return true;
+    }
+};
+
 struct Request {
     uint64_t id = 0;
-    std::vector<char> text;
+    std::vector<char> text;  // until admitted
     uint32_t len = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
     void* dmem = nullptr;  // one stream-ordered allocation
@@ -49,11 +75,10 @@ struct Request {
     std::vector<ServeUnit> units;
     size_t next_unit = 0;   // first unit not yet given to a pass
     size_t done_units = 0;
-    std::vector<std::vector<SaRec>> recs;  // per unit
     uint64_t hits = 0, passes = 0, hsps = 0;
     int status = SA_OK;
     bool done = false;
-    std::vector<SaRec> out[2];  // per strand, when done
+    SegBuf out[2];  // per strand; written by the runner only, read once done
 };
 
 struct Server {
@@ -70,6 +95,7 @@ struct Server {
     std::map<uint64_t, std::shared_ptr<Request>> all;
     cudaStream_t admit_stream = nullptr, free_stream = nullptr;
     std::thread admitter, runner;
+    bool trace = false;  // SA_SERVE_TRACE=1: one stderr line per pass and per request build
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -161,17 +187,8 @@ int build_request(Server& sv, Request& r) {
     return SA_OK;
 }
 
-// Completes a request (lock held): per-strand lists, buffers released.
+// Completes a request (lock held): device buffers released.
 void finish(Server& sv, Request& r, int status) {
-    if (status == SA_OK) {
-        for (size_t i = 0; i < r.units.size(); ++i) {
-            auto& dst = r.out[r.units[i].strand];
-            dst.insert(dst.end(), r.recs[i].begin(), r.recs[i].end());
-            r.hsps += r.recs[i].size();
-        }
-    }
-    r.recs.clear();
-    r.recs.shrink_to_fit();
     if (r.dmem) {
         cudaFreeAsync(r.dmem, sv.free_stream);
         r.dmem = nullptr;
@@ -194,7 +211,11 @@ void admitter_loop(Server& sv) {
         sv.queued.pop_front();
         sv.in_use += r->dbytes;
         lk.unlock();
+        const double t_build = sv.now();
         int st = build_request(sv, *r);
+        if (sv.trace)
+            std::fprintf(stderr, "[sa_serve] build %.4f-%.4f s: request %llu, %u bases, status %d\n", t_build, sv.now(),
+                         (unsigned long long)r->id, r->len, st);
         lk.lock();
         r->text.clear();
         r->text.shrink_to_fit();
@@ -209,6 +230,27 @@ void admitter_loop(Server& sv) {
         sv.cv_run.notify_all();
     }
 }
+
+// Appends each unit's HSPs of a completed device group to its request's
+// strand list (units of a request run in order, so the lists stay in seeder
+// order); called on the runner thread.
+struct PassSink : SaBatchSink {
+    const std::vector<std::pair<std::shared_ptr<Request>, size_t>>& owner;
+    explicit PassSink(const std::vector<std::pair<std::shared_ptr<Request>, size_t>>& o) : owner(o) {}
+    int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t*) override {
+        uint64_t at = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            Request& r = *owner[u0 + i].first;
+            if (!r.out[r.units[owner[u0 + i].second].strand].append(recs + at, cnt[i])) {
+                sa_set_error(SA_ERR_NOMEM, "cannot hold the HSP list of request %llu", (unsigned long long)r.id);
+                return SA_ERR_NOMEM;
+            }
+            r.hsps += cnt[i];
+            at += cnt[i];
+        }
+        return SA_OK;
+    }
+};
 
 void runner_loop(Server& sv) {
     cudaSetDevice(sv.view.dev);
@@ -246,12 +288,19 @@ void runner_loop(Server& sv) {
             if (full) break;
         }
         lk.unlock();
-        std::vector<std::vector<SaRec>> recs;
+        // every unit is non-empty (cut_units), so the batched path's group
+        // indices are indices into `units` and `owner`
         std::vector<uint64_t> hits;
+        PassSink sink(owner);
         SaRunResult res{};
-        res.recs = &recs;
         res.hits = &hits;
+        res.sink = &sink;
+        const double t_pass = sv.now();
         const int st = sa_run_units(units.data(), (uint32_t)units.size(), true, &res);
+        if (sv.trace)
+            std::fprintf(stderr, "[sa_serve] pass %.4f-%.4f s: %zu units, %llu slots, %llu hits, device %.2f ms, status %d\n",
+                         t_pass, sv.now(), units.size(), (unsigned long long)slots,
+                         (unsigned long long)res.tot.num_hits, res.ms_total, st);
         lk.lock();
         for (size_t i = 0; i < owner.size(); ++i) {
             Request& r = *owner[i].first;
@@ -260,7 +309,6 @@ void runner_loop(Server& sv) {
                 finish(sv, r, st);
                 continue;
             }
-            r.recs[owner[i].second] = std::move(recs[i]);
             r.hits += hits[i];
             if (++r.done_units == r.units.size()) finish(sv, r, SA_OK);
         }
@@ -300,6 +348,8 @@ int sa_serve_start(const sa_serve_cfg* cfg) {
     sv->budget = free_b > sv->cfg.hbm_reserve ? free_b - sv->cfg.hbm_reserve : 0;
     SA_CUDA_OK(cudaStreamCreateWithFlags(&sv->admit_stream, cudaStreamNonBlocking));
     SA_CUDA_OK(cudaStreamCreateWithFlags(&sv->free_stream, cudaStreamNonBlocking));
+    const char* tr = std::getenv("SA_SERVE_TRACE");
+    sv->trace = tr && *tr && *tr != '0';
     sv->t0 = Clock::now();
     Server* p = sv.get();
     sv->admitter = std::thread(admitter_loop, std::ref(*p));
@@ -319,7 +369,6 @@ int sa_serve_submit(const char* query, uint32_t len, uint64_t* request_id) {
     r->len = len;
     r->text.assign(query, query + len);
     r->units = cut_units(len, sv->cfg, (uint32_t)sv->view.params.seed_size);
-    r->recs.resize(r->units.size());
     r->dbytes = request_bytes(len, sv->cfg.strands);
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->stop) return SA_ERR_STATE;
@@ -380,16 +429,16 @@ int sa_serve_wait(uint64_t request_id, int timeout_ms, sa_segment** fw, uint64_t
         sa_set_error(r->status, "request %llu failed", (unsigned long long)request_id);
         return r->status;
     }
+    // the lists are handed over without a copy (freed by sa_free_segments)
+    for (int s = 0; s < 2; ++s)
+        if (!r->out[s].p && !(r->out[s].p = (sa_segment*)malloc(sizeof(sa_segment)))) return SA_ERR_NOMEM;
+    *fw = r->out[0].p;
+    *fw_len = r->out[0].n;
+    *rc = r->out[1].p;
+    *rc_len = r->out[1].n;
     for (int s = 0; s < 2; ++s) {
-        const std::vector<SaRec>& v = r->out[s];
-        sa_segment* o = (sa_segment*)malloc(sizeof(sa_segment) * (v.empty() ? 1 : v.size()));
-        if (!o) {
-            if (s == 1) free(*fw);
-            return SA_ERR_NOMEM;
-        }
-        if (!v.empty()) std::memcpy(o, v.data(), v.size() * sizeof(sa_segment));
-        (s == 0 ? *fw : *rc) = o;
-        (s == 0 ? *fw_len : *rc_len) = v.size();
+        r->out[s].p = nullptr;
+        r->out[s].n = r->out[s].cap = 0;
     }
     return SA_OK;
 }
