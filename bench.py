@@ -510,8 +510,11 @@ def run_ours(args):
         out["e2e"] = {"value": e2e_hits / e2e_s_max, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                       "d2h_bytes_per_step": int(d2h), "path": f"sa_seed_and_filter per 250 kbp unit from "
                       f"{e2e_threads} host threads (C++ seeder), host wall time", "steps": k_e2e}
-        # batched with host buffers: query text up, HSP lists down
+        # batched with host buffers: query text up, HSP lists down (one untimed
+        # step first: it sizes the pinned output buffer)
         sf.set_timing(True)
+        sf.send_query_write_request(w.query, 1)
+        sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
         barrier()
         t0 = time.perf_counter()
         outs = None

@@ -437,7 +437,8 @@ class SeedFilter:
         self._chk(self.lib.sa_set_tuning(lane_cap, ext_block, ext_ctas_per_sm, tile_hits), "set_tuning")
 
     def get_tuning(self) -> dict:
-        names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas", "substeps")
+        names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas", "substeps", "call_range_ctas",
+                 "call_lane_ctas")
         return {n: int(self.lib.sa_get_tuning_param(n.encode())) for n in names}
 
     def set_timing(self, on: bool) -> None:

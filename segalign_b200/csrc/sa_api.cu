@@ -153,7 +153,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 1};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 2, 148, 0};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -381,7 +381,7 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     DevState& d = g.devs[s->dev_idx];
     SaWork& w = s->w;
     cudaStream_t st = s->stream;
-    const int Gr = std::min(g.tuning.range_ctas, SA_MAX_CTAS);
+    const int Gr = std::min(g.tuning.call_range_ctas, SA_MAX_CTAS);
     SA_CUDA_OK(cudaMemcpyAsync(w.desc, s->h_desc, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.units, s->h_units, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
@@ -397,7 +397,9 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     xa.xdrop = g.params.xdrop;
     xa.hspthresh = g.params.hspthresh;
     xa.noentropy = g.params.noentropy;
-    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st);
+    const int lane_grid = g.tuning.call_lane_ctas > 0 ? g.tuning.call_lane_ctas
+                                                     : std::max(1, d.num_sms * g.tuning.ext_ctas_per_sm / 2);
+    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st, lane_grid);
     tm.mark(2);
     sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
     tm.mark(3);
@@ -1426,9 +1428,21 @@ int sa_set_tuning_param(const char* name, int value) {
         t.step_bases = value;
         return SA_OK;
     }
-    if (n == "range_ctas") {
-        if (value < 1 || value > SA_MAX_CTAS) return SA_ERR_ARG;
-        t.range_ctas = value;
+    if (n == "range_ctas" || n == "call_range_ctas") {
+        if (value < 1 || value > SA_MAX_CTAS) {
+            sa_set_error(SA_ERR_ARG, "%s must be 1..%d (got %d)", name, SA_MAX_CTAS, value);
+            return SA_ERR_ARG;
+        }
+        (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
+        return SA_OK;
+    }
+    if (n == "call_lane_ctas") {
+        if (value < 0 || value > 8 * SA_MAX_CTAS) {
+            sa_set_error(SA_ERR_ARG, "call_lane_ctas must be 0 (half the batched grid) .. %d (got %d)",
+                         8 * SA_MAX_CTAS, value);
+            return SA_ERR_ARG;
+        }
+        t.call_lane_ctas = value;
         return SA_OK;
     }
     if (n == "substeps") {
@@ -1453,6 +1467,8 @@ int sa_get_tuning_param(const char* name) {
     if (n == "step_bases") return t.step_bases;
     if (n == "substeps") return t.substeps;
     if (n == "range_ctas") return t.range_ctas;
+    if (n == "call_range_ctas") return t.call_range_ctas;
+    if (n == "call_lane_ctas") return t.call_lane_ctas;
     return SA_ERR_ARG;
 }
 

@@ -839,11 +839,11 @@ void sa_prepare_extend_lane(const SaParams& p, const SaTuning& t) {
 }
 
 void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, const SaTuning& t, int num_sms,
-                           cudaStream_t st) {
+                           cudaStream_t st, int grid_ctas) {
     sa_prepare_extend_lane(p, t);
     // Register budget follows the CTAs per SM: 4 -> <= 64 registers, 3 -> <= 85, 2 -> <= 128.
     const SaExtK a = sa_ext_args(w, x, t);
-    const int grid = num_sms * t.ext_ctas_per_sm;
+    const int grid = grid_ctas > 0 ? grid_ctas : num_sms * t.ext_ctas_per_sm;
     const size_t smem = sa_lane_smem(a.tile_hits);
     const bool exact = !sa_lane_fast_form(p, t.step_bases);
     if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, grid, smem, st);

@@ -120,6 +120,11 @@ struct SaTuning {
     int tile_hits;       // hits per warp tile
     int step_bases;      // bases a lane scores per step of the lane-per-hit kernel (8, 16 or 32)
     int substeps;        // steps a lane may take per iteration of the lane-per-hit kernel
+    int call_range_ctas; // CTAs of the range-partitioned kernels of a plain or rm call (at most
+                         // MAX_SEEDS seed words: fewer CTAs than a batch needs)
+    int call_lane_ctas;  // CTAs of a plain or rm call's lane kernel; 0: half of the batched
+                         // grid, so that concurrent calls' kernels share the SMs and fill
+                         // each other's ramp-up and tail instead of queueing
 };
 
 // ---- sa_pack.cu ----
@@ -154,8 +159,9 @@ struct SaExtendArgs {
     int32_t xdrop, hspthresh, noentropy;
 };
 // Phase A (lane per hit) and phase B (warp per long hit); B must follow A.
+// grid: CTAs of the persistent launch (0: num_sms x ext_ctas_per_sm).
 void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
-                           int num_sms, cudaStream_t st);
+                           int num_sms, cudaStream_t st, int grid = 0);
 void sa_launch_extend_warp(SaWork& w, const SaExtendArgs& a, const SaParams& p, const SaTuning& t,
                            int num_sms, cudaStream_t st);
 

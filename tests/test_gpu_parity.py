@@ -127,6 +127,22 @@ def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step, sub):
         sf.set_tuning(**saved)
 
 
+@pytest.mark.parametrize("lane_ctas,range_ctas", [(1, 1), (37, 16), (148, 148), (1000, 1024)])
+def test_call_grid_knobs_do_not_change_results(setup, lane_ctas, range_ctas):
+    """A plain call's lane-kernel grid and range-kernel grid (down to one CTA,
+    and above the resident limit) give the same HSPs and tile counts."""
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    seeds = host_seeds(w.query, 500_000, 700_000)
+    want, st = oracle.seed_and_filter(p, setup["R"], setup["Q"], setup["idx"], setup["pos"], seeds, False)
+    saved = sf.get_tuning()
+    sf.set_tuning(call_lane_ctas=lane_ctas, call_range_ctas=range_ctas)
+    try:
+        compare_segments(sf.seed_and_filter(seeds, False, 0), want, f"call_lane_ctas={lane_ctas}")
+        assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
+    finally:
+        sf.set_tuning(**saved)
+
+
 def test_host_table_upload(setup):
     w, p, sf = setup["w"], setup["p"], setup["sf"]
     sf.send_seed_pos_table(setup["idx"], setup["pos"])

@@ -33,12 +33,15 @@ def test_autotune_keeps_results_and_caches(sf, tmp_path):
     assert res["candidates"] > 0 and res["rejected"] == 0 and res["from_cache"] == 0
     assert res["ms_best"] <= res["ms_start"]
     tuned = sf.get_tuning()
-    for k in DEFAULT:
+    knobs = [k for k in DEFAULT if k in res]  # the batched path's knobs (not call_range_ctas)
+    assert len(knobs) == 6
+    for k in knobs:
         assert tuned[k] == res[k], k
+    assert tuned["call_range_ctas"] == DEFAULT["call_range_ctas"]
     for u, (g, x) in enumerate(zip(sf.seed_and_filter_batch(units), want)):
         compare_segments(g, x, f"unit {u} after tuning")
     sf.set_tuning(**DEFAULT)
     again = sf.autotune(units, cache_path=cache, quick=True, repeats=1)
     assert again["from_cache"] == 1 and again["candidates"] == 0
-    assert {k: again[k] for k in DEFAULT} == {k: res[k] for k in DEFAULT}
+    assert {k: again[k] for k in knobs} == {k: res[k] for k in knobs}
     assert open(cache).read().count("\n") == 1
