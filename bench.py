@@ -96,6 +96,16 @@ def lane_traffic(hits: float, workload: str):
     return per_hit * hits, f"ncu dram bytes per hit of {d['workload']} x this launch's hits"
 
 
+def lane_limit(workload: str):
+    """The lane kernel's measured issue-bound limit (ncu full capture) recorded
+    beside its DRAM traffic in profiles/extend_lane_dram.json, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "extend_lane_dram.json")) as f:
+            return json.load(f)[workload].get("issue")
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -409,7 +419,7 @@ def run_ours(args):
     sf = SeedFilter()
     sf.initialize_interface(1)
     sf.generate_shape_pos("12of19")
-    os.environ.setdefault("SA_SLOTS_PER_GPU", "8")  # concurrent plain calls per GPU (e2e leg)
+    os.environ.setdefault("SA_SLOTS_PER_GPU", "12")  # concurrent plain calls per GPU (e2e leg)
     sf.initialize_processor(transition, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
     sf.send_ref_write_request(w.target)
     t = time.perf_counter()
@@ -465,7 +475,8 @@ def run_ours(args):
     traffic, traffic_src = lane_traffic(hits, args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_source": traffic_src, "kernel": "sa_k_extend_lane",
-                "peak_source": peak_src, "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg}
+                "peak_source": peak_src, "alg_bytes_per_launch": alg_bytes, "launch_ms": lane_ms_avg,
+                "limit": lane_limit(args.workload)}
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
