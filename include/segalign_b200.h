@@ -239,7 +239,9 @@ typedef struct {
     uint64_t long_hits;      /* hits finished by the warp-per-hit kernel       */
     uint64_t tiles;          /* 32-base tiles the reference would scan          */
     uint32_t num_iter;       /* MAX_HITS iterations                            */
-    uint32_t pad;
+    uint32_t batch_calls;    /* calls that shared the device pass (call coalescing);
+                              * above 1, hits_extended, seeds_with_hits, survivors,
+                              * long_hits, tiles and the ms_* times are the pass's */
     /* device time of the call's phases (CUDA events on the call's stream),
      * filled when sa_set_timing(1) is on */
     double ms_total, ms_lookup, ms_extend_lane, ms_extend_warp, ms_dedup, ms_copy;

@@ -63,7 +63,7 @@ class SegAlignError(RuntimeError):
 class CallStats(C.Structure):
     _fields_ = [("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("hits_extended", C.c_uint64),
                 ("seeds_with_hits", C.c_uint64), ("survivors", C.c_uint64), ("num_hsps", C.c_uint64),
-                ("long_hits", C.c_uint64), ("tiles", C.c_uint64), ("num_iter", C.c_uint32), ("pad", C.c_uint32),
+                ("long_hits", C.c_uint64), ("tiles", C.c_uint64), ("num_iter", C.c_uint32), ("batch_calls", C.c_uint32),
                 ("ms_total", C.c_double), ("ms_lookup", C.c_double), ("ms_extend_lane", C.c_double),
                 ("ms_extend_warp", C.c_double), ("ms_dedup", C.c_double), ("ms_copy", C.c_double)]
 

@@ -108,6 +108,22 @@ struct Slot {
     uint64_t graph_key = 0;
     uint64_t graph_kernels = 0;
     bool graph_off = false;  // capture failed once: launch directly
+    uint32_t max_units = 64;  // units per batched pass (batched kinds)
+};
+
+// A queued plain call (call coalescing): its inputs, then its result.
+struct CallReq {
+    const uint64_t* seeds = nullptr;  // the caller's words, copied to `staged` before queueing
+    uint64_t* staged = nullptr;       // pinned copy of the words
+    uint32_t n = 0;
+    int rev = 0;
+    uint32_t buffer = 0;
+    bool taken = false, done = false;  // taken into a pass; result ready (both under Global::mu)
+    int status = SA_OK;
+    std::string err;
+    sa_segment* out = nullptr;
+    uint64_t out_len = 0;
+    sa_call_stats stats{};
 };
 
 // Phase timing with CUDA events on the slot stream (enabled by sa_set_timing).
@@ -163,6 +179,12 @@ struct Global {
     uint64_t long_cap = 0;
     uint64_t batch_slot_cap = 0;
     uint64_t batch_surv_cap = 0;
+    // call coalescing: calls per pass (0 = every call runs alone), queued calls,
+    // and pinned staging buffers of max_seeds words for the callers' seeds
+    uint32_t coalesce_calls = 0;
+    std::deque<CallReq*> pending;
+    std::mutex pinned_mu;
+    std::vector<uint64_t*> pinned_free, pinned_all;
 };
 
 Global& G() {
@@ -250,8 +272,14 @@ void free_slot(Slot* s) {
 }
 
 // Carves one slot workspace out of a single device allocation.
+// Workspace kinds: plain calls (host seed words), batched passes (device
+// seeding over query windows), or both (passes of coalesced plain calls, and
+// plain calls one at a time), with at most `units` units per pass.
+enum SlotKind { kSlotPlain = 0, kSlotBatch = 1, kSlotBoth = 2 };
+
 int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_cap, Slot** out,
-              bool batch = false) {
+              SlotKind kind = kSlotPlain, uint64_t units = SA_MAX_UNITS) {
+    const bool batch = kind != kSlotPlain, host_seeds = kind != kSlotBatch;
     DevState& d = G().devs[dev_idx];
     SA_CUDA_OK(cudaSetDevice(d.dev));
     Slot* s = new Slot();
@@ -264,12 +292,13 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
     w.seed_cap = seed_cap;
     w.surv_cap = surv_cap;
     w.long_cap = long_cap;
-    const uint64_t nunits = batch ? SA_MAX_UNITS : 64;
+    const uint64_t nunits = batch ? std::max<uint64_t>(64, std::min<uint64_t>(units, SA_MAX_UNITS)) : 64;
+    s->max_units = (uint32_t)nunits;
     std::vector<Part> parts = {
-        {(void**)&w.seeds, batch ? 0 : 8 * seed_cap},
+        {(void**)&w.seeds, host_seeds ? 8 * seed_cap : 0},
         {(void**)&w.s_lo, 4 * seed_cap},
         {(void**)&w.s_cnt, 4 * seed_cap},
-        {(void**)&w.s_P, batch ? 0 : 8 * seed_cap},
+        {(void**)&w.s_P, host_seeds ? 8 * seed_cap : 0},
         {(void**)&w.cs.E, 8 * (seed_cap + 1)},
         {(void**)&w.cs.lo, 4 * (seed_cap + 1)},
         {(void**)&w.cs.qpos, 4 * (seed_cap + 1)},
@@ -350,7 +379,7 @@ void release_slot(Slot* s) {
         std::lock_guard<std::mutex> lk(g.mu);
         g.free_slots.push_back(s);
     }
-    g.cv.notify_one();
+    g.cv.notify_all();  // waiters for a slot and coalesced callers share the condition
 }
 
 int map_device_error(unsigned long long e) {
@@ -495,6 +524,7 @@ int run_call(Slot* s, const uint64_t* seeds, uint32_t n, int rev, const Packed& 
     t_stats.long_hits = c.long_count;
     t_stats.tiles = c.base_steps;
     t_stats.num_iter = (uint32_t)c.num_iter;
+    t_stats.batch_calls = 1;
     if (c.error) return map_device_error(c.error);
     const uint64_t nh = c.uniq_count;
     if (nh + 1 > s->h_out_cap) {
@@ -578,6 +608,7 @@ void drop_keys(DevState& d, uint32_t buffer) {
 struct BatchResult {
     std::vector<std::vector<SaRec>> recs;  // per unit (body only), unless sink is set
     std::vector<uint64_t> hits;            // per unit
+    std::vector<uint32_t> iters;           // per unit: MAX_HITS iterations
     SaCounters tot{};
     sa_call_stats timing{};
     SaBatchSink* sink = nullptr;  // records go here instead of recs
@@ -602,13 +633,14 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
         bu[i].q_start = u.start;
         bu[i].q_end = u.end;
         bu[i].keys = u.keys;
+        bu[i].seeds = u.seeds;
         bu[i].unit = i;
         bu[i].pad = 0;
         hu[i].q_packed = u.q_packed;
         hu[i].q_len = u.q_len;
         hu[i].rm_lo = hu[i].rm_hi = 0;
         hu[i].flags = 0;
-        slots += (uint64_t)(u.end - u.start) * S;
+        slots += sa_unit_slots(u, S);
     }
     SaCallDesc* hd = s->h_desc;
     hd->num_seeds = slots;
@@ -659,6 +691,8 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     res.tot.base_steps += c.base_steps;
     std::vector<unsigned long long> hb(n), he(n);
     std::vector<uint32_t> cnt(n);
+    if (res.iters.size() >= u1)
+        SA_CUDA_OK(cudaMemcpyAsync(res.iters.data() + u0, w.unit_iters, 4ull * n, cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaMemcpyAsync(hb.data(), w.unit_hit_base, 8ull * n, cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaMemcpyAsync(he.data(), w.unit_hit_end, 8ull * n, cudaMemcpyDeviceToHost, st));
     SA_CUDA_OK(cudaMemcpyAsync(cnt.data(), w.scope_count, 4ull * n, cudaMemcpyDeviceToHost, st));
@@ -695,7 +729,7 @@ int run_batch_range(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
         uint32_t b = a;
         uint64_t slots = 0;
         while (b < u1 && b - a < SA_MAX_UNITS) {
-            uint64_t add = (uint64_t)(units[b].end - units[b].start) * S;
+            uint64_t add = sa_unit_slots(units[b], S);
             if (b > a && slots + add > s->w.seed_cap) break;
             if (add > s->w.seed_cap) {
                 sa_set_error(SA_ERR_CAPACITY, "one unit needs %llu seed slots (capacity %llu, SA_BATCH_SLOT_CAP)",
@@ -729,7 +763,7 @@ int run_resolved(const SaResolvedUnit* units, uint32_t n, bool want_out, BatchRe
     DevState& d = g.devs[0];
     if (!d.batch) {
         Slot* s = nullptr;
-        SA_TRY(make_slot(0, g.batch_slot_cap, g.batch_surv_cap, g.long_cap, &s, true));
+        SA_TRY(make_slot(0, g.batch_slot_cap, g.batch_surv_cap, g.long_cap, &s, kSlotBatch));
         d.batch = s;
     }
     std::vector<SaResolvedUnit> live;
@@ -741,7 +775,224 @@ int run_resolved(const SaResolvedUnit* units, uint32_t n, bool want_out, BatchRe
         }
     if (!res.sink) res.recs.resize(live.size());
     res.hits.assign(live.size(), 0);
+    res.iters.assign(live.size(), 0);
     return run_batch_range(d, d.batch, live.data(), 0, (uint32_t)live.size(), want_out, res);
+}
+
+// ---------------------------------------------------------------------------
+// Call coalescing.  Concurrent sa_seed_and_filter calls on one GPU share
+// device passes: a caller stages its seed words in pinned memory and queues
+// its call; then either another caller's pass takes it, or the caller gets a
+// free slot and runs every queued call (its own among them, oldest first, up
+// to the slot's unit and seed capacity) as the units of one batched pass with
+// explicit seed words.  The batched path gives each unit exactly the HSP list
+// of a plain call on the same words (per-unit MAX_HITS iterations and dedup
+// scopes), so a call's result does not depend on its neighbours.  A pass that
+// reports a device error (bad key, MAX_HITS, coordinates) re-runs its calls
+// one at a time on the plain path, so each call gets its own status.
+// ---------------------------------------------------------------------------
+void free_staging() {
+    Global& g = G();
+    std::lock_guard<std::mutex> lk(g.pinned_mu);
+    for (uint64_t* p : g.pinned_all) cudaFreeHost(p);
+    g.pinned_all.clear();
+    g.pinned_free.clear();
+}
+
+uint64_t* take_staging() {
+    Global& g = G();
+    {
+        std::lock_guard<std::mutex> lk(g.pinned_mu);
+        if (!g.pinned_free.empty()) {
+            uint64_t* p = g.pinned_free.back();
+            g.pinned_free.pop_back();
+            return p;
+        }
+    }
+    uint64_t* p = nullptr;
+    if (cudaMallocHost(&p, 8 * std::max<uint64_t>(g.max_seeds, 1)) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(g.pinned_mu);
+    g.pinned_all.push_back(p);
+    return p;
+}
+
+void give_staging(uint64_t* p) {
+    Global& g = G();
+    std::lock_guard<std::mutex> lk(g.pinned_mu);
+    g.pinned_free.push_back(p);
+}
+
+// Hands each live call of a completed group its output: header {0, 0, HSPs,
+// hits} (src/seed_filter.cu:756-759) then its HSPs.
+struct CallSink : SaBatchSink {
+    const std::vector<CallReq*>& live;
+    explicit CallSink(const std::vector<CallReq*>& l) : live(l) {}
+    int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) override {
+        uint64_t at = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            CallReq& c = *live[u0 + i];
+            sa_segment* o = (sa_segment*)malloc(sizeof(sa_segment) * (cnt[i] + 1ull));
+            if (!o) {
+                sa_set_error(SA_ERR_NOMEM, "host allocation of %u records failed", cnt[i] + 1);
+                return SA_ERR_NOMEM;
+            }
+            o[0] = sa_segment{0, 0, cnt[i], (int32_t)(uint32_t)hits[i]};
+            if (cnt[i]) std::memcpy(o + 1, recs + at, cnt[i] * sizeof(sa_segment));
+            at += cnt[i];
+            c.out = o;
+            c.out_len = cnt[i] + 1ull;
+            c.stats.num_hits = hits[i];
+            c.stats.num_hsps = cnt[i];
+        }
+        return SA_OK;
+    }
+};
+
+// The plain path for one queued call on slot s (a pass's fallback).
+void run_call_alone(Slot* s, CallReq& c) {
+    Global& g = G();
+    DevState& d = g.devs[s->dev_idx];
+    const Packed& q = c.rev ? d.qr[c.buffer] : d.qf[c.buffer];
+    const sa_call_stats keep = t_stats;
+    c.status = run_call(s, c.staged, c.n, c.rev, q, 0, 0, 0, &c.out, &c.out_len);
+    c.stats = t_stats;
+    c.stats.batch_calls = 1;
+    if (c.status != SA_OK) c.err = t_err;
+    t_stats = keep;
+}
+
+// One pass over queued calls on slot s (results and statuses into the calls).
+void run_coalesced(Slot* s, const std::vector<CallReq*>& calls) {
+    Global& g = G();
+    DevState& d = g.devs[s->dev_idx];
+    SaWork& w = s->w;
+    std::vector<CallReq*> live;
+    std::vector<SaResolvedUnit> ru;
+    uint64_t off = 0;
+    int r = cudaSetDevice(d.dev) == cudaSuccess ? SA_OK : SA_ERR_CUDA;
+    for (CallReq* c : calls) {
+        const Packed& q = c->rev ? d.qr[c->buffer] : d.qf[c->buffer];
+        if (!q.data) {
+            c->status = SA_ERR_STATE;
+            c->err = "query buffer " + std::to_string(c->buffer) + " is not resident";
+            continue;
+        }
+        if (c->n == 0) {  // no seeds: header only (src/seed_filter.cu:736-777 with num_hits = 0)
+            c->out = (sa_segment*)malloc(sizeof(sa_segment));
+            if (!c->out) {
+                c->status = SA_ERR_NOMEM;
+                c->err = "host allocation failed";
+                continue;
+            }
+            c->out[0] = sa_segment{0, 0, 0, 0};
+            c->out_len = 1;
+            c->stats.batch_calls = 1;
+            continue;
+        }
+        if (r == SA_OK &&
+            cudaMemcpyAsync(w.seeds + off, c->staged, 8ull * c->n, cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+            r = SA_ERR_CUDA;
+        SaResolvedUnit u{nullptr, q.data, (uint32_t)q.len, 0, c->n, c->rev};
+        u.seeds = w.seeds + off;
+        ru.push_back(u);
+        live.push_back(c);
+        off += c->n;
+    }
+    if (live.empty()) return;
+    if (r != SA_OK) {
+        for (CallReq* c : live) {
+            c->status = SA_ERR_CUDA;
+            c->err = "seed upload failed";
+        }
+        return;
+    }
+    BatchResult res;
+    CallSink sink(live);
+    res.sink = &sink;
+    res.hits.assign(live.size(), 0);
+    res.iters.assign(live.size(), 0);
+    r = run_batch_range(d, s, ru.data(), 0, (uint32_t)ru.size(), true, res);
+    if (r == SA_OK) {
+        for (size_t i = 0; i < live.size(); ++i) {
+            sa_call_stats& st = live[i]->stats;
+            st.num_seeds = live[i]->n;
+            st.num_iter = res.iters[i];
+            st.batch_calls = (uint32_t)live.size();
+            // totals of the pass (the call's own when it ran alone)
+            st.hits_extended = res.tot.extended;
+            st.seeds_with_hits = res.tot.nnz;
+            st.survivors = res.tot.surv_count;
+            st.long_hits = res.tot.long_count;
+            st.tiles = res.tot.base_steps;
+            st.ms_total = res.timing.ms_total;
+            st.ms_lookup = res.timing.ms_lookup;
+            st.ms_extend_lane = res.timing.ms_extend_lane;
+            st.ms_extend_warp = res.timing.ms_extend_warp;
+            st.ms_dedup = res.timing.ms_dedup;
+            st.ms_copy = res.timing.ms_copy;
+        }
+        return;
+    }
+    // a device error or a failed allocation: each call alone on the plain path
+    for (CallReq* c : live) {
+        free(c->out);
+        c->out = nullptr;
+        c->out_len = 0;
+        c->stats = sa_call_stats{};
+        run_call_alone(s, *c);
+    }
+}
+
+// sa_seed_and_filter with coalescing (SA_COALESCE > 1).
+int seed_and_filter_coalesced(const uint64_t* seeds, uint32_t num_seeds, int rev, uint32_t buffer,
+                              sa_segment** out, uint64_t* out_len) {
+    Global& g = G();
+    CallReq c;
+    c.seeds = seeds;
+    c.n = num_seeds;
+    c.rev = rev ? 1 : 0;
+    c.buffer = buffer;
+    c.staged = take_staging();
+    if (!c.staged) {
+        sa_set_error(SA_ERR_NOMEM, "pinned staging allocation failed");
+        return SA_ERR_NOMEM;
+    }
+    if (num_seeds) std::memcpy(c.staged, seeds, 8ull * num_seeds);
+    {
+        std::unique_lock<std::mutex> lk(g.mu);
+        g.pending.push_back(&c);
+        while (true) {
+            g.cv.wait(lk, [&] { return c.done || (!c.taken && !g.free_slots.empty()); });
+            if (c.done) break;
+            Slot* s = g.free_slots.front();
+            g.free_slots.pop_front();
+            std::vector<CallReq*> pass;
+            uint64_t words = 0;
+            while (!g.pending.empty() && pass.size() < std::min<uint32_t>(g.coalesce_calls, s->max_units)) {
+                CallReq* r = g.pending.front();
+                if (!pass.empty() && words + r->n > s->w.seed_cap) break;
+                g.pending.pop_front();
+                r->taken = true;
+                pass.push_back(r);
+                words += r->n;
+            }
+            lk.unlock();
+            run_coalesced(s, pass);
+            lk.lock();
+            for (CallReq* r : pass) r->done = true;
+            g.free_slots.push_back(s);
+            g.cv.notify_all();
+        }
+    }
+    give_staging(c.staged);
+    t_stats = c.stats;
+    if (c.status != SA_OK) {
+        sa_set_error(c.status, "%s", c.err.c_str());
+        return c.status;
+    }
+    *out = c.out;
+    *out_len = c.out_len;
+    return SA_OK;
 }
 
 // Output of sa_seed_and_filter_batch, written as groups complete: per unit a
@@ -1100,6 +1351,7 @@ int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_si
         return SA_ERR_ARG;
     }
     // release old slots
+    free_staging();
     {
         std::lock_guard<std::mutex> lk(g.mu);
         for (auto* s : g.free_slots) free_slot(s);
@@ -1131,10 +1383,21 @@ int sa_initialize_processor(int transition, uint32_t wga_chunk, uint32_t seed_si
     g.batch_slot_cap = env_u64("SA_BATCH_SLOT_CAP", 1ull << 28);
     g.batch_surv_cap = pow2_floor(env_u64("SA_BATCH_SURV_CAP", 1ull << 29));
     const int per_gpu = (int)env_u64("SA_SLOTS_PER_GPU", 2);
+    // call coalescing (opt-in): up to SA_COALESCE calls (and SA_COALESCE_SEEDS
+    // words) per pass.  Off by default: with free slots the passes stay small,
+    // and on a 16-core host the per-call graphs on 12 slots measured faster
+    // (genome scale, 16 seeder threads: 0.373 s per step against 0.43-0.52 s).
+    g.coalesce_calls = (uint32_t)std::min<uint64_t>(env_u64("SA_COALESCE", 0), 1024);
+    const uint64_t pass_seeds =
+        std::max<uint64_t>(g.max_seeds, std::min<uint64_t>((uint64_t)g.coalesce_calls * g.max_seeds,
+                                                           env_u64("SA_COALESCE_SEEDS", 1ull << 23)));
     for (size_t di = 0; di < g.devs.size(); ++di) {
         for (int k = 0; k < per_gpu; ++k) {
             Slot* s = nullptr;
-            SA_TRY(make_slot((int)di, g.max_seeds, g.surv_cap, g.long_cap, &s));
+            if (g.coalesce_calls > 1)
+                SA_TRY(make_slot((int)di, pass_seeds, g.surv_cap, g.long_cap, &s, kSlotBoth, g.coalesce_calls));
+            else
+                SA_TRY(make_slot((int)di, g.max_seeds, g.surv_cap, g.long_cap, &s));
             std::lock_guard<std::mutex> lk(g.mu);
             g.devs[di].slots.push_back(s);
             g.free_slots.push_back(s);
@@ -1170,6 +1433,7 @@ int sa_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint3
                      (unsigned long long)g.max_seeds);
         return SA_ERR_MAX_SEEDS;
     }
+    if (g.coalesce_calls > 1) return seed_and_filter_coalesced(seeds, num_seeds, rev, buffer, out, out_len);
     Slot* s = acquire_slot();
     DevState& d = g.devs[s->dev_idx];
     const Packed& q = rev ? d.qr[buffer] : d.qf[buffer];
@@ -1251,6 +1515,7 @@ int sa_rm_clear_query(void) {
 // src/seed_filter.cu:882-890 (without cudaDeviceReset: only this library's buffers are freed)
 int sa_shutdown_processor(void) {
     Global& g = G();
+    free_staging();
     {
         std::lock_guard<std::mutex> lk(g.mu);
         for (auto& d : g.devs)

@@ -20,24 +20,34 @@ struct SaCallDesc {
 
 #define SA_BATCH_ITERS 16
 
-// Batched unit: a query window [start, end) of one packed query, seeded on the device.
+// Batched unit: either a query window [q_start, q_end) of one packed query,
+// seeded on the device from its per-position keys (S slots per position), or
+// (seeds != null) the explicit seed words of one plain call, one slot per
+// word, words [q_start, q_end) of `seeds`.
 struct SaBatchUnit {
     uint64_t slot_begin;    // first seed slot of the unit in the flattened slot space
-    uint32_t q_start, q_end;// seed positions j in [q_start, q_end)
+    uint32_t q_start, q_end;// seed positions j (or word indices) in [q_start, q_end)
     const uint32_t* keys;   // per-position seed keys of the unit's query strand
+    const uint64_t* seeds;  // explicit seed words (key << 32 | j), or null
     uint32_t unit;          // index into the SaUnit table
     uint32_t pad;
 };
 
 // A batched unit resolved to device pointers (library query buffer or a
-// serving request's own buffers).
+// serving request's own buffers), or a plain call's seed words on the device.
 struct SaResolvedUnit {
     const uint32_t* keys;      // per-position seed keys of this strand
     const uint32_t* q_packed;  // packed strand (forward or reverse complement)
     uint32_t q_len;
-    uint32_t start, end;       // seed positions [start, end)
+    uint32_t start, end;       // seed positions [start, end) (word indices with seeds)
     int32_t rev;
+    const uint64_t* seeds = nullptr;  // explicit seed words (device), or null
 };
+
+// Seed slots of a resolved unit: S per position, one per explicit word.
+inline uint64_t sa_unit_slots(const SaResolvedUnit& u, uint64_t S) {
+    return (uint64_t)(u.end - u.start) * (u.seeds ? 1 : S);
+}
 
 // Receives the output of one completed device group of a batched run:
 // units [u0, u0 + n) of the run's non-empty units, in order, their HSP

@@ -160,15 +160,32 @@ struct SaSlotInfo {
     uint32_t unit, j, lo, cnt;
 };
 
+// Slot s of batch unit u: its query position, bucket start and hit count.
+// An explicit word whose key is outside the table sets bad_key (a plain call
+// reports it as SA_ERR_BAD_SEED, src/seed_filter.cu:129-154 reads past the
+// table there); a device-seeded slot never has such a key.
 __device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu, uint32_t u, uint64_t s,
-                                              const uint32_t* __restrict__ index, uint32_t nbuckets, int S) {
+                                              const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
+                                              bool& bad_key) {
     SaSlotInfo r;
     const SaBatchUnit B = bu[u];
     const uint64_t off = s - B.slot_begin;
     r.unit = B.unit;
-    r.j = B.q_start + (uint32_t)(off / S);
-    const uint32_t v = (uint32_t)(off % S);
-    uint32_t key = __ldg(B.keys + r.j);
+    uint32_t key;
+    uint32_t v = 0;
+    if (B.seeds) {  // find_num_hits (src/seed_filter.cu:129-154) on the call's own words
+        const uint64_t word = __ldg(reinterpret_cast<const unsigned long long*>(B.seeds) + B.q_start + off);
+        key = (uint32_t)(word >> 32);
+        r.j = (uint32_t)word;
+        if (key >= nbuckets) {
+            bad_key = true;
+            key = SA_INVALID_KEY;
+        }
+    } else {
+        r.j = B.q_start + (uint32_t)(off / S);
+        v = (uint32_t)(off % S);
+        key = __ldg(B.keys + r.j);
+    }
     r.lo = 0;
     r.cnt = 0;
     if (key != SA_INVALID_KEY) {
@@ -186,19 +203,21 @@ __global__ void __launch_bounds__(256)
 sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc,
                    const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
                    uint32_t* __restrict__ s_lo, uint32_t* __restrict__ s_cnt, unsigned long long* cta_a,
-                   unsigned long long* cta_b) {
+                   unsigned long long* cta_b, SaCounters* ctr) {
     uint64_t a, b;
     sa_cta_range(desc->num_seeds, a, b);
     const uint32_t nu = desc->num_units;
     unsigned long long hits = 0, nz = 0;
+    bool bad_key = false;
     for (uint64_t s = a + threadIdx.x; s < b; s += 256) {
         const uint32_t u = sa_find_unit(bu, nu, s);
-        const SaSlotInfo si = sa_slot(bu, u, s, index, nbuckets, S);
+        const SaSlotInfo si = sa_slot(bu, u, s, index, nbuckets, S, bad_key);
         s_lo[s] = si.lo;
         s_cnt[s] = si.cnt;
         hits += si.cnt;
         nz += si.cnt != 0;
     }
+    if (bad_key) atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_BAD_KEY);
     __shared__ unsigned long long ws[9];
     unsigned long long tot;
     sa_block_excl_sum<unsigned long long, 256>(hits, ws, &tot);
@@ -236,7 +255,9 @@ sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restri
                 const uint64_t c = cbase + ec;
                 cs.E[c] = hbase + eh;
                 cs.lo[c] = s_lo[s];
-                cs.qpos[c] = B.q_start + (uint32_t)((s - B.slot_begin) / S);
+                cs.qpos[c] = B.seeds ? (uint32_t)__ldg(reinterpret_cast<const unsigned long long*>(B.seeds) +
+                                                       B.q_start + (s - B.slot_begin))
+                                     : B.q_start + (uint32_t)((s - B.slot_begin) / S);
                 cs.unit[c] = B.unit;
                 cs.scope[c] = u;  // batch unit index; turned into (unit, iteration) by sa_k_bscope
             }
@@ -324,7 +345,8 @@ __global__ void sa_k_bscope(SaSeedList cs, const unsigned long long* __restrict_
 void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, uint32_t n_bunits, const SaParams& p,
                             int G, cudaStream_t st) {
     const int S = p.transition ? 1 + p.kmer_size : 1;
-    sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a, w.cta_b);
+    sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a, w.cta_b,
+                                          w.ctr);
     sa_note_launch();
     sa_k_scan_partials<<<1, 1024, 0, st>>>(w.cta_a, w.cta_b, G, &w.ctr->num_hits, &w.ctr->nnz);
     sa_note_launch();
