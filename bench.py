@@ -529,13 +529,18 @@ def run_ours(args):
         barrier()
         t0 = time.perf_counter()
         outs = None
+        t_write = t_call = 0.0
         for _ in range(k_e2e):
+            t1 = time.perf_counter()
             sf.send_query_write_request(w.query, 1)
+            t2 = time.perf_counter()
             outs = sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
+            t_write, t_call = t_write + t2 - t1, t_call + time.perf_counter() - t2
         barrier()
         eb_s = allreduce((time.perf_counter() - t0) / k_e2e, "max")
         out["e2e_batched"] = {"value": e2e_hits / eb_s, "unit": UNIT, "h2d_bytes_per_step": len(w.query),
-                              "d2h_bytes_per_step": int(sum(len(o) for o in outs) * 16)}
+                              "d2h_bytes_per_step": int(sum(len(o) for o in outs) * 16),
+                              "query_write_s": t_write / k_e2e, "batch_call_s": t_call / k_e2e}
         # bit-exact: batched units == plain per-call results (concatenated per strand)
         bf = np.concatenate([o[1:] for o in outs[: len(plus)]]) if plus else np.zeros(0)
         br = np.concatenate([o[1:] for o in outs[len(plus):]]) if minus else np.zeros(0)
