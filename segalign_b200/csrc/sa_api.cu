@@ -169,7 +169,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 2, 148, 0};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -1701,6 +1701,14 @@ int sa_set_tuning_param(const char* name, int value) {
         (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
         return SA_OK;
     }
+    if (n == "switch_now") {
+        if (value != 0 && value != 1) {
+            sa_set_error(SA_ERR_ARG, "switch_now must be 0 or 1 (got %d)", value);
+            return SA_ERR_ARG;
+        }
+        t.switch_now = value;
+        return SA_OK;
+    }
     if (n == "call_lane_ctas") {
         if (value < 0 || value > 8 * SA_MAX_CTAS) {
             sa_set_error(SA_ERR_ARG, "call_lane_ctas must be 0 (half the batched grid) .. %d (got %d)",
@@ -1734,6 +1742,7 @@ int sa_get_tuning_param(const char* name) {
     if (n == "range_ctas") return t.range_ctas;
     if (n == "call_range_ctas") return t.call_range_ctas;
     if (n == "call_lane_ctas") return t.call_lane_ctas;
+    if (n == "switch_now") return t.switch_now;
     return SA_ERR_ARG;
 }
 

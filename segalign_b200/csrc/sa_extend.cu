@@ -47,6 +47,7 @@ struct SaExtK {
     uint32_t lane_cap;
     uint32_t tile_hits;
     uint32_t substeps;  // steps per lane-kernel iteration (at most)
+    uint32_t switch_now;  // 1: a lane starts its left side in the step after its right side ends
 };
 
 // Reverse the order of the 8 nibbles of a word.
@@ -302,6 +303,30 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     int S = 0, best = 0, bpos = 0, Rbest = 0, Rpos = -1;
     uint32_t tiles = 0, tiles_acc = 0, ext_acc = 0;  // per-lane statistics (32-bit per lane)
 
+    // Start of a direction of the current hit (dir 0: right of the hit; 1:
+    // left, read rightwards in the reversed copies): offsets, bases
+    // available, word shifts and the first NW + 1 words of both sequences.
+    auto begin_dir = [&](const uint32_t* __restrict__ qp, uint32_t qlen) {
+        const uint32_t ref_len = a.ref_len;
+        const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
+        avail = min(ref_len - sr, qlen - sq);
+        sh_r = (sr & 7u) * 4u;
+        sh_q = (sq & 7u) * 4u;
+        pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
+        pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
+#pragma unroll
+        for (int j = 0; j <= NW; ++j) {
+            w_r[j] = __ldg(pr + j);
+            w_q[j] = __ldg(pq + j);
+        }
+        pr += NW + 1;
+        pq += NW + 1;
+        o = 0;
+        S = 0;
+        best = 0;
+        bpos = 0;
+    };
+
     while (true) {
         // ---- idle lanes take the next hits of the warp tile, in order ----
         const uint32_t idle = __ballot_sync(SA_FULL, !has);
@@ -386,26 +411,7 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
             }
             if (setup) {
                 setup = false;
-                const uint32_t* __restrict__ qp = U.q_packed;
-                const uint32_t qlen = U.q_len;
-                const uint32_t ref_len = a.ref_len;
-                const uint32_t sr = dir ? ref_len - rl : rl, sq = dir ? qlen - ql : ql;
-                avail = min(ref_len - sr, qlen - sq);
-                sh_r = (sr & 7u) * 4u;
-                sh_q = (sq & 7u) * 4u;
-                pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
-                pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
-#pragma unroll
-                for (int j = 0; j <= NW; ++j) {
-                    w_r[j] = __ldg(pr + j);
-                    w_q[j] = __ldg(pq + j);
-                }
-                pr += NW + 1;
-                pq += NW + 1;
-                o = 0;
-                S = 0;
-                best = 0;
-                bpos = 0;
+                begin_dir(U.q_packed, U.q_len);
             }
         }
         const bool done = !__any_sync(SA_FULL, has) && exhausted && tile_pos >= tile_n;
@@ -505,6 +511,17 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     total = Rbest + best;
                     tiles_acc += tiles;
                     has = false;
+                }
+            }
+            // switch_now: a lane whose right side ended in this step starts
+            // its left side at once and scans in the iteration's remaining
+            // steps instead of idling until the next iteration
+            if (a.switch_now && sub + 1 < a.substeps && __any_sync(SA_FULL, setup)) {
+                if (setup) {
+                    setup = false;
+                    const SaUnit U = a.units[unit_id];
+                    begin_dir(U.q_packed, U.q_len);
+                    scanning = true;
                 }
             }
         }
@@ -778,6 +795,7 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.lane_cap = (uint32_t)t.lane_cap;
     a.tile_hits = (uint32_t)t.tile_hits;
     a.substeps = (uint32_t)t.substeps;
+    a.switch_now = t.switch_now ? 1u : 0u;
     return a;
 }
 

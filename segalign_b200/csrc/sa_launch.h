@@ -130,6 +130,8 @@ struct SaTuning {
     int tile_hits;       // hits per warp tile
     int step_bases;      // bases a lane scores per step of the lane-per-hit kernel (8, 16 or 32)
     int substeps;        // steps a lane may take per iteration of the lane-per-hit kernel
+    int switch_now;      // 1: a lane whose right side ends starts its left side in the same
+                         // iteration (with substeps > 1) instead of at the next one
     int call_range_ctas; // CTAs of the range-partitioned kernels of a plain or rm call (at most
                          // MAX_SEEDS seed words: fewer CTAs than a batch needs)
     int call_lane_ctas;  // CTAs of a plain or rm call's lane kernel; 0: half of the batched

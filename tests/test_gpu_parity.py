@@ -127,6 +127,25 @@ def test_tuning_does_not_change_results(setup, lane_cap, ctas, tile, step, sub):
         sf.set_tuning(**saved)
 
 
+@pytest.mark.parametrize("sub,sw", [(1, 1), (2, 0), (2, 1), (3, 0), (3, 1), (8, 1)])
+def test_switch_now_does_not_change_results(setup, sub, sw):
+    """Starting a hit's left side in the same iteration as its right side ends
+    (switch_now) or at the next one gives the same HSPs and tile counts."""
+    w, p, sf = setup["w"], setup["p"], setup["sf"]
+    for rev in (False, True):
+        text = setup["rctext"] if rev else w.query
+        seeds = host_seeds(text, 100_000, 300_000)
+        want, st = oracle.seed_and_filter(p, setup["R"], setup["QR"] if rev else setup["Q"], setup["idx"],
+                                          setup["pos"], seeds, rev)
+        saved = sf.get_tuning()
+        sf.set_tuning(substeps=sub, switch_now=sw)
+        try:
+            compare_segments(sf.seed_and_filter(seeds, rev, 0), want, f"substeps={sub} switch_now={sw} rev={rev}")
+            assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
+        finally:
+            sf.set_tuning(**saved)
+
+
 @pytest.mark.parametrize("lane_ctas,range_ctas", [(1, 1), (37, 16), (148, 148), (1000, 1024)])
 def test_call_grid_knobs_do_not_change_results(setup, lane_ctas, range_ctas):
     """A plain call's lane-kernel grid and range-kernel grid (down to one CTA,
