@@ -283,7 +283,7 @@ typedef struct {
 } sa_autotune_cfg;
 
 typedef struct {
-    int32_t ext_ctas_per_sm, step_bases, tile_hits, lane_cap, range_ctas, substeps;
+    int32_t ext_ctas_per_sm, step_bases, tile_hits, lane_cap, range_ctas, substeps, switch_now;
     int32_t candidates;      /* settings timed                           */
     int32_t rejected;        /* settings that failed or changed results  */
     int32_t from_cache;

@@ -102,7 +102,8 @@ class AutotuneCfg(C.Structure):
 
 class AutotuneResult(C.Structure):
     _fields_ = [("ext_ctas_per_sm", C.c_int32), ("step_bases", C.c_int32), ("tile_hits", C.c_int32),
-                ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("substeps", C.c_int32), ("candidates", C.c_int32),
+                ("lane_cap", C.c_int32), ("range_ctas", C.c_int32), ("substeps", C.c_int32), ("switch_now", C.c_int32),
+                ("candidates", C.c_int32),
                 ("rejected", C.c_int32), ("from_cache", C.c_int32), ("ms_start", C.c_double),
                 ("ms_best", C.c_double)]
 

@@ -14,6 +14,8 @@
 //   lane_cap         bases a lane scans before a hit moves to a whole warp
 //   range_ctas       CTAs of the lookup, compaction and sort kernels
 //   substeps         steps a lane may take per lane-kernel iteration
+//   switch_now       whether a lane starts a hit's left side within the
+//                    iteration in which its right side ends
 // Results are cached per GPU name and workload signature in a JSON-lines
 // file, so a later run applies them without a sweep.
 #include <cstdio>
@@ -39,7 +41,8 @@ const Knob kKnobs[] = {
     {"tile_hits", {96, 128, 160, 224, 320}, {128, 160, 224}},
     {"lane_cap", {1024, 2048, 4096, 8192}, {2048, 4096}},
     {"range_ctas", {148, 296, 592}, {296}},
-    {"substeps", {1, 2, 3, 4}, {1, 2}},
+    {"substeps", {1, 2, 3, 4}, {2, 3}},
+    {"switch_now", {0, 1}, {0, 1}},
 };
 constexpr int kNumKnobs = sizeof(kKnobs) / sizeof(kKnobs[0]);
 
@@ -206,6 +209,7 @@ int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* c
     out->lane_cap = cur[3];
     out->range_ctas = cur[4];
     out->substeps = cur[5];
+    out->switch_now = cur[6];
     return SA_OK;
 }
 

@@ -34,7 +34,7 @@ def test_autotune_keeps_results_and_caches(sf, tmp_path):
     assert res["ms_best"] <= res["ms_start"]
     tuned = sf.get_tuning()
     knobs = [k for k in DEFAULT if k in res]  # the batched path's knobs (not call_range_ctas)
-    assert len(knobs) == 6
+    assert len(knobs) == 7
     for k in knobs:
         assert tuned[k] == res[k], k
     assert tuned["call_range_ctas"] == DEFAULT["call_range_ctas"]
