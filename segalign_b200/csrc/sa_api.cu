@@ -86,6 +86,10 @@ struct DevState {
     uint64_t num_index = 0;
     Packed qf[kMaxBuffers], qr[kMaxBuffers];
     uint32_t* qkeys[kMaxBuffers][2] = {};  // per-position seed keys (batched seeding)
+    uint64_t qkeys_cap[kMaxBuffers][2] = {};  // bytes allocated for qkeys
+    bool qkeys_ok[kMaxBuffers][2] = {};       // qkeys hold the keys of the resident query
+    char* stage = nullptr;                 // text staging of uploads (grow-only)
+    uint64_t stage_cap = 0;
     std::vector<Slot*> slots;
     Slot* batch = nullptr;                 // workspace of batched calls
 };
@@ -209,9 +213,18 @@ void set_shape_positions(SaParams& p, const std::string& shape) {
 
 // Allocates a packed sequence of len bases followed by its reversed copy
 // (sa_rev_words), all words E-filled.
+// A packed sequence of the same word count reuses its allocation (a new
+// query block of the same size is written in place); the device is first
+// synchronized, as cudaFree would, so no earlier work still reads it.
 int alloc_packed(Packed& pk, uint64_t len) {
-    pk.release();
     const uint64_t nw = sa_rev_words(len);
+    if (pk.base && sa_rev_words(pk.len) == nw) {
+        SA_CUDA_OK(cudaDeviceSynchronize());
+        pk.len = len;
+        sa_launch_pad_fill(pk.base, 2 * nw, 0);
+        return SA_OK;
+    }
+    pk.release();
     SA_CUDA_OK(cudaMalloc(&pk.base, 2 * nw * sizeof(uint32_t)));
     pk.data = pk.base + SA_PADW;
     pk.len = len;
@@ -233,23 +246,26 @@ int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed*
     SA_CUDA_OK(cudaSetDevice(d.dev));
     SA_TRY(alloc_packed(pk, len));
     if (rc) SA_TRY(alloc_packed(*rc, len));
-    char* d_text = nullptr;
     const uint64_t chunk = 1ull << 28;  // 256 MiB text per round
-    SA_CUDA_OK(cudaMalloc(&d_text, std::min<uint64_t>(len ? len : 1, chunk) + 16));
+    const uint64_t need = std::min<uint64_t>(len ? len : 1, chunk) + 16;
+    if (d.stage_cap < need) {
+        if (d.stage) cudaFree(d.stage);
+        d.stage = nullptr;
+        d.stage_cap = 0;
+        SA_CUDA_OK(cudaMalloc(&d.stage, need));
+        d.stage_cap = need;
+    }
+    char* d_text = d.stage;
     for (uint64_t off = 0; off < len; off += chunk) {
         uint64_t n = std::min(chunk, len - off);
         cudaError_t e = cudaMemcpy(d_text, text + off, n, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) {
-            cudaFree(d_text);
-            return sa_cuda_fail(e, "cudaMemcpy(text)", __FILE__, __LINE__);
-        }
+        if (e != cudaSuccess) return sa_cuda_fail(e, "cudaMemcpy(text)", __FILE__, __LINE__);
         // chunk is a multiple of 8 bases, so word boundaries line up
         sa_launch_pack_text(d_text, n, pk.data + off / 8, 0);
     }
     finish_packed(pk);
     if (rc) make_rc_packed(pk, *rc);
     cudaError_t e = cudaDeviceSynchronize();
-    cudaFree(d_text);
     if (e != cudaSuccess) return sa_cuda_fail(e, "pack", __FILE__, __LINE__);
     return SA_OK;
 }
@@ -584,25 +600,41 @@ int check_ready(bool need_query) {
 // ---------------------------------------------------------------------------
 int ensure_keys(DevState& d, uint32_t buffer, int rev) {
     Global& g = G();
-    if (d.qkeys[buffer][rev]) return SA_OK;
+    if (d.qkeys[buffer][rev] && d.qkeys_ok[buffer][rev]) return SA_OK;
     const Packed& q = rev ? d.qr[buffer] : d.qf[buffer];
     if (!q.data) {
         sa_set_error(SA_ERR_STATE, "query buffer %u is not resident", buffer);
         return SA_ERR_STATE;
     }
     SA_CUDA_OK(cudaSetDevice(d.dev));
-    SA_CUDA_OK(cudaMalloc(&d.qkeys[buffer][rev], 4 * (q.len ? q.len : 1)));
+    const uint64_t need = 4 * (q.len ? q.len : 1);
+    if (d.qkeys_cap[buffer][rev] < need) {  // a new query of the same size reuses the array
+        if (d.qkeys[buffer][rev]) cudaFree(d.qkeys[buffer][rev]);
+        d.qkeys[buffer][rev] = nullptr;
+        d.qkeys_cap[buffer][rev] = 0;
+        SA_CUDA_OK(cudaMalloc(&d.qkeys[buffer][rev], need));
+        d.qkeys_cap[buffer][rev] = need;
+    }
     sa_launch_query_keys(q.data, q.len, g.params, d.qkeys[buffer][rev], 0);
     SA_CUDA_OK(cudaDeviceSynchronize());
+    d.qkeys_ok[buffer][rev] = true;
     return SA_OK;
 }
 
+// Keys of a buffer whose query is rewritten: recomputed on next use, in place.
+void invalidate_keys(DevState& d, uint32_t buffer) {
+    for (int r = 0; r < 2; ++r) d.qkeys_ok[buffer][r] = false;
+}
+
 void drop_keys(DevState& d, uint32_t buffer) {
-    for (int r = 0; r < 2; ++r)
+    for (int r = 0; r < 2; ++r) {
         if (d.qkeys[buffer][r]) {
             cudaFree(d.qkeys[buffer][r]);
             d.qkeys[buffer][r] = nullptr;
         }
+        d.qkeys_cap[buffer][r] = 0;
+        d.qkeys_ok[buffer][r] = false;
+    }
 }
 
 struct BatchResult {
@@ -1416,7 +1448,7 @@ int sa_send_query_write_request(const char* query_buffer, size_t start_addr, uin
         return SA_ERR_ARG;
     }
     for (auto& d : g.devs) {
-        drop_keys(d, buffer);
+        invalidate_keys(d, buffer);
         SA_TRY(upload_pack(d, query_buffer + start_addr, len, d.qf[buffer], &d.qr[buffer]));
     }
     return SA_OK;
@@ -1534,6 +1566,9 @@ int sa_shutdown_processor(void) {
             d.qr[b].release();
             drop_keys(d, b);
         }
+        if (d.stage) cudaFree(d.stage);
+        d.stage = nullptr;
+        d.stage_cap = 0;
     }
     sa_clear_ref();
     g.processor_ready = false;
