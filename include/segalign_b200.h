@@ -297,9 +297,12 @@ int sa_autotune(const sa_unit* units, uint32_t n_units, const sa_autotune_cfg* c
  * "substeps" (1..8 steps a lane may take per iteration of the lane kernel),
  * "step_bases" (8, 16 or 32 bases scored per lane step), "range_ctas" (CTAs of the
  * lookup/sort kernels of a batched pass), "call_range_ctas" (the same for one plain or
- * rm call), "call_lane_ctas" (CTAs of one plain or rm call's lane kernel; 0 = half of
- * the batched grid, so that concurrent calls share the GPU).  Results never depend on them.  Returns SA_OK or
- * SA_ERR_ARG; sa_get_tuning_param returns the current value. */
+ * rm call), "call_lane_ctas" (CTAs of one plain call's lane kernel; 0 = half of
+ * the batched grid, so that concurrent calls share the GPU), "switch_now" (0/1: a lane
+ * starts a hit's left side in the iteration its right side ends), and for the lane
+ * kernel of one rm call "rm_lane_ctas" (0 = the batched grid), "rm_substeps" (1..8),
+ * "rm_switch_now" (0/1).  Results never depend on them.  Returns SA_OK or SA_ERR_ARG;
+ * sa_get_tuning_param returns the current value. */
 int sa_set_tuning_param(const char* name, int value);
 int sa_get_tuning_param(const char* name);
 

@@ -173,7 +173,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -442,9 +442,15 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     xa.xdrop = g.params.xdrop;
     xa.hspthresh = g.params.hspthresh;
     xa.noentropy = g.params.noentropy;
-    const int lane_grid = g.tuning.call_lane_ctas > 0 ? g.tuning.call_lane_ctas
-                                                     : std::max(1, d.num_sms * g.tuning.ext_ctas_per_sm / 2);
-    sa_launch_extend_lane(w, xa, g.params, g.tuning, d.num_sms, st, lane_grid);
+    SaTuning t = g.tuning;
+    int lane_grid = g.tuning.call_lane_ctas > 0 ? g.tuning.call_lane_ctas
+                                                : std::max(1, d.num_sms * g.tuning.ext_ctas_per_sm / 2);
+    if (mode == 1) {  // repeat-masker call
+        t.substeps = g.tuning.rm_substeps;
+        t.switch_now = g.tuning.rm_switch_now;
+        lane_grid = g.tuning.rm_lane_ctas > 0 ? g.tuning.rm_lane_ctas : d.num_sms * g.tuning.ext_ctas_per_sm;
+    }
+    sa_launch_extend_lane(w, xa, g.params, t, d.num_sms, st, lane_grid);
     tm.mark(2);
     sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
     tm.mark(3);
@@ -1736,12 +1742,29 @@ int sa_set_tuning_param(const char* name, int value) {
         (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
         return SA_OK;
     }
-    if (n == "switch_now") {
+    if (n == "switch_now" || n == "rm_switch_now") {
         if (value != 0 && value != 1) {
-            sa_set_error(SA_ERR_ARG, "switch_now must be 0 or 1 (got %d)", value);
+            sa_set_error(SA_ERR_ARG, "%s must be 0 or 1 (got %d)", name, value);
             return SA_ERR_ARG;
         }
-        t.switch_now = value;
+        (n == "switch_now" ? t.switch_now : t.rm_switch_now) = value;
+        return SA_OK;
+    }
+    if (n == "rm_substeps") {
+        if (value < 1 || value > 8) {
+            sa_set_error(SA_ERR_ARG, "rm_substeps must be 1..8 (got %d)", value);
+            return SA_ERR_ARG;
+        }
+        t.rm_substeps = value;
+        return SA_OK;
+    }
+    if (n == "rm_lane_ctas") {
+        if (value < 0 || value > 8 * SA_MAX_CTAS) {
+            sa_set_error(SA_ERR_ARG, "rm_lane_ctas must be 0 (the batched grid) .. %d (got %d)", 8 * SA_MAX_CTAS,
+                         value);
+            return SA_ERR_ARG;
+        }
+        t.rm_lane_ctas = value;
         return SA_OK;
     }
     if (n == "call_lane_ctas") {
@@ -1778,6 +1801,9 @@ int sa_get_tuning_param(const char* name) {
     if (n == "call_range_ctas") return t.call_range_ctas;
     if (n == "call_lane_ctas") return t.call_lane_ctas;
     if (n == "switch_now") return t.switch_now;
+    if (n == "rm_switch_now") return t.rm_switch_now;
+    if (n == "rm_substeps") return t.rm_substeps;
+    if (n == "rm_lane_ctas") return t.rm_lane_ctas;
     return SA_ERR_ARG;
 }
 

@@ -134,9 +134,12 @@ struct SaTuning {
                          // iteration (with substeps > 1) instead of at the next one
     int call_range_ctas; // CTAs of the range-partitioned kernels of a plain or rm call (at most
                          // MAX_SEEDS seed words: fewer CTAs than a batch needs)
-    int call_lane_ctas;  // CTAs of a plain or rm call's lane kernel; 0: half of the batched
+    int call_lane_ctas;  // CTAs of a plain call's lane kernel; 0: half of the batched
                          // grid, so that concurrent calls' kernels share the SMs and fill
                          // each other's ramp-up and tail instead of queueing
+    // a repeat-masker call's lane kernel (its hits are windowed and its calls
+    // large): CTAs (0: the batched grid), steps per iteration, switch_now
+    int rm_lane_ctas, rm_substeps, rm_switch_now;
 };
 
 // ---- sa_pack.cu ----

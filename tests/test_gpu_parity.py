@@ -205,8 +205,10 @@ def test_transitions_small(built):
         compare_segments(g, x, f"batched transition unit {units[u]}")
 
 
-@pytest.mark.parametrize("exclude", [False, True])
-def test_repeat_masker_self_alignment(built, exclude):
+@pytest.mark.parametrize("exclude,rm_knobs", [(False, None), (True, None), (True, (37, 3, 1)), (False, (600, 1, 1))])
+def test_repeat_masker_self_alignment(built, exclude, rm_knobs):
+    """rm calls against the oracle, with the default lane settings of an rm
+    call and with other (rm_lane_ctas, rm_substeps, rm_switch_now)."""
     w = small_workload(scale=0.5, seed=9)
     T = w.target
     p = oracle.params(rm_exclude_diag=exclude)
@@ -219,6 +221,9 @@ def test_repeat_masker_self_alignment(built, exclude):
     sf.generate_seed_pos_table(None, 1, 19, 12)
     sf.rm_send_query_write_request()
     sf.set_rm_exclude_diagonal(exclude)
+    saved = sf.get_tuning()
+    if rm_knobs:
+        sf.set_tuning(rm_lane_ctas=rm_knobs[0], rm_substeps=rm_knobs[1], rm_switch_now=rm_knobs[2])
     try:
         R = oracle.encode(T)
         RC = oracle.rc_codes(R)
@@ -231,9 +236,11 @@ def test_repeat_masker_self_alignment(built, exclude):
             got = sf.rm_seed_and_filter(seeds, rev, ref_start, ref_end)
             want, st = oracle.seed_and_filter(p, R, RC if rev else R, idx, pos, seeds, rev, 1, ref_start, ref_end)
             assert st["hits_extended"] < st["num_hits"]
-            compare_segments(got, want, f"rm rev={rev} exclude={exclude}")
+            compare_segments(got, want, f"rm rev={rev} exclude={exclude} knobs={rm_knobs}")
+            assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
     finally:
         sf.set_rm_exclude_diagonal(False)
+        sf.set_tuning(**saved)
 
 
 def test_hsp_set_reused_after_overflow(setup):
