@@ -101,6 +101,25 @@ def test_tuning_validation(built):
     assert lib.sa_set_tuning(8192, 256, 3, 160) == 0
 
 
+def test_named_tuning_parameters(built):
+    """Each named knob accepts its documented range, rejects values outside it
+    without changing the current value, and reads back what was set."""
+    lib = sa.load_library()
+    ranges = {b"substeps": (1, 8), b"rm_substeps": (1, 8), b"switch_now": (0, 1), b"rm_switch_now": (0, 1),
+              b"range_ctas": (1, 1024), b"call_range_ctas": (1, 1024), b"call_lane_ctas": (0, 8192),
+              b"rm_lane_ctas": (0, 8192)}
+    for name, (lo, hi) in ranges.items():
+        old = lib.sa_get_tuning_param(name)
+        assert lo <= old <= hi, (name, old)
+        for bad in (lo - 1, hi + 1):
+            assert lib.sa_set_tuning_param(name, bad) == -1, (name, bad)
+            assert lib.sa_get_tuning_param(name) == old
+        for good in (lo, hi, old):
+            assert lib.sa_set_tuning_param(name, good) == 0, (name, good)
+            assert lib.sa_get_tuning_param(name) == good
+    assert lib.sa_get_tuning_param(b"no_such_knob") == -1
+
+
 def test_serve_calls_without_a_running_loop(built):
     """Serving calls report SA_ERR_STATE until sa_serve_start succeeds; stop is harmless."""
     import ctypes as C
