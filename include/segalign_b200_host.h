@@ -132,6 +132,77 @@ int sa_format_rm_intervals(const sa_chrom_table* chroms, uint64_t block_start, c
 
 void sa_free_text(char* text);
 
+/* ---- FASTA ingest and the whole-file driver (src/main.cpp:297-730) ---- */
+
+/* A FASTA file joined into sequence blocks as src/main.cpp:336-455 (query)
+ * and :486-528 (target) join it: records are concatenated with '&' after
+ * each; a block closes after the record that takes its length above
+ * seq_block_size (that record gets no '&'); the last block's length excludes
+ * its trailing '&'.  Chromosome starts and block starts are offsets into
+ * text.  Records are read with kseq's rules (common/kseq.h): name up to the
+ * first white space, sequence lines up to the next '>'/'@'/'+' line, empty
+ * lines skipped, trailing '\r' dropped; gzip or plain. */
+typedef struct {
+    const char* text;
+    uint64_t text_len;
+    uint32_t num_chroms;
+    uint32_t num_blocks;
+    const char* const* names;
+    const uint64_t* chrom_start;
+    const uint32_t* chrom_len;
+    const uint64_t* block_start;
+    const uint32_t* block_len;
+    void* impl;
+} sa_seq_set;
+
+/* Reads `path` (seq_block_size 0 = 500,000,000, src/graph.h:10).  Free with sa_seq_set_free. */
+int sa_fasta_load(const char* path, uint32_t seq_block_size, sa_seq_set* out);
+void sa_seq_set_free(sa_seq_set* s);
+
+/* One target file against one query file, src/main.cpp:297-730: every target
+ * block is sent and its seed table built; the query blocks stream through the
+ * two query buffers (BUFFER_DEPTH = 2): block k is written into buffer k % 2
+ * by a loader thread once block k - 2 has finished, while the seeders work on
+ * block k - 1 from the other buffer.  Each query block is cut into intervals
+ * of interval_size over [0, len - seed_size) and each interval into chunk_size
+ * SeedAndFilter calls per strand (src/seeder.cpp:47-121).  Per interval, the
+ * lastz --segments lines of its HSPs (sa_format_segments: plus strand, then
+ * minus) go to segments_path, and its HSP records to hsp_path as
+ * {u32 target block, u32 query block, u32 interval, u32 strand, sa_segment}.
+ * Needs sa_initialize_interface, sa_generate_shape_pos, sa_host_set_shape and
+ * sa_initialize_processor first; replaces the resident target and query
+ * buffers 0 and 1. */
+typedef struct {
+    const char* target_path;
+    const char* query_path;
+    const char* segments_path;  /* NULL: no segments file           */
+    const char* hsp_path;       /* NULL: no HSP record file         */
+    uint32_t seq_block_size;    /* 0 = 500,000,000                  */
+    uint32_t interval_size;     /* 0 = 10,000,000                   */
+    uint32_t interval_overlap;  /* extra bases seeded past each interval; 0 as in the reference */
+    uint32_t chunk_size;        /* 0 = 250,000                      */
+    int32_t strand;             /* 0 or 3 both, 1 plus, 2 minus     */
+    int32_t num_threads;        /* concurrent seeder calls; 0 = 16  */
+    uint32_t step;              /* seed table step; 0 = 1           */
+    uint32_t pad;
+} sa_align_cfg;
+
+typedef struct {
+    uint64_t ref_blocks;
+    uint64_t query_blocks;
+    uint64_t intervals;
+    uint64_t num_seeds;
+    uint64_t num_hits;
+    uint64_t num_hsps;
+    double seconds;              /* whole call                                   */
+    double read_seconds;         /* FASTA parsing and block assembly             */
+    double table_seconds;        /* target uploads and seed-table builds         */
+    double query_write_seconds;  /* query block uploads (loader thread)          */
+    double overlap_seconds;      /* of those, while the seeders ran the other buffer */
+} sa_align_stats;
+
+int sa_align_fasta(const sa_align_cfg* cfg, sa_align_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

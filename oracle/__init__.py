@@ -286,3 +286,186 @@ def format_rm_intervals(chroms, block_start, runs, markend=False):
     if out and markend:
         out.append("# segalign_repeat_masker end-of-file\n")
     return "".join(out)
+
+
+# --------------------------------------------------------------------------
+# The reference's own seed-filter code on the GPU (oracle/ref_harness.cu,
+# built by `make -C oracle ref_kernels` from the reference tree).  It pins the
+# oracle's extension/dedup half; it needs a GPU, and its binaries travel with
+# the repository snapshot (oracle/_ref/ is git-ignored, not copy-ignored).
+# --------------------------------------------------------------------------
+REF_HARNESS = {"plain": os.path.join(HERE, "_ref", "ref_seedfilter"),
+               "rm": os.path.join(HERE, "_ref", "ref_seedfilter_rm")}
+
+# src/main.cpp:152-171: named shapes in the T/0 form GenerateShapePos reads.
+_T_SHAPES = {"12of19": "TTT0T00TT00T0T0TTTT", "14of22": "TTT0T0TT00TT00T0T0TTTT"}
+
+
+def ref_harness_available(mode: str = "plain") -> bool:
+    return os.path.exists(REF_HARNESS[mode])
+
+
+def shape_t_form(shape: str) -> str:
+    return _T_SHAPES.get(shape, shape.replace("1", "T"))
+
+
+def ref_safe_texts(target: bytes, query: bytes) -> tuple[bytes, bytes]:
+    """Inputs on which the reference's find_hsps never indexes its short[4]
+    count arrays with a code >= 4 (src/seed_filter.cu:416-423,567-573): target
+    N/n become lowercase 'a' and query lowercase becomes 'N'.  Seeds are
+    unchanged (both classes invalidate a seed window, common/ntcoding.cpp:10-19)
+    and so is every score (L and N score -1000 against every code, L-N included,
+    src/main.cpp:180-261); only pairs of equal non-ACGT codes disappear."""
+    t = np.frombuffer(target, dtype=np.uint8).copy()
+    t[(t == ord("N")) | (t == ord("n"))] = ord("a")
+    q = np.frombuffer(query, dtype=np.uint8).copy()
+    q[(q >= ord("a")) & (q <= ord("z"))] = ord("N")
+    return t.tobytes(), q.tobytes()
+
+
+def ref_tail_keys(target: bytes, p: Params) -> np.ndarray:
+    """Keys of the seed windows that start within 32 bases (+ seed size) of the
+    target end; a hit on one of them would start a tile past the end."""
+    L = len(target)
+    ss = p.seed_size
+    keys = [lib().or_kmer_index(target, q, C.byref(p)) for q in range(max(L - ss - 31, 0), L - ss + 1)]
+    return np.array([k for k in keys if k != (1 << 31)], dtype=np.uint64)
+
+
+def ref_filter_seeds(seeds: np.ndarray, tail_keys: np.ndarray, query_len: int, seed_size: int = 19) -> np.ndarray:
+    """Drops seeds whose hits could start a tile past a sequence end (the
+    harness refuses them; see oracle/ref_harness.cu)."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    keep = (s & np.uint64(0xFFFFFFFF)) + np.uint64(seed_size + 32) <= np.uint64(query_len)
+    if len(tail_keys):
+        keep &= ~np.isin(s >> np.uint64(32), tail_keys)
+    return s[keep]
+
+
+def ref_seed_and_filter(calls, target: bytes, query: bytes | None = None, *, mode: str = "plain", xdrop=910,
+                        hspthresh=3000, noentropy=False, shape="12of19", transition=False, max_hits: int = 0,
+                        wga_chunk: int = 250_000, step: int = 1, records: bool = True, ambiguous: str = "",
+                        timeout: float = 1200, workdir: str | None = None) -> list[dict]:
+    """Runs the reference's own SeedAndFilter (src/seed_filter.cu:654-778, or
+    repeat_masker_src/seed_filter.cu:723-855 for mode "rm") over `calls` in one
+    process, after its own InitializeInterface / SendRefWriteRequest /
+    InitializeProcessor / GenerateSeedPosTable / SendQueryWriteRequest.
+
+    Each call is a dict: `rev`; `seeds` (uint64 words) or `range` = (j0, j1)
+    for seeds made by the harness as src/seeder.cpp:57-74; rm calls also give
+    `ref_start`, `ref_end`.  Returns per call {"segments" (header row first,
+    its ref_start/query_start zero), "num_seeds", "num_hits", "seconds"}."""
+    import struct
+    import tempfile
+
+    exe = REF_HARNESS[mode]
+    if not os.path.exists(exe):
+        raise FileNotFoundError(f"{exe} missing: run `make -C oracle ref_kernels` where the reference tree is")
+    sm = sub_mat(xdrop, ambiguous)
+    ts = shape_t_form(shape).encode()
+    q = b"" if mode == "rm" else (query or b"")
+    with tempfile.TemporaryDirectory(dir=workdir) as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(b"SAREFIN1")
+            f.write(struct.pack("<IIIiiIII", 1 if mode == "rm" else 0, int(transition), int(noentropy), xdrop,
+                                hspthresh, wga_chunk, step, int(records)))
+            f.write(struct.pack("<qI", int(max_hits), len(ts)) + ts)
+            f.write(sm.astype("<i4").tobytes())
+            f.write(struct.pack("<Q", len(target)) + target)
+            f.write(struct.pack("<Q", len(q)) + q)
+            f.write(struct.pack("<I", len(calls)))
+            for c in calls:
+                a, b = (c["ref_start"], c["ref_end"]) if mode == "rm" else (c.get("buffer", 0), 0)
+                f.write(struct.pack("<III", int(c["rev"]), a, b))
+                if "seeds" in c:
+                    s = np.ascontiguousarray(c["seeds"], dtype="<u8")
+                    f.write(struct.pack("<IQ", 0, len(s)) + s.tobytes())
+                else:
+                    f.write(struct.pack("<III", 1, *c["range"]))
+        r = subprocess.run([exe, fin, fout], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference harness exit {r.returncode}: {r.stderr.strip()[-2000:]}")
+        out = []
+        with open(fout, "rb") as f:
+            assert f.read(8) == b"SAREFOUT"
+            (n_calls,) = struct.unpack("<I", f.read(4))
+            for _ in range(n_calls):
+                n, ns, secs, hlen, hscore = struct.unpack("<QQdIi", f.read(32))
+                segs = np.zeros(n, dtype=SEGMENT_DTYPE)
+                segs[0]["len"], segs[0]["score"] = hlen, hscore
+                if records and n > 1:
+                    segs[1:] = np.frombuffer(f.read(16 * (n - 1)), dtype=SEGMENT_DTYPE)
+                out.append({"segments": segs if records else segs[:1], "num_seeds": ns,
+                            "num_hits": hscore & 0xFFFFFFFF, "num_hsps": hlen, "seconds": secs})
+    return out
+
+
+# --------------------------------------------------------------------------
+# FASTA ingest and blocks (pure Python restatement; small inputs only)
+# --------------------------------------------------------------------------
+def fasta_records(data: bytes):
+    """kseq's reading rules (common/kseq.h:183-224): records start at '>' or
+    '@'; name = header up to the first white space; sequence lines follow
+    until a line starting with '>', '+' or '@'; empty lines are skipped; a
+    line's trailing '\\r' is dropped once the sequence is longer than one
+    character.  FASTA only (no '+' quality sections)."""
+    recs = []
+    i, n = 0, len(data)
+    pending = False
+    while True:
+        if not pending:
+            while i < n and data[i] not in b">@":
+                i += 1
+            if i >= n:
+                return recs
+            i += 1
+        pending = False
+        j = i
+        while j < n and not chr(data[j]).isspace():
+            j += 1
+        if j >= n and j == i:
+            return recs
+        name = data[i:j].decode()
+        i = j
+        if i < n and data[i] != ord("\n"):
+            while i < n and data[i] != ord("\n"):
+                i += 1
+        i += 1  # past the header's newline (or the delimiter)
+        seq = bytearray()
+        while i < n and data[i] not in b">+@":
+            if data[i] == ord("\n"):
+                i += 1
+                continue
+            k = data.find(b"\n", i)
+            k = n if k < 0 else k
+            seq += data[i:k]
+            if len(seq) > 1 and seq[-1] == ord("\r"):
+                seq.pop()
+            i = k + 1
+        if i < n and data[i] in b">@":
+            pending = True
+            i += 1
+        recs.append((name, bytes(seq)))
+        if i >= n:
+            return recs
+
+
+def fasta_blocks(data: bytes, block_size: int = 500_000_000):
+    """Blocks of src/main.cpp:336-455/486-528 -> (text, chroms [(name, start, len)], blocks [(start, len)])."""
+    text = bytearray()
+    chroms, blocks = [], []
+    bstart, blen = 0, 0
+    for name, seq in fasta_records(data):
+        chroms.append((name, len(text), len(seq)))
+        text += seq
+        blen += len(seq)
+        if blen > block_size:
+            blocks.append((bstart, blen))
+            bstart, blen = len(text), 0
+        else:
+            text += b"&"
+            blen += 1
+    if blen > 0:
+        blocks.append((bstart, blen - 1))
+    return bytes(text), chroms, blocks

@@ -51,6 +51,7 @@ EXPORTS = [
     "sa_set_tuning_param", "sa_get_tuning_param",
     "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
     "sa_rm_seeder_run", "sa_free_rm_runs", "sa_format_segments", "sa_format_rm_intervals", "sa_free_text",
+    "sa_fasta_load", "sa_seq_set_free", "sa_align_fasta",
 ]
 
 
@@ -143,6 +144,27 @@ class SeederStats(C.Structure):
                 ("call_seconds", C.c_double), ("copy_seconds", C.c_double)]
 
 
+class SeqSet(C.Structure):
+    _fields_ = [("text", C.c_void_p), ("text_len", C.c_uint64), ("num_chroms", C.c_uint32),
+                ("num_blocks", C.c_uint32), ("names", C.POINTER(C.c_char_p)), ("chrom_start", C.POINTER(C.c_uint64)),
+                ("chrom_len", C.POINTER(C.c_uint32)), ("block_start", C.POINTER(C.c_uint64)),
+                ("block_len", C.POINTER(C.c_uint32)), ("impl", C.c_void_p)]
+
+
+class AlignCfg(C.Structure):
+    _fields_ = [("target_path", C.c_char_p), ("query_path", C.c_char_p), ("segments_path", C.c_char_p),
+                ("hsp_path", C.c_char_p), ("seq_block_size", C.c_uint32), ("interval_size", C.c_uint32),
+                ("interval_overlap", C.c_uint32), ("chunk_size", C.c_uint32), ("strand", C.c_int32),
+                ("num_threads", C.c_int32), ("step", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class AlignStats(C.Structure):
+    _fields_ = [("ref_blocks", C.c_uint64), ("query_blocks", C.c_uint64), ("intervals", C.c_uint64),
+                ("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
+                ("seconds", C.c_double), ("read_seconds", C.c_double), ("table_seconds", C.c_double),
+                ("query_write_seconds", C.c_double), ("overlap_seconds", C.c_double)]
+
+
 _lib = None
 _lib_lock = threading.Lock()
 _P = C.POINTER
@@ -195,6 +217,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
             "sa_seed_and_filter_noalloc": (C.c_int, [u64p, C.c_uint32, C.c_int, C.c_uint32, _P(C.c_uint8),
                                                      C.c_uint64, u64p]),
             "sa_kernel_launches": (C.c_uint64, []),
+            "sa_fasta_load": (C.c_int, [C.c_char_p, C.c_uint32, _P(SeqSet)]),
+            "sa_seq_set_free": (None, [_P(SeqSet)]),
+            "sa_align_fasta": (C.c_int, [_P(AlignCfg), _P(AlignStats)]),
             "sa_serve_start": (C.c_int, [_P(ServeCfg)]),
             "sa_serve_submit": (C.c_int, [C.c_char_p, C.c_uint32, u64p]),
             "sa_serve_wait": (C.c_int, [C.c_uint64, C.c_int, segpp, u64p, segpp, u64p, _P(ServeStats)]),
@@ -484,6 +509,19 @@ class SeedFilter:
     def serve_stop(self) -> None:
         self._chk(self.lib.sa_serve_stop(), "serve_stop")
 
+    def align_fasta(self, target_path: str, query_path: str, segments_path: str | None = None,
+                    hsp_path: str | None = None, seq_block_size: int = 0, interval_size: int = 0,
+                    interval_overlap: int = 0, chunk_size: int = 0, strand: int = 3, num_threads: int = 0,
+                    step: int = 1, shape: str = "12of19", transition: bool = False) -> dict:
+        """Whole-file driver (sa_align_fasta): target blocks, double-buffered query blocks, segments out."""
+        self.lib.sa_host_set_shape(shape.encode(), int(transition))
+        enc = lambda x: x.encode() if x else None  # noqa: E731
+        cfg = AlignCfg(enc(target_path), enc(query_path), enc(segments_path), enc(hsp_path), seq_block_size,
+                       interval_size, interval_overlap, chunk_size, strand, num_threads, step, 0)
+        st = AlignStats()
+        self._chk(self.lib.sa_align_fasta(C.byref(cfg), C.byref(st)), "align_fasta")
+        return {k: getattr(st, k) for k, _ in AlignStats._fields_}
+
     def seeder_run(self, query, buffer: int = 0, strand: int = 3, num_threads: int = 4,
                    interval_size: int = 10_000_000, chunk_size: int = 250_000, interval_overlap: int = 0,
                    max_chunks: int = 0, shape: str = "12of19", transition: bool = False):
@@ -498,6 +536,23 @@ class SeedFilter:
         f = _take_segments(self.lib, fw, fl.value)
         r = _take_segments(self.lib, rc, rl.value)
         return f, r, {k: getattr(st, k) for k, _ in SeederStats._fields_}
+
+
+def fasta_load(path: str, seq_block_size: int = 0) -> dict:
+    """A FASTA file joined into '&'-separated blocks (sa_fasta_load):
+    {"text": bytes, "chroms": [(name, start, len)], "blocks": [(start, len)]}."""
+    lib = load_library()
+    ss = SeqSet()
+    st = lib.sa_fasta_load(path.encode(), seq_block_size, C.byref(ss))
+    if st != 0:
+        raise SegAlignError(st, "fasta_load", (lib.sa_last_error() or b"").decode())
+    try:
+        text = C.string_at(ss.text, ss.text_len) if ss.text_len else b""
+        chroms = [(ss.names[i].decode(), ss.chrom_start[i], ss.chrom_len[i]) for i in range(ss.num_chroms)]
+        blocks = [(ss.block_start[i], ss.block_len[i]) for i in range(ss.num_blocks)]
+    finally:
+        lib.sa_seq_set_free(C.byref(ss))
+    return {"text": text, "chroms": chroms, "blocks": blocks}
 
 
 def _take_text(lib, ptr: C.c_void_p, n: int) -> str:

@@ -19,8 +19,9 @@ OBJ = os.path.join(HERE, "_obj")
 LIB = os.path.join(HERE, "libsegalign_b200.so")
 SYNTH = os.path.join(HERE, "libsa_synth.so")
 
-CU_SOURCES = ["sa_pack.cu", "sa_lookup.cu", "sa_extend.cu", "sa_sort.cu", "sa_api.cu", "sa_host.cpp", "sa_noalloc.cu", "sa_serve.cu", "sa_tune.cu"]
-HEADERS = ["sa_internal.cuh", "sa_launch.h", "sa_radix.cuh"]
+CU_SOURCES = ["sa_pack.cu", "sa_lookup.cu", "sa_extend.cu", "sa_sort.cu", "sa_api.cu", "sa_host.cpp", "sa_noalloc.cu", "sa_serve.cu", "sa_tune.cu",
+              "sa_ingest.cpp"]
+HEADERS = ["sa_internal.cuh", "sa_launch.h", "sa_radix.cuh", "sa_host_internal.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -68,7 +69,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | N
         with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
             list(ex.map(_run, jobs))
     if force or jobs or _stale(LIB, objs):
-        _run([nvcc, "-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([nvcc, "-shared", "-o", LIB] + objs + ["-lcudart", "-lz"])
     synth_src = os.path.join(CSRC, "synth.cpp")
     if force or _stale(SYNTH, [synth_src]):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-o", SYNTH, synth_src])

@@ -398,7 +398,13 @@ void release_slot(Slot* s) {
     g.cv.notify_all();  // waiters for a slot and coalesced callers share the condition
 }
 
-int map_device_error(unsigned long long e) {
+int map_device_error(unsigned long long e) { return sa_map_device_error(e); }
+
+uint64_t max_hits_now();
+
+}  // namespace
+
+int sa_map_device_error(unsigned long long e) {
     switch (e) {
         case 0: return SA_OK;
         case 1: sa_set_error(SA_ERR_BAD_SEED, "seed key outside the 4^K seed table"); return SA_ERR_BAD_SEED;
@@ -409,6 +415,21 @@ int map_device_error(unsigned long long e) {
         default: sa_set_error(SA_ERR_CUDA, "device error %llu", e); return SA_ERR_CUDA;
     }
 }
+
+SaCallGrids sa_call_grids(const SaTuning& t, int num_sms, int mode) {
+    SaCallGrids c;
+    c.range_ctas = std::min(t.call_range_ctas, SA_MAX_CTAS);
+    c.lane_tuning = t;
+    c.lane_ctas = t.call_lane_ctas > 0 ? t.call_lane_ctas : std::max(1, num_sms * t.ext_ctas_per_sm / 2);
+    if (mode == 1) {  // repeat-masker call
+        c.lane_tuning.substeps = t.rm_substeps;
+        c.lane_tuning.switch_now = t.rm_switch_now;
+        c.lane_ctas = t.rm_lane_ctas > 0 ? t.rm_lane_ctas : num_sms * t.ext_ctas_per_sm;
+    }
+    return c;
+}
+
+namespace {
 
 uint64_t max_hits_now() {
     Global& g = G();
@@ -426,7 +447,8 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     DevState& d = g.devs[s->dev_idx];
     SaWork& w = s->w;
     cudaStream_t st = s->stream;
-    const int Gr = std::min(g.tuning.call_range_ctas, SA_MAX_CTAS);
+    const SaCallGrids cg = sa_call_grids(g.tuning, d.num_sms, mode);
+    const int Gr = cg.range_ctas;
     SA_CUDA_OK(cudaMemcpyAsync(w.desc, s->h_desc, sizeof(SaCallDesc), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.units, s->h_units, sizeof(SaUnit), cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, s->h_scope_flags, 4 * SA_MAX_ITERS, cudaMemcpyHostToDevice, st));
@@ -442,15 +464,7 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     xa.xdrop = g.params.xdrop;
     xa.hspthresh = g.params.hspthresh;
     xa.noentropy = g.params.noentropy;
-    SaTuning t = g.tuning;
-    int lane_grid = g.tuning.call_lane_ctas > 0 ? g.tuning.call_lane_ctas
-                                                : std::max(1, d.num_sms * g.tuning.ext_ctas_per_sm / 2);
-    if (mode == 1) {  // repeat-masker call
-        t.substeps = g.tuning.rm_substeps;
-        t.switch_now = g.tuning.rm_switch_now;
-        lane_grid = g.tuning.rm_lane_ctas > 0 ? g.tuning.rm_lane_ctas : d.num_sms * g.tuning.ext_ctas_per_sm;
-    }
-    sa_launch_extend_lane(w, xa, g.params, t, d.num_sms, st, lane_grid);
+    sa_launch_extend_lane(w, xa, g.params, cg.lane_tuning, d.num_sms, st, cg.lane_ctas);
     tm.mark(2);
     sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);
     tm.mark(3);

@@ -165,13 +165,18 @@ __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, ui
                                                uint32_t avail, int neg, int xdrop, int& P, int& B, int& at,
                                                bool& stop) {
     int mn = INT_MAX;
+    // Bases in pairs: the running best and minimum take both prefixes of a
+    // pair with one 3-input max / min (DPX on sm_90 and later).
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-        int t = sa_tbl(tblb, lo, hi, kk);
-        if (EDGE && off0 + kk >= avail) t = neg;
-        P += t;
-        B = max(B, P);
-        mn = min(mn, P);
+    for (int kk = 0; kk < 8; kk += 2) {
+        int t0 = sa_tbl(tblb, lo, hi, kk);
+        int t1 = sa_tbl(tblb, lo, hi, kk + 1);
+        if (EDGE && off0 + kk >= avail) t0 = neg;
+        if (EDGE && off0 + kk + 1 >= avail) t1 = neg;
+        const int P0 = P + t0;
+        P = P0 + t1;
+        B = __vimax3_s32(B, P0, P);
+        mn = __vimin3_s32(mn, P0, P);
     }
     if (!stop) at = B;
     stop = stop || ((B >> SH) - (mn >> SH) > xdrop);

@@ -17,6 +17,7 @@
 
 #include "../../include/segalign_b200.h"
 #include "../../include/segalign_b200_host.h"
+#include "sa_host_internal.h"
 
 namespace {
 
@@ -229,6 +230,72 @@ int sa_build_sub_mat(int xdrop, const char* ambiguous, int* m) {
     return SA_OK;
 }
 
+}  // extern "C"
+
+int sa_host_seed_size() { return g_shape.seed_size; }
+int sa_host_kmer_size() { return g_shape.kmer_size; }
+
+int sa_host_run_calls(const std::vector<SaHostCall>& calls, const char* query, const char* rctext, uint32_t buffer,
+                      int nthreads, std::vector<SaHostCallOut>& res, SaHostRunStats* st) {
+    res.assign(calls.size(), SaHostCallOut());
+    std::atomic<uint64_t> next{0}, nseeds{0}, nhits{0}, nhsps{0};
+    std::atomic<uint64_t> ns_seed{0}, ns_call{0};
+    std::atomic<int> err{0};
+    using SClock = std::chrono::steady_clock;
+    auto ns_since = [](SClock::time_point t) {
+        return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(SClock::now() - t).count();
+    };
+    auto worker = [&]() {
+        std::vector<uint64_t> seeds;
+        while (!err) {
+            uint64_t c = next.fetch_add(1);
+            if (c >= calls.size()) break;
+            const SaHostCall& cl = calls[c];
+            const char* txt = cl.strand ? rctext : query;
+            const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
+            auto t_seed = SClock::now();
+            seeds.resize((uint64_t)(cl.j1 - cl.j0) * per);
+            const uint64_t need = chunk_seeds(g_shape, txt, cl.j0, cl.j1, seeds.data(), seeds.size());
+            ns_seed += ns_since(t_seed);
+            if (need == 0) continue;  // src/seeder.cpp:76
+            sa_segment* out = nullptr;
+            uint64_t ol = 0;
+            auto t_call = SClock::now();
+            int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, buffer, &out, &ol);
+            ns_call += ns_since(t_call);
+            if (r != SA_OK) {
+                err = r;
+                break;
+            }
+            sa_call_stats cs;
+            sa_last_call_stats(&cs);
+            nseeds += need;
+            nhits += cs.num_hits;
+            nhsps += ol - 1;
+            res[c].p = out;
+            res[c].n = ol - 1;
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < std::max(1, nthreads); ++t) th.emplace_back(worker);
+    for (auto& t : th) t.join();
+    if (err) {
+        for (auto& r : res) sa_free_segments(r.p);
+        res.clear();
+        return err;
+    }
+    if (st) {
+        st->num_seeds = nseeds;
+        st->num_hits = nhits;
+        st->num_hsps = nhsps;
+        st->seed_seconds = ns_seed * 1e-9;
+        st->call_seconds = ns_call * 1e-9;
+    }
+    return SA_OK;
+}
+
+extern "C" {
+
 // Seeder pipeline over one query block (src/main.cpp:373-386 intervals,
 // :707 q_len = Lq - seed_size; src/seeder.cpp:47-121 chunks and strands).
 // Calls run on cfg->num_threads host threads; results are concatenated per
@@ -246,11 +313,7 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
     }
     const char* rctext = rcbuf.get();
     const uint32_t qlen_s = query_len - (uint32_t)g_shape.seed_size;
-    struct Call {
-        int strand;
-        uint32_t j0, j1;
-    };
-    std::vector<Call> calls;
+    std::vector<SaHostCall> calls;
     for (uint64_t cur = 0; cur < qlen_s; cur += cfg->interval_size) {
         uint32_t s = (uint32_t)cur;
         uint32_t e = (uint32_t)std::min<uint64_t>(qlen_s, cur + cfg->interval_size + cfg->interval_overlap);
@@ -264,62 +327,16 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
         }
     }
     if (cfg->max_chunks && calls.size() > cfg->max_chunks) calls.resize(cfg->max_chunks);
-    // each call's output array (header + HSPs), kept until the final assembly
-    struct CallOut {
-        sa_segment* p = nullptr;
-        uint64_t n = 0;  // HSPs (without the header)
-    };
-    std::vector<CallOut> res(calls.size());
-    std::atomic<uint64_t> next{0}, nseeds{0}, nhits{0}, nhsps{0};
-    std::atomic<uint64_t> ns_seed{0}, ns_call{0}, ns_copy{0};
-    std::atomic<int> err{0};
+    std::vector<SaHostCallOut> res;
+    SaHostRunStats rs;
+    const int nt = std::max(1, cfg->num_threads);
     using SClock = std::chrono::steady_clock;
-    auto ns_since = [](SClock::time_point t) {
-        return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(SClock::now() - t).count();
-    };
-    auto worker = [&]() {
-        std::vector<uint64_t> seeds;
-        while (!err) {
-            uint64_t c = next.fetch_add(1);
-            if (c >= calls.size()) break;
-            const Call& cl = calls[c];
-            const char* txt = cl.strand ? rctext : query;
-            const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
-            auto t_seed = SClock::now();
-            seeds.resize((uint64_t)(cl.j1 - cl.j0) * per);
-            const uint64_t need = chunk_seeds(g_shape, txt, cl.j0, cl.j1, seeds.data(), seeds.size());
-            ns_seed += ns_since(t_seed);
-            if (need == 0) continue;  // src/seeder.cpp:190
-            sa_segment* out = nullptr;
-            uint64_t ol = 0;
-            auto t_call = SClock::now();
-            int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, cfg->buffer, &out, &ol);
-            ns_call += ns_since(t_call);
-            if (r != SA_OK) {
-                err = r;
-                break;
-            }
-            sa_call_stats cs;
-            sa_last_call_stats(&cs);
-            nseeds += need;
-            nhits += cs.num_hits;
-            nhsps += ol - 1;
-            res[c].p = out;
-            res[c].n = ol - 1;
-        }
-    };
-    int nt = std::max(1, cfg->num_threads);
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t) th.emplace_back(worker);
-    for (auto& t : th) t.join();
+    int err = sa_host_run_calls(calls, query, rctext, cfg->buffer, nt, res, &rs);
+    if (err) return err;
     auto t_asm = SClock::now();
     auto free_all = [&]() {
         for (auto& r : res) sa_free_segments(r.p);
     };
-    if (err) {
-        free_all();
-        return err;
-    }
     // per strand, the calls' HSP lists concatenated in call order: offsets
     // first, then the copies spread over the worker threads
     uint64_t nf = 0, nr = 0;
@@ -354,14 +371,14 @@ int sa_seeder_run(const sa_seeder_cfg* cfg, const char* query, uint32_t query_le
     *fw_len = nf;
     *rc_len = nr;
     if (stats) {
-        stats->num_seeds = nseeds;
-        stats->num_hits = nhits;
-        stats->num_hsps = nhsps;
+        stats->num_seeds = rs.num_seeds;
+        stats->num_hits = rs.num_hits;
+        stats->num_hsps = rs.num_hsps;
         stats->num_calls = calls.size();
         stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        stats->seed_seconds = ns_seed * 1e-9;
-        stats->call_seconds = ns_call * 1e-9;
-        stats->copy_seconds = ns_copy * 1e-9 + std::chrono::duration<double>(SClock::now() - t_asm).count();
+        stats->seed_seconds = rs.seed_seconds;
+        stats->call_seconds = rs.call_seconds;
+        stats->copy_seconds = std::chrono::duration<double>(SClock::now() - t_asm).count();
     }
     return SA_OK;
 }

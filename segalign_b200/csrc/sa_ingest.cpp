@@ -1,0 +1,404 @@
+// sa_ingest.cpp — FASTA ingest, sequence blocks and the whole-file driver
+// with double-buffered query blocks.
+//
+// Reference: src/main.cpp:297-534 reads the query and the target with kseq
+// (common/kseq.h), concatenates their records with '&' into blocks of
+// DEFAULT_SEQ_BLOCK_SIZE (src/graph.h:10), and cuts every query block into
+// intervals; src/main.cpp:594-730 then sends each target block, and streams
+// the query blocks through BUFFER_DEPTH = 2 device buffers: a block is written
+// into a buffer once the seeders have finished every interval of the block
+// that used it, while the seeders work on the other buffer.  Segments of each
+// interval go out in lastz --segments form (src/segment_printer.cpp:51-147).
+//
+// The FASTA reader follows kseq's published parsing rules:
+//   * a record starts at '>' (or '@'); its name runs up to the first white
+//     space, the rest of the header line is a comment;
+//   * sequence lines follow until a line starting with '>', '+' or '@';
+//     empty lines are skipped; every other character is kept as is; a line's
+//     trailing '\r' is dropped once the sequence holds more than one
+//     character;
+//   * after a '+' line (FASTQ) quality lines are read until they are as long
+//     as the sequence; a missing or mismatched quality ends the input;
+//   * gzip-compressed and plain files are read alike (zlib).
+#include <zlib.h>
+
+#include <algorithm>
+#include <cctype>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/segalign_b200.h"
+#include "../../include/segalign_b200_host.h"
+#include "sa_host_internal.h"
+
+namespace {
+
+class FastaReader {
+  public:
+    explicit FastaReader(const char* path) : f_(gzopen(path, "r")) {}
+    ~FastaReader() {
+        if (f_) gzclose(f_);
+    }
+    bool ok() const { return f_ != nullptr; }
+
+    // Next record; false at the end of the input (or on a truncated FASTQ record).
+    bool next(std::string& name, std::string& seq) {
+        int c;
+        if (!pending_) {  // skip to the next header character
+            while ((c = getc()) >= 0 && c != '>' && c != '@') {
+            }
+            if (c < 0) return false;
+        }
+        pending_ = false;
+        name.clear();
+        seq.clear();
+        // name: up to the first white space
+        bool any = false;
+        while ((c = getc()) >= 0 && !std::isspace(c)) {
+            name.push_back((char)c);
+            any = true;
+        }
+        if (c < 0 && !any) return false;
+        if (c >= 0 && c != '\n')  // comment: the rest of the header line
+            while ((c = getc()) >= 0 && c != '\n') {
+            }
+        // sequence lines
+        while ((c = getc()) >= 0 && c != '>' && c != '+' && c != '@') {
+            if (c == '\n') continue;
+            seq.push_back((char)c);
+            int d;
+            while ((d = getc()) >= 0 && d != '\n') seq.push_back((char)d);
+            if (seq.size() > 1 && seq.back() == '\r') seq.pop_back();
+        }
+        if (c == '>' || c == '@') pending_ = true;
+        if (c != '+') return true;
+        // FASTQ quality: skip the '+' line, then quality lines up to the sequence length
+        while ((c = getc()) >= 0 && c != '\n') {
+        }
+        if (c < 0) return false;
+        size_t ql = 0;
+        while (ql < seq.size()) {
+            size_t line = 0;
+            int d;
+            bool got = false;
+            while ((d = getc()) >= 0 && d != '\n') {
+                ++line;
+                got = true;
+            }
+            if (!got && d < 0) break;
+            ql += line;
+            if (d < 0) break;
+        }
+        return ql == seq.size();
+    }
+
+  private:
+    int getc() {
+        if (pos_ >= len_) {
+            if (eof_) return -1;
+            int n = gzread(f_, buf_, sizeof buf_);
+            if (n <= 0) {
+                eof_ = true;
+                return -1;
+            }
+            len_ = n;
+            pos_ = 0;
+        }
+        return (unsigned char)buf_[pos_++];
+    }
+    gzFile f_;
+    char buf_[1 << 16];
+    int pos_ = 0, len_ = 0;
+    bool eof_ = false, pending_ = false;
+};
+
+struct SeqSetImpl {
+    std::string text;
+    std::vector<std::string> names;
+    std::vector<const char*> name_ptrs;
+    std::vector<uint64_t> chrom_start;
+    std::vector<uint32_t> chrom_len;
+    std::vector<uint64_t> block_start;
+    std::vector<uint32_t> block_len;
+};
+
+// Records joined into blocks as src/main.cpp:336-455 (query) and :486-528
+// (target) join them: each record is appended at the running position; a
+// block closes after the record that takes its length above block_size (no
+// '&' after that record), otherwise a '&' follows the record; the last block
+// drops its trailing '&' from its length.
+int load_fasta(const char* path, uint64_t block_size, SeqSetImpl& s) {
+    FastaReader rd(path);
+    if (!rd.ok()) {
+        sa_set_error(SA_ERR_ARG, "cannot open FASTA file %s", path);
+        return SA_ERR_ARG;
+    }
+    std::string name, seq;
+    uint64_t blk_len = 0;
+    s.block_start.push_back(0);
+    while (rd.next(name, seq)) {
+        s.names.push_back(name);
+        s.chrom_start.push_back(s.text.size());
+        s.chrom_len.push_back((uint32_t)seq.size());
+        s.text += seq;
+        blk_len += seq.size();
+        if (blk_len > block_size) {
+            s.block_len.push_back((uint32_t)blk_len);
+            s.block_start.push_back(s.text.size());
+            blk_len = 0;
+        } else {
+            s.text.push_back('&');
+            blk_len += 1;
+        }
+    }
+    if (blk_len > 0) {
+        s.block_len.push_back((uint32_t)(blk_len - 1));
+    } else {
+        s.block_start.pop_back();  // the last record closed a block: no open block follows
+    }
+    for (auto& n : s.names) s.name_ptrs.push_back(n.c_str());
+    return SA_OK;
+}
+
+void fill_view(SeqSetImpl* impl, sa_seq_set* out) {
+    out->text = impl->text.data();
+    out->text_len = impl->text.size();
+    out->num_chroms = (uint32_t)impl->names.size();
+    out->num_blocks = (uint32_t)impl->block_len.size();
+    out->names = impl->name_ptrs.data();
+    out->chrom_start = impl->chrom_start.data();
+    out->chrom_len = impl->chrom_len.data();
+    out->block_start = impl->block_start.data();
+    out->block_len = impl->block_len.data();
+    out->impl = impl;
+}
+
+sa_chrom_table table_of(const SeqSetImpl& s) {
+    sa_chrom_table t;
+    t.names = s.name_ptrs.data();
+    t.starts = s.chrom_start.data();
+    t.lens = s.chrom_len.data();
+    t.count = (uint32_t)s.names.size();
+    t.pad = 0;
+    return t;
+}
+
+double secs_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+}
+
+}  // namespace
+
+extern "C" {
+
+int sa_fasta_load(const char* path, uint32_t seq_block_size, sa_seq_set* out) {
+    if (!path || !out) return SA_ERR_ARG;
+    auto* impl = new SeqSetImpl();
+    int r = load_fasta(path, seq_block_size ? seq_block_size : 500000000u, *impl);
+    if (r != SA_OK) {
+        delete impl;
+        return r;
+    }
+    fill_view(impl, out);
+    return SA_OK;
+}
+
+void sa_seq_set_free(sa_seq_set* s) {
+    if (!s) return;
+    delete static_cast<SeqSetImpl*>(s->impl);
+    std::memset(s, 0, sizeof *s);
+}
+
+// src/main.cpp:297-730 for one target file and one query file, processor
+// already initialised (sa_initialize_interface, sa_generate_shape_pos,
+// sa_initialize_processor).
+int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
+    if (!cfg_in || !cfg_in->target_path || !cfg_in->query_path) return SA_ERR_ARG;
+    auto t_all = std::chrono::steady_clock::now();
+    sa_align_cfg cfg = *cfg_in;
+    if (!cfg.seq_block_size) cfg.seq_block_size = 500000000u;
+    if (!cfg.interval_size) cfg.interval_size = 10000000u;
+    if (!cfg.chunk_size) cfg.chunk_size = 250000u;
+    if (!cfg.strand) cfg.strand = 3;
+    if (!cfg.num_threads) cfg.num_threads = 16;
+    if (!cfg.step) cfg.step = 1;
+    const int seed_size = sa_host_seed_size();
+    sa_align_stats st{};
+
+    // query first, then target (src/main.cpp:297-534)
+    SeqSetImpl Q, T;
+    auto t_read = std::chrono::steady_clock::now();
+    int r = load_fasta(cfg.query_path, cfg.seq_block_size, Q);
+    if (r == SA_OK) r = load_fasta(cfg.target_path, cfg.seq_block_size, T);
+    if (r != SA_OK) return r;
+    st.read_seconds = secs_since(t_read);
+    st.ref_blocks = T.block_len.size();
+    st.query_blocks = Q.block_len.size();
+    const sa_chrom_table ttab = table_of(T), qtab = table_of(Q);
+
+    FILE* seg = nullptr;
+    FILE* hsp = nullptr;
+    if (cfg.segments_path && !(seg = fopen(cfg.segments_path, "wb"))) {
+        sa_set_error(SA_ERR_ARG, "cannot open %s", cfg.segments_path);
+        return SA_ERR_ARG;
+    }
+    if (cfg.hsp_path && !(hsp = fopen(cfg.hsp_path, "wb"))) {
+        if (seg) fclose(seg);
+        sa_set_error(SA_ERR_ARG, "cannot open %s", cfg.hsp_path);
+        return SA_ERR_ARG;
+    }
+    const uint32_t nq = (uint32_t)Q.block_len.size();
+    for (uint32_t rb = 0; rb < T.block_len.size() && r == SA_OK; ++rb) {
+        const char* rtext = T.text.data();
+        const uint64_t rstart = T.block_start[rb];
+        const uint32_t rlen = T.block_len[rb];
+        auto t_tab = std::chrono::steady_clock::now();
+        if (rb > 0) sa_clear_ref();
+        r = sa_send_ref_write_request(rtext, rstart, rlen);
+        if (r == SA_OK) r = sa_generate_seed_pos_table(rtext, rstart, rlen, cfg.step, seed_size, sa_host_kmer_size());
+        st.table_seconds += secs_since(t_tab);
+        if (r != SA_OK) break;
+
+        // The loader writes query block k into buffer k % 2 once the seeders
+        // have released that buffer (block k - 2 done), while the seeders run
+        // block k - 1 from the other buffer.
+        std::mutex mu;
+        std::condition_variable cv;
+        std::vector<int> loaded(nq, 0);  // 1 loaded, -1 failed
+        int done_upto = -1;               // blocks [0, done_upto] finished seeding
+        bool abort = false;
+        std::string rc_text[2];
+        double write_s = 0, overlap_s = 0;
+        std::thread loader([&]() {
+            for (uint32_t k = 0; k < nq; ++k) {
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    cv.wait(lk, [&] { return abort || (int)k - 2 <= done_upto; });
+                    if (abort) return;
+                }
+                const uint32_t b = k & 1;
+                const uint64_t qs = Q.block_start[k];
+                const uint32_t ql = Q.block_len[k];
+                auto t0 = std::chrono::steady_clock::now();
+                const bool busy = (int)k - 1 > done_upto;  // the seeders are still on the other buffer
+                rc_text[b].resize(ql);
+                sa_host_revcomp(&rc_text[b][0], Q.text.data() + qs, ql);
+                int w = sa_send_query_write_request(Q.text.data(), qs, ql, b);
+                const double dt = secs_since(t0);
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    write_s += dt;
+                    if (busy) overlap_s += dt;
+                    loaded[k] = w == SA_OK ? 1 : -1;
+                }
+                cv.notify_all();
+                if (w != SA_OK) return;
+            }
+        });
+        for (uint32_t k = 0; k < nq && r == SA_OK; ++k) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return loaded[k] != 0; });
+                if (loaded[k] < 0) {
+                    r = SA_ERR_STATE;
+                    break;
+                }
+            }
+            const uint32_t b = k & 1;
+            const uint64_t qs = Q.block_start[k];
+            const uint32_t ql = Q.block_len[k];
+            if (ql > (uint32_t)seed_size) {
+                // intervals over [0, Lq - seed_size) (src/main.cpp:373-386, :707)
+                const uint32_t qlen_s = ql - (uint32_t)seed_size;
+                std::vector<SaHostCall> calls;
+                std::vector<uint32_t> call_iv;
+                uint32_t niv = 0;
+                for (uint64_t cur = 0; cur < qlen_s; cur += cfg.interval_size, ++niv) {
+                    const uint32_t s = (uint32_t)cur;
+                    const uint32_t e = (uint32_t)std::min<uint64_t>(qlen_s, cur + cfg.interval_size + cfg.interval_overlap);
+                    if (cfg.strand & 1)
+                        for (uint64_t i = s; i < e; i += cfg.chunk_size) {
+                            calls.push_back({0, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg.chunk_size, e)});
+                            call_iv.push_back(niv);
+                        }
+                    if (cfg.strand & 2) {
+                        const uint32_t rs = qlen_s - e, re = qlen_s - s;
+                        for (uint64_t i = rs; i < re; i += cfg.chunk_size) {
+                            calls.push_back({1, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg.chunk_size, re)});
+                            call_iv.push_back(niv);
+                        }
+                    }
+                }
+                std::vector<SaHostCallOut> res;
+                SaHostRunStats rs;
+                r = sa_host_run_calls(calls, Q.text.data() + qs, rc_text[b].data(), b, cfg.num_threads, res, &rs);
+                if (r == SA_OK) {
+                    st.num_seeds += rs.num_seeds;
+                    st.num_hits += rs.num_hits;
+                    st.num_hsps += rs.num_hsps;
+                    st.intervals += niv;
+                    // per interval: plus-strand lists then minus-strand lists, call order
+                    size_t c = 0;
+                    for (uint32_t iv = 0; iv < niv; ++iv) {
+                        std::vector<sa_segment> fw, rc;
+                        for (; c < calls.size() && call_iv[c] == iv; ++c) {
+                            if (!res[c].p) continue;
+                            auto& dst = calls[c].strand ? rc : fw;
+                            dst.insert(dst.end(), res[c].p + 1, res[c].p + 1 + res[c].n);
+                        }
+                        if (hsp) {
+                            for (int sd = 0; sd < 2; ++sd)
+                                for (const sa_segment& h : sd ? rc : fw) {
+                                    const uint32_t key[4] = {rb, k, iv, (uint32_t)sd};
+                                    fwrite(key, 4, 4, hsp);
+                                    fwrite(&h, sizeof h, 1, hsp);
+                                }
+                        }
+                        if (seg && (fw.size() || rc.size())) {
+                            char *pt = nullptr, *mt = nullptr;
+                            uint64_t pl = 0, ml = 0;
+                            int f = sa_format_segments(&ttab, rstart, &qtab, qs, ql, fw.data(), fw.size(), rc.data(),
+                                                       rc.size(), &pt, &pl, &mt, &ml);
+                            if (f == SA_OK) {
+                                fwrite(pt, 1, pl, seg);
+                                fwrite(mt, 1, ml, seg);
+                            }
+                            sa_free_text(pt);
+                            sa_free_text(mt);
+                            if (f != SA_OK) r = f;
+                        }
+                    }
+                    for (auto& x : res) sa_free_segments(x.p);
+                }
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                done_upto = (int)k;
+                if (r != SA_OK) abort = true;
+            }
+            cv.notify_all();
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            abort = true;  // no further blocks for this target block
+        }
+        cv.notify_all();
+        loader.join();
+        st.query_write_seconds += write_s;
+        st.overlap_seconds += overlap_s;
+    }
+    if (seg) fclose(seg);
+    if (hsp) fclose(hsp);
+    st.seconds = secs_since(t_all);
+    if (stats) *stats = st;
+    return r;
+}
+
+}  // extern "C"

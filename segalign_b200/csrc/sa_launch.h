@@ -218,6 +218,20 @@ struct SaResidentView {
 };
 int sa_resident_view(uint32_t buffer, SaResidentView* v);
 
+// Grids and lane-kernel settings of one plain (mode 0) or repeat-masker
+// (mode 1) call: CTAs of the range-partitioned kernels (lookup, dedup), CTAs of
+// the lane kernel, and the tuning the lane kernel runs with.
+struct SaCallGrids {
+    int range_ctas;
+    int lane_ctas;
+    SaTuning lane_tuning;
+};
+SaCallGrids sa_call_grids(const SaTuning& t, int num_sms, int mode);
+
+// Status code (and sa_last_error message) of a device-detected error code
+// of SaCounters::error.
+int sa_map_device_error(unsigned long long e);
+
 // Counts kernel launches of this library (reported by sa_kernel_launches()).
 void sa_note_launch();
 

@@ -181,7 +181,9 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     SA_CUDA_OK(cudaMemcpyAsync(w.desc, &desc, sizeof desc, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.units, &unit, sizeof unit, cudaMemcpyHostToDevice, st));
     SA_CUDA_OK(cudaMemcpyAsync(w.scope_flags, flags, sizeof flags, cudaMemcpyHostToDevice, st));
-    const int G = std::min(v.tuning.range_ctas, SA_MAX_CTAS);
+    // the grids and lane-kernel settings of a plain call (sa_seed_and_filter)
+    const SaCallGrids cg = sa_call_grids(v.tuning, v.num_sms, 0);
+    const int G = cg.range_ctas;
     sa_launch_lookup_seeds(w, v.index, (uint32_t)v.nbuckets, v.params, G, st);
     if (!w.hash_clean) sa_launch_hash_clear(w, st);
     w.hash_clean = false;
@@ -194,7 +196,7 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
     xa.xdrop = v.params.xdrop;
     xa.hspthresh = v.params.hspthresh;
     xa.noentropy = v.params.noentropy;
-    sa_launch_extend_lane(w, xa, v.params, v.tuning, v.num_sms, st);
+    sa_launch_extend_lane(w, xa, v.params, cg.lane_tuning, v.num_sms, st, cg.lane_ctas);
     sa_launch_extend_warp(w, xa, v.params, v.tuning, v.num_sms, st);
     sa_launch_dedup(w, 0, 0, G, st);
     SA_CUDA_OK(cudaGetLastError());
@@ -207,10 +209,7 @@ int sa_seed_and_filter_noalloc(const uint64_t* seeds, uint32_t num_seeds, int re
         sa_set_error(SA_ERR_CAPACITY, "more than %u distinct HSPs (no-allocation limit)", SA_NOALLOC_MAX_SURVIVORS);
         return SA_ERR_CAPACITY;
     }
-    if (c.error) {
-        sa_set_error(SA_ERR_CUDA, "device error %llu", (unsigned long long)c.error);
-        return c.error == 1 || c.error == 5 ? SA_ERR_BAD_SEED : SA_ERR_MAX_HITS;
-    }
+    if (c.error) return sa_map_device_error(c.error);
     const uint64_t nh = c.uniq_count;
     *out_len = nh + 1;
     if (nh + 1 > out_cap) {

@@ -62,3 +62,33 @@ def test_noalloc_rejects_more_seeds_than_its_limit(sf):
     sf.initialize_processor(False, 250_000, 19, build_sub_mat(910), 910, 3000, False)
     seeds = host_seeds(sf.w.query, 750_000, 999_000)
     compare_segments(sf.seed_and_filter_noalloc(seeds, False, 0), sf.seed_and_filter(seeds, False, 0), "re-init")
+
+
+def test_noalloc_distinct_hsp_limit_then_next_call_recovers(built):
+    """A call with more distinct HSPs than the shared array's HSP set holds
+    (262,144) fails with SA_ERR_CAPACITY; it leaves the set dirty, and the next
+    call through the same array must still equal the regular entry point."""
+    from tests.helpers import random_text
+
+    rng = np.random.default_rng(7)
+    T = random_text(rng, 12_000_000)
+    Q = random_text(rng, 300_000)
+    f = SeedFilter()
+    f.initialize_interface(1)
+    f.generate_shape_pos("12of19")
+    # hspthresh 300: almost every random hit is kept, each with its own HSP
+    f.initialize_processor(False, 250_000, 19, build_sub_mat(910), 910, 300, False)
+    f.send_ref_write_request(T)
+    f.generate_seed_pos_table(None, 1, 19, 12)
+    f.send_query_write_request(Q, 0)
+    seeds = host_seeds(Q, 0, 250_000)
+    want = f.seed_and_filter(seeds, False, 0)
+    assert len(want) - 1 > 262_144
+    big = np.zeros(len(want) + 16, dtype=want.dtype)  # room for the output: only the HSP set can overflow
+    with pytest.raises(SegAlignError) as e:
+        f.seed_and_filter_noalloc(seeds, False, 0, out=big)
+    assert e.value.code == -8 and "distinct HSPs" in str(e.value)
+    for a, b in ((0, 40_000), (100_000, 160_000)):
+        s = host_seeds(Q, a, b)
+        compare_segments(f.seed_and_filter_noalloc(s, False, 0), f.seed_and_filter(s, False, 0),
+                         f"after the overflow [{a},{b})")
