@@ -9,18 +9,26 @@ target blocks of 1-50 kbp at 15-35% divergence (5% inverted), 12% repeats,
 overlap cut into 250 kbp SeedAndFilter units.
 
 One step = one pass of the hot path over the whole query (both strands):
-  value  batched form, target table + query resident in HBM, seeds generated
-         on the GPU, HSPs left in HBM; device time from CUDA events on the
-         library's stream;
+  value  batched form, target table + query text resident in HBM: device
+         seeding (per-position keys recomputed every step), lookup, X-drop,
+         dedup, and the HSP lists copied to the host per unit; CUDA events
+         on the current stream bracket each step (the calls return once the
+         lists are on the host; device-only event time of the library's
+         stream beside it);
   e2e    the reference-facing C ABI: the C++ seeder builds each unit's seed
          words on the host and calls sa_seed_and_filter(), which copies them to
          the GPU and copies the HSP list back (host wall time);
   e2e_batched  host query text -> GPU -> batched call -> HSP lists on the host.
-Ranks (torchrun) are weak-scaled: each rank runs its own genome pair of the
-same shape; value = all ranks' extensions / the slowest rank's time.
+Beside them: like-for-like batched/plain ratios, uneven windows, serving on
+the resident table, an unranked timing of the reference's own kernels on a
+sample of the same units, the CPU port on a bounded sample, and the 600 Mbp
+legs (batched and plain with transitions, serving on that table, repeat-masker
+self-alignment).  Ranks (torchrun) are weak-scaled: each rank runs its own
+genome pair of the same shape; value = all ranks' extensions / the slowest
+rank's time.
 
 --impl reference times the reference semantics on the host cores (the CPU
-port in oracle/, the reference's own kernels being GPU-only), rank 0 only.
+port in oracle/), rank 0 only.
 """
 from __future__ import annotations
 
@@ -57,13 +65,24 @@ def parse_args():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--serve-requests", type=int, default=None,
-                    help="requests per load in the serving leg (default 48; 16 for --workload large)")
+                    help="requests per load in the genome serving leg (default 200)")
+    ap.add_argument("--large-serve-requests", type=int, default=24,
+                    help="requests per load in the serving leg on the 600 Mbp table")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 600 Mbp legs (batched and plain with transitions, serving, repeat masker)")
+    ap.add_argument("--large-cpu-units", type=int, default=0,
+                    help="units of the 600 Mbp leg also run through the CPU port (0 = none: its table build "
+                         "takes minutes on the host)")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the unranked timing of the reference's own kernels (oracle/_ref)")
+    ap.add_argument("--ref-gpu-units", type=int, default=16,
+                    help="250 kbp units of the genome workload timed through the reference's own kernels")
     ap.add_argument("--workload", choices=["genome", "large"], default="genome",
                     help="genome: 100 Mbp x 108 Mbp (the headline); large: 600 Mbp x 600 Mbp with transitions, "
                          "a query sample of --query-sample bases against the whole target")
     ap.add_argument("--query-sample", type=int, default=12_000_000, help="query bases used by --workload large")
-    ap.add_argument("--rm-intervals", type=int, default=4,
-                    help="--workload large: repeat-masker intervals run on the 600 Mbp target (0 = skip)")
+    ap.add_argument("--rm-intervals", type=int, default=8,
+                    help="repeat-masker intervals run on the 600 Mbp target (0 = skip)")
     return ap.parse_args()
 
 
@@ -269,23 +288,25 @@ def run_uneven(sf, query_len: int, chunked_outs, chunked_units) -> dict:
             "bit_exact_distinct_vs_250kbp_chunks": bool(exact), "autotune_quick": tuned}
 
 
-def run_serving(sf, target: bytes, n_req: int, table: str) -> dict:
-    """Serving leg: capacity from a closed-loop burst, then Poisson arrivals at
-    0.5x, 1x and 2x of it; latency = submission -> HSP lists on the host."""
+def run_serving(sf, target: bytes, n_req: int, table: str, bursts: int = 3) -> dict:
+    """Serving leg: capacity = median rate of `bursts` closed-loop bursts of
+    the request set (after one untimed burst that grows the request-buffer
+    pool and pinned output buffers), then Poisson arrivals at 0.5x, 1x and 2x
+    of it; latency = submission -> HSP lists on the host."""
     reqs = serve_requests(target, n_req, seed=105)
     sf.serve_start(interval_size=INTERVAL, interval_overlap=OVERLAP, chunk_size=CHUNK, strands=3)
     try:
         alone = {}
         for k in range(4):  # a sample run alone, to compare with the same requests in the mix
             alone[k] = sf.serve_wait(sf.serve_submit(reqs[k]))[:2]
-        # capacity: everything submitted at once (one untimed burst first, so
-        # that the request-buffer pool and pinned output buffers are grown)
         for r in [sf.serve_submit(q) for q in reqs]:
             sf.serve_wait(r)
-        ids = [sf.serve_submit(q) for q in reqs]
-        st = [sf.serve_wait(r)[2] for r in ids]
-        span = max(x["done_s"] for x in st) - min(x["submit_s"] for x in st)
-        cap = len(reqs) / span
+        caps = []
+        for _ in range(bursts):
+            ids = [sf.serve_submit(q) for q in reqs]
+            st = [sf.serve_wait(r)[2] for r in ids]
+            caps.append(len(reqs) / (max(x["done_s"] for x in st) - min(x["submit_s"] for x in st)))
+        cap = float(statistics.median(caps))
         rates = []
         exact = True
         for load in (0.5, 1.0, 2.0):
@@ -317,7 +338,47 @@ def run_serving(sf, target: bytes, n_req: int, table: str) -> dict:
     return {"workload": f"{n_req} requests per load, lengths log-uniform 10 kbp-20 Mbp (mean "
                         f"{np.mean([len(q) for q in reqs]) / 1e6:.2f} Mbp), 30% target blocks at 20% divergence, "
                         f"both strands, against the resident {table}",
-            "capacity_rps": cap, "loads": rates, "bit_exact_alone_vs_mix": bool(exact)}
+            "capacity_rps": cap, "capacity_bursts_rps": caps, "loads": rates,
+            "bit_exact_alone_vs_mix": bool(exact)}
+
+
+def ref_gpu_baseline(sf, w, calls, n_units: int) -> dict:
+    """Unranked: the reference's own SeedAndFilter (src/seed_filter.cu, compiled
+    unmodified for sm_100a, oracle/ref_harness.cu) on the first n_units units
+    of the workload, per-call wall time on this GPU, and whether its outputs
+    equal ours call by call.  Inputs pass through oracle.ref_safe_texts, which
+    changes no seed and no score (our results on them equal those on the
+    original texts), and seeds the harness would refuse are dropped on both
+    sides."""
+    import oracle
+    from segalign_b200 import host_revcomp, host_seeds
+
+    if not oracle.ref_harness_available("plain"):
+        return {"unavailable": "oracle/_ref/ref_seedfilter not built (needs the reference tree at build time)"}
+    T, Q = oracle.ref_safe_texts(w.target, w.query)
+    p = oracle.params()
+    tk = oracle.ref_tail_keys(T, p)
+    rct = host_revcomp(Q)
+    sample = []
+    for (_, rev, a, b) in calls[:n_units]:
+        seeds = oracle.ref_filter_seeds(host_seeds(rct if rev else Q, a, b), tk, len(Q))
+        if len(seeds):
+            sample.append({"rev": rev, "seeds": seeds})
+    t0 = time.perf_counter()
+    ref = oracle.ref_seed_and_filter(sample, T, Q, timeout=900)
+    harness_s = time.perf_counter() - t0
+    exact = True
+    for c, r in zip(sample, ref):
+        got = sf.seed_and_filter(c["seeds"], bool(c["rev"]), 0)
+        exact = exact and len(got) == len(r["segments"]) and \
+            np.array_equal(got.view(np.uint32)[2:], r["segments"].view(np.uint32)[2:])
+    secs = sum(r["seconds"] for r in ref)
+    hits = sum(r["num_hits"] for r in ref)
+    return {"value": hits / secs, "unit": UNIT, "calls": len(ref), "extensions": hits, "seconds": secs,
+            "hsps": int(sum(r["num_hsps"] for r in ref)), "harness_wall_s": harness_s,
+            "kind": "reference src/seed_filter.cu SeedAndFilter compiled for sm_100a, one call at a time, "
+                    "per-call wall time (host vectors in and out)",
+            "bit_exact_vs_ours": bool(exact)}
 
 
 def allreduce_value(x: float, op: str, dist=None, device: str = "cuda") -> float:
@@ -391,10 +452,61 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Our implementation
 # ---------------------------------------------------------------------------
+def timed_batch_steps(sf, units, steps: int, flush, barrier):
+    """`steps` timed passes of the batched form, each from the resident query
+    text to the HSP lists on the host: device seeding (per-position keys
+    recomputed), lookup, extension, dedup, the records' copy to the host and
+    their per-unit lists.  Returns per-step wall seconds, device milliseconds
+    (CUDA events of the library's stream) and the last step's statistics."""
+    import torch
+
+    wall, dev, lane, warp, lk, dd = [], [], [], [], [], []
+    outs = st = None
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        # CUDA events on the current stream bracket the step: the calls return
+        # only once the HSP lists are on the host, so the end event is taken
+        # after the whole step
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sf.refresh_query_keys(0)
+        outs = sf.seed_and_filter_batch(units)
+        e1.record()
+        e1.synchronize()
+        wall.append(e0.elapsed_time(e1) / 1000.0)
+        st = sf.last_call_stats()
+        dev.append(st["ms_total"])
+        lane.append(st["ms_extend_lane"])
+        warp.append(st["ms_extend_warp"])
+        lk.append(st["ms_lookup"])
+        dd.append(st["ms_dedup"])
+    barrier()
+    mean = lambda x: sum(x) / len(x)  # noqa: E731
+    return {"wall_s": wall, "dev_ms": mean(dev), "lane_ms": mean(lane), "warp_ms": mean(warp), "lookup_ms": mean(lk),
+            "dedup_ms": mean(dd), "stats": st, "outs": outs}
+
+
+def plain_device_ms(sf, w, calls) -> float:
+    """Device time of the plain path: every unit as its own sa_seed_and_filter
+    call, one at a time, summed over the units (CUDA events per call)."""
+    from segalign_b200 import host_revcomp, host_seeds
+
+    rct = host_revcomp(w.query)
+    sf.set_timing(True)
+    total = 0.0
+    for (_, rev, a, b) in calls:
+        seeds = host_seeds(rct if rev else w.query, a, b)
+        if len(seeds):
+            sf.seed_and_filter(seeds, bool(rev), 0)
+            total += sf.last_call_stats()["ms_total"]
+    return total
+
+
 def run_ours(args):
     import torch
 
-    from segalign_b200 import SeedFilter, build_sub_mat, synth
+    from segalign_b200 import SeedFilter, build_sub_mat
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -438,31 +550,20 @@ def run_ours(args):
     sf.set_timing(True)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
-    # ---- value: batched, device resident ----
+    # ---- value: batched form, query text resident -> HSP lists on the host ----
     for _ in range(args.warmup):
-        sf.seed_and_filter_batch(units, keep_on_device=True)
+        sf.refresh_query_keys(0)
+        sf.seed_and_filter_batch(units)
     barrier()
     l0 = sf.kernel_launches()
-    dev_ms, hits, hsps, lane_ms, warp_ms, surv, tiles, nnz, longs = [], 0, 0, [], [], 0, 0, 0, 0
-    lk_ms, dd_ms = [], []
     with ClockSampler(gpu_index(local)) as clk:
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            sf.seed_and_filter_batch(units, keep_on_device=True)
-            st = sf.last_call_stats()
-            dev_ms.append(st["ms_total"])
-            lane_ms.append(st["ms_extend_lane"])
-            warp_ms.append(st["ms_extend_warp"])
-            lk_ms.append(st["ms_lookup"])
-            dd_ms.append(st["ms_dedup"])
-            hits, hsps, surv, tiles, nnz, longs = (st["num_hits"], st["num_hsps"], st["survivors"], st["tiles"],
-                                                   st["seeds_with_hits"], st["long_hits"])
-        barrier()
-        wall_s = time.perf_counter() - t0
+        tb = timed_batch_steps(sf, units, args.steps, flush, barrier)
     launches = sf.kernel_launches() - l0
-    ms_step = sum(dev_ms) / len(dev_ms)
+    st = tb["stats"]
+    outs = tb["outs"]
+    hits, hsps, surv, tiles, nnz, longs = (st["num_hits"], st["num_hsps"], st["survivors"], st["tiles"],
+                                           st["seeds_with_hits"], st["long_hits"])
+    ms_step = 1000.0 * sum(tb["wall_s"]) / len(tb["wall_s"])
     job = job_figures(ms_step, float(hits), float(hsps), dist)
     ms_step_max, hits_all, hsps_all, value = job["ms_per_step"], job["extensions"], job["hsps"], job["value"]
 
@@ -470,9 +571,8 @@ def run_ours(args):
     # = 24 B per hit-bearing seed (E, lo, j, scope, unit) + 4 B per hit (pos)
     # + 24 B per 32-base tile scanned (2 sequences x 32 bases x 3 bits)
     # + 16 B per surviving HSP record
-    lane_ms_avg = sum(lane_ms) / len(lane_ms)
-    st_tiles = tiles
-    alg_bytes = 24.0 * nnz + 4.0 * hits + 24.0 * st_tiles + 16.0 * surv
+    lane_ms_avg = tb["lane_ms"]
+    alg_bytes = 24.0 * nnz + 4.0 * hits + 24.0 * tiles + 16.0 * surv
     peak, peak_src = peaks()
     achieved = alg_bytes / (lane_ms_avg / 1000.0) / 1e9
     traffic, traffic_src = lane_traffic(hits, args.workload)
@@ -485,19 +585,19 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic",
-        "config": {"workload": desc, "path": "batched, device-resident", "units": len(units),
-                   "target_bp": len(w.target), "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)",
-                   "scale": args.scale},
+        "config": {"workload": desc, "path": "batched: resident query text -> device seeding, lookup, X-drop, dedup "
+                   "-> HSP lists on the host", "units": len(units), "target_bp": len(w.target),
+                   "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)", "scale": args.scale},
         "hsps_per_s": hsps_all / (ms_step_max / 1000.0),
         "extensions_per_step": hits_all, "hsps_per_step": hsps_all,
-        "phase_ms": {"lookup": sum(lk_ms) / len(lk_ms), "extend_lane": lane_ms_avg,
-                     "extend_warp": sum(warp_ms) / len(warp_ms), "dedup": sum(dd_ms) / len(dd_ms),
-                     "wall_per_step": 1000 * wall_s / args.steps},
+        "device_ms_per_step": tb["dev_ms"],
+        "phase_ms": {"lookup": tb["lookup_ms"], "extend_lane": lane_ms_avg, "extend_warp": tb["warp_ms"],
+                     "dedup": tb["dedup_ms"], "device_total": tb["dev_ms"], "wall_per_step": ms_step},
         "table_build_ms": table_ms,
         "roofline": roofline,
         "gpu_launches": launches,
         "clocks": clk.summary(),
-        "counts": {"survivors": surv, "long_hits": longs, "tiles": st_tiles, "seeds_with_hits": nnz},
+        "counts": {"survivors": surv, "long_hits": longs, "tiles": tiles, "seeds_with_hits": nnz},
     }
 
     # ---- e2e: reference-facing C ABI (host seeds in, host HSP lists out) ----
@@ -531,26 +631,34 @@ def run_ours(args):
         sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
         barrier()
         t0 = time.perf_counter()
-        outs = None
+        outs1 = None
         t_write = t_call = 0.0
         for _ in range(k_e2e):
             t1 = time.perf_counter()
             sf.send_query_write_request(w.query, 1)
             t2 = time.perf_counter()
-            outs = sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
+            outs1 = sf.seed_and_filter_batch([(1, r, a, b) for (_, r, a, b) in units])
             t_write, t_call = t_write + t2 - t1, t_call + time.perf_counter() - t2
         barrier()
         eb_s = allreduce((time.perf_counter() - t0) / k_e2e, "max")
         out["e2e_batched"] = {"value": e2e_hits / eb_s, "unit": UNIT, "h2d_bytes_per_step": len(w.query),
-                              "d2h_bytes_per_step": int(sum(len(o) for o in outs) * 16),
+                              "d2h_bytes_per_step": int(sum(len(o) for o in outs1) * 16),
                               "query_write_s": t_write / k_e2e, "batch_call_s": t_call / k_e2e}
+        sf.clear_query(1)
         # bit-exact: batched units == plain per-call results (concatenated per strand)
         bf = np.concatenate([o[1:] for o in outs[: len(plus)]]) if plus else np.zeros(0)
         br = np.concatenate([o[1:] for o in outs[len(plus):]]) if minus else np.zeros(0)
         out["bit_exact_batched_vs_plain"] = bool(
             len(bf) == len(fw) and len(br) == len(rc) and np.array_equal(bf.view(np.uint32), fw.view(np.uint32))
             and np.array_equal(br.view(np.uint32), rc.view(np.uint32)))
-        out["batched_vs_plain"] = out["value"] / out["e2e"]["value"]
+        # like for like: host buffers on both sides, and device time on both sides
+        dp_ms = plain_device_ms(sf, w, units) if world == 1 else None
+        out["batched_vs_plain"] = {
+            "e2e_batched_over_e2e": out["e2e_batched"]["value"] / out["e2e"]["value"],
+            "device_plain_ms": dp_ms, "device_batched_ms": tb["dev_ms"],
+            "device_plain_over_device_batched": (dp_ms / tb["dev_ms"]) if dp_ms else None,
+            "note": "e2e: host buffers on both sides; device: the units one call at a time (events, summed) "
+                    "against one batched pass"}
 
     # ---- batched form over uneven windows, distinct HSPs vs the chunked run ----
     if not args.no_e2e:
@@ -561,10 +669,17 @@ def run_ours(args):
     # ---- serving form (one GPU): Poisson request stream over the resident table ----
     if world == 1 and not args.no_serve:
         sf.set_timing(False)
-        n_req = args.serve_requests or (16 if args.workload == "large" else 48)
+        n_req = args.serve_requests or (args.large_serve_requests if args.workload == "large" else 200)
         table = ("600 Mbp target table (transitions on)" if args.workload == "large"
                  else "100 Mbp genome-scale target table")
         out["serving"] = run_serving(sf, w.target, n_req, table)
+
+    # ---- unranked: the reference's own kernels on a sample of the same units ----
+    if world == 1 and rank == 0 and not args.no_ref_gpu and args.workload == "genome":
+        try:
+            out["ref_gpu_baseline"] = ref_gpu_baseline(sf, w, calls, args.ref_gpu_units)
+        except Exception as e:  # the reference harness is a checker: report, do not fail the bench
+            out["ref_gpu_baseline"] = {"unavailable": f"{type(e).__name__}: {str(e)[:300]}"}
 
     # ---- CPU baseline on a bounded sample (rank 0, one GPU only) ----
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -574,32 +689,23 @@ def run_ours(args):
         out["cpu_baseline"] = {"value": cpu_v, "unit": UNIT, "cores": threads, "kind": "port",
                                "sample": f"first {args.cpu_chunks} 250 kbp units of the same workload "
                                          f"({r['hits']} extensions, {r['seconds']:.1f} s)"}
-        if not args.no_e2e:
-            # the sampled calls (seeder order), GPU batched units vs CPU port, bit-exact
-            samp = calls[: args.cpu_chunks]
-            gf = [outs[unit_of[c]][1:] for c in samp if c[1] == 0]
-            gr = [outs[unit_of[c]][1:] for c in samp if c[1] == 1]
-            gf = np.concatenate(gf) if gf else np.zeros(0, dtype=r["fw"].dtype)
-            gr = np.concatenate(gr) if gr else np.zeros(0, dtype=r["rc"].dtype)
-            out["bit_exact_vs_cpu_sample"] = bool(
-                len(gf) == len(r["fw"]) and len(gr) == len(r["rc"])
-                and np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32))
-                and np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))
+        # the sampled calls (seeder order), GPU batched units vs CPU port, bit-exact
+        samp = calls[: args.cpu_chunks]
+        gf = [outs[unit_of[c]][1:] for c in samp if c[1] == 0]
+        gr = [outs[unit_of[c]][1:] for c in samp if c[1] == 1]
+        gf = np.concatenate(gf) if gf else np.zeros(0, dtype=r["fw"].dtype)
+        gr = np.concatenate(gr) if gr else np.zeros(0, dtype=r["rc"].dtype)
+        out["bit_exact_vs_cpu_sample"] = bool(
+            len(gf) == len(r["fw"]) and len(gr) == len(r["rc"])
+            and np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32))
+            and np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))
 
-    # ---- repeat-masker self-alignment of the large target (last: it re-sends the target) ----
-    if args.workload == "large" and args.rm_intervals and world == 1:
-        sf.set_rm_exclude_diagonal(True)
-        try:
-            runs, rst = sf.rm_seeder_run(w.target, strand=3, num_threads=16, max_intervals=args.rm_intervals,
-                                         transition=transition)
-        finally:
-            sf.set_rm_exclude_diagonal(False)
-        out["rm_self_alignment"] = {
-            "workload": f"first {rst['num_intervals']} of the 10 Mbp intervals of the 600 Mbp target against "
-                        "their neighbour windows (proportion 0.2), both strands, transitions, diagonal excluded, M 1",
-            "seconds": rst["seconds"], "hits": rst["num_hits"], "hits_per_s": rst["num_hits"] / rst["seconds"],
-            "hsps": rst["num_hsps"], "calls": rst["num_calls"], "runs": int(len(runs)),
-            "covered_bases": int(runs["len"].sum()) if len(runs) else 0}
+    # ---- the 600 Mbp legs (one GPU): config 4 batched and plain, config 5 serving, repeat masker ----
+    if world == 1 and args.workload == "genome" and not args.no_large:
+        del w, outs
+        out["large"] = run_large(sf, args, flush, barrier)
+    elif args.workload == "large" and args.rm_intervals and world == 1:
+        out["rm_self_alignment"] = run_rm(sf, w.target, args.rm_intervals, transition)
 
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -607,6 +713,106 @@ def run_ours(args):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def run_rm(sf, target: bytes, n_intervals: int, transition: bool) -> dict:
+    """Repeat-masker self-alignment of the 600 Mbp target: the first n_intervals
+    10 Mbp intervals against their neighbour windows (it re-sends the target)."""
+    sf.set_rm_exclude_diagonal(True)
+    try:
+        runs, rst = sf.rm_seeder_run(target, strand=3, num_threads=16, max_intervals=n_intervals,
+                                     transition=transition)
+    finally:
+        sf.set_rm_exclude_diagonal(False)
+    return {"workload": f"first {rst['num_intervals']} of the 10 Mbp intervals of the 600 Mbp target against "
+                        "their neighbour windows (proportion 0.2), both strands, transitions, diagonal excluded, M 1",
+            "seconds": rst["seconds"], "hits": rst["num_hits"], "hits_per_s": rst["num_hits"] / rst["seconds"],
+            "hsps": rst["num_hsps"], "calls": rst["num_calls"], "runs": int(len(runs)),
+            "covered_bases": int(runs["len"].sum()) if len(runs) else 0}
+
+
+def run_large(sf, args, flush, barrier) -> dict:
+    """The 600 Mbp target (12 chr, GC 41%, 45% repeats) with transitions: the
+    batched form over a query sample (value as for the genome workload), the
+    plain C-ABI path on the same units, the serving form on that resident
+    table, and the repeat-masker self-alignment of the target."""
+    from segalign_b200 import build_sub_mat, synth
+
+    t0 = time.perf_counter()
+    w = synth.make(4, seed=104, scale=args.scale)
+    q = w.query[: args.query_sample]
+    gen_s = time.perf_counter() - t0
+    sf.initialize_processor(True, CHUNK, SEED_SIZE, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(w.target)
+    t = time.perf_counter()
+    sf.generate_seed_pos_table(None, 1, SEED_SIZE, 12)
+    barrier()
+    table_ms = 1000 * (time.perf_counter() - t)
+    sf.send_query_write_request(q, 0)
+    calls = seeder_calls(len(q))
+    units = [c for c in calls if c[1] == 0] + [c for c in calls if c[1] == 1]
+    sf.set_timing(True)
+    sf.refresh_query_keys(0)
+    sf.seed_and_filter_batch(units)  # warm-up
+    barrier()
+    tb = timed_batch_steps(sf, units, 2, flush, barrier)
+    st = tb["stats"]
+    wall = sum(tb["wall_s"]) / len(tb["wall_s"])
+    alg = 24.0 * st["seeds_with_hits"] + 4.0 * st["num_hits"] + 24.0 * st["tiles"] + 16.0 * st["survivors"]
+    peak, _ = peaks()
+    res = {"workload": f"600 Mbp target (12 chr) x the first {len(q) / 1e6:.0f} Mbp of a 600 Mbp query, GC 41%, "
+                       "45% repeats, 12of19 with one transition (13 seed words per position), both strands, "
+                       f"{len(units)} units of 250 kbp", "generate_s": gen_s, "table_build_ms": table_ms,
+           "value": st["num_hits"] / wall, "unit": UNIT, "ms_per_step": 1000 * wall,
+           "device_ms_per_step": tb["dev_ms"], "extensions_per_step": st["num_hits"], "hsps_per_step": st["num_hsps"],
+           "phase_ms": {"lookup": tb["lookup_ms"], "extend_lane": tb["lane_ms"], "extend_warp": tb["warp_ms"],
+                        "dedup": tb["dedup_ms"]},
+           "roofline": {"kernel": "sa_k_extend_lane", "achieved": alg / (tb["lane_ms"] / 1000) / 1e9, "peak": peak,
+                        "frac": alg / (tb["lane_ms"] / 1000) / 1e9 / peak, "unit": "GB/s",
+                        "traffic": lane_traffic(st["num_hits"], "large")[0]}}
+    outs = tb["outs"]
+    # plain path with host buffers on the same units (seeds with transitions on the host)
+    sf.set_timing(False)
+    fw, rc, sst = sf.seeder_run(q, buffer=0, strand=3, num_threads=16, interval_size=INTERVAL, chunk_size=CHUNK,
+                                interval_overlap=OVERLAP, transition=True)
+    barrier()
+    t0 = time.perf_counter()
+    fw, rc, sst = sf.seeder_run(q, buffer=0, strand=3, num_threads=16, interval_size=INTERVAL, chunk_size=CHUNK,
+                                interval_overlap=OVERLAP, transition=True)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    nplus = sum(1 for c in calls if c[1] == 0)
+    bf = np.concatenate([o[1:] for o in outs[:nplus]])
+    br = np.concatenate([o[1:] for o in outs[nplus:]])
+    res["e2e"] = {"value": sst["num_hits"] / e2e_s, "unit": UNIT, "seconds": e2e_s,
+                  "h2d_bytes_per_step": int(sst["num_seeds"] * 8), "d2h_bytes_per_step": int(
+                      (sst["num_hsps"] + sst["num_calls"]) * 16),
+                  "path": "sa_seed_and_filter per 250 kbp unit from 16 host threads (C++ seeder with transitions)"}
+    res["bit_exact_batched_vs_plain"] = bool(
+        len(bf) == len(fw) and len(br) == len(rc) and np.array_equal(bf.view(np.uint32), fw.view(np.uint32))
+        and np.array_equal(br.view(np.uint32), rc.view(np.uint32)))
+    # CPU port on a bounded sample of the same units, bit-exact against the batched units
+    if args.large_cpu_units:
+        pw = synth.Workload(w.target, q, w.target_chr, w.query_chr)
+        r = cpu_sample(pw, args.large_cpu_units, os.cpu_count() or 1, True)
+        samp = calls[:args.large_cpu_units]
+        unit_of = {c: i for i, c in enumerate(units)}
+        gf = [outs[unit_of[c]][1:] for c in samp if c[1] == 0]
+        gr = [outs[unit_of[c]][1:] for c in samp if c[1] == 1]
+        gf = np.concatenate(gf) if gf else np.zeros(0, dtype=r["fw"].dtype)
+        gr = np.concatenate(gr) if gr else np.zeros(0, dtype=r["rc"].dtype)
+        res["cpu_sample"] = {"value": r["hits"] / r["seconds"], "units": args.large_cpu_units, "extensions": r["hits"],
+                             "bit_exact": bool(len(gf) == len(r["fw"]) and len(gr) == len(r["rc"]) and
+                                               np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32)) and
+                                               np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))}
+        _TABLES.clear()
+    del outs
+    if not args.no_serve:
+        res["serving"] = run_serving(sf, w.target, args.large_serve_requests,
+                                     "600 Mbp target table (transitions on)")
+    if args.rm_intervals:
+        res["rm_self_alignment"] = run_rm(sf, w.target, args.rm_intervals, True)
+    return res
 
 
 def main():

@@ -171,6 +171,13 @@ typedef struct {
 int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment** out, uint64_t* out_len,
                              uint64_t* offsets);
 
+/* Device seeding of a resident query buffer (no reference counterpart; it
+ * replaces the host loop of src/seeder.cpp:57-74 for the batched form): the
+ * per-position 12-mer keys of both strands are computed on the GPU now.  The
+ * batched form otherwise computes them on first use after each query write
+ * and keeps them while the query stays. */
+int sa_refresh_query_keys(uint32_t buffer);
+
 /* ---- serving form (no reference counterpart) ----
  * A request loop over the resident target and seed table.  A request is one
  * query sequence; it is cut into units exactly as the seeder cuts a query

@@ -51,7 +51,7 @@ EXPORTS = [
     "sa_set_tuning_param", "sa_get_tuning_param",
     "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
     "sa_rm_seeder_run", "sa_free_rm_runs", "sa_format_segments", "sa_format_rm_intervals", "sa_free_text",
-    "sa_fasta_load", "sa_seq_set_free", "sa_align_fasta",
+    "sa_fasta_load", "sa_seq_set_free", "sa_align_fasta", "sa_refresh_query_keys",
 ]
 
 
@@ -218,6 +218,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                                      C.c_uint64, u64p]),
             "sa_kernel_launches": (C.c_uint64, []),
             "sa_fasta_load": (C.c_int, [C.c_char_p, C.c_uint32, _P(SeqSet)]),
+            "sa_refresh_query_keys": (C.c_int, [C.c_uint32]),
             "sa_seq_set_free": (None, [_P(SeqSet)]),
             "sa_align_fasta": (C.c_int, [_P(AlignCfg), _P(AlignStats)]),
             "sa_serve_start": (C.c_int, [_P(ServeCfg)]),
@@ -391,6 +392,10 @@ class SeedFilter:
     def shutdown_processor(self) -> None:
         self._chk(self.lib.sa_shutdown_processor(), "ShutdownProcessor")
 
+    def refresh_query_keys(self, buffer: int = 0) -> None:
+        """Recomputes the per-position keys of a resident query buffer on the GPU."""
+        self._chk(self.lib.sa_refresh_query_keys(buffer), "refresh_query_keys")
+
     def seed_and_filter_batch(self, units, keep_on_device: bool = False):
         """Batched form: units = [(buffer, rev, start, end), ...].
 
@@ -464,7 +469,7 @@ class SeedFilter:
 
     def get_tuning(self) -> dict:
         names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas", "substeps", "call_range_ctas",
-                 "call_lane_ctas", "switch_now", "rm_lane_ctas", "rm_substeps", "rm_switch_now")
+                 "call_lane_ctas", "switch_now", "rm_lane_ctas", "rm_substeps", "rm_switch_now", "refill", "rm_refill")
         return {n: int(self.lib.sa_get_tuning_param(n.encode())) for n in names}
 
     def set_timing(self, on: bool) -> None:

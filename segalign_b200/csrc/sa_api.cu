@@ -20,6 +20,7 @@
 
 #include "../../include/segalign_b200.h"
 #include "sa_launch.h"
+#include "sa_slot_pool.h"
 
 // ---------------------------------------------------------------------------
 // Errors
@@ -173,7 +174,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0, 1, 1};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -380,13 +381,23 @@ int make_slot(int dev_idx, uint64_t seed_cap, uint64_t surv_cap, uint64_t long_c
     return SA_OK;
 }
 
+// Takes a free slot (g.mu held): the first one of the device with the most
+// free slots (sa_slot_pool.h).
+Slot* take_free_slot_locked() {
+    Global& g = G();
+    std::vector<int> dev(g.free_slots.size());
+    for (size_t i = 0; i < dev.size(); ++i) dev[i] = g.free_slots[i]->dev_idx;
+    const size_t k = sa_pick_free_slot(dev, (int)g.devs.size());
+    Slot* s = g.free_slots[k];
+    g.free_slots.erase(g.free_slots.begin() + (std::ptrdiff_t)k);
+    return s;
+}
+
 Slot* acquire_slot() {
     Global& g = G();
     std::unique_lock<std::mutex> lk(g.mu);
     g.cv.wait(lk, [&] { return !g.free_slots.empty(); });
-    Slot* s = g.free_slots.front();
-    g.free_slots.pop_front();
-    return s;
+    return take_free_slot_locked();
 }
 
 void release_slot(Slot* s) {
@@ -424,6 +435,7 @@ SaCallGrids sa_call_grids(const SaTuning& t, int num_sms, int mode) {
     if (mode == 1) {  // repeat-masker call
         c.lane_tuning.substeps = t.rm_substeps;
         c.lane_tuning.switch_now = t.rm_switch_now;
+        c.lane_tuning.refill = t.rm_refill;
         c.lane_ctas = t.rm_lane_ctas > 0 ? t.rm_lane_ctas : num_sms * t.ext_ctas_per_sm;
     }
     return c;
@@ -1016,8 +1028,7 @@ int seed_and_filter_coalesced(const uint64_t* seeds, uint32_t num_seeds, int rev
         while (true) {
             g.cv.wait(lk, [&] { return c.done || (!c.taken && !g.free_slots.empty()); });
             if (c.done) break;
-            Slot* s = g.free_slots.front();
-            g.free_slots.pop_front();
+            Slot* s = take_free_slot_locked();
             std::vector<CallReq*> pass;
             uint64_t words = 0;
             while (!g.pending.empty() && pass.size() < std::min<uint32_t>(g.coalesce_calls, s->max_units)) {
@@ -1596,6 +1607,19 @@ int sa_shutdown_processor(void) {
 }
 
 
+int sa_refresh_query_keys(uint32_t buffer) {
+    SA_TRY(check_ready(true));
+    Global& g = G();
+    if (buffer >= (uint32_t)kMaxBuffers) return SA_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g.batch_mu);
+    for (auto& d : g.devs)
+        for (int rev = 0; rev < 2; ++rev) {
+            d.qkeys_ok[buffer][rev] = false;
+            SA_TRY(ensure_keys(d, buffer, rev));
+        }
+    return SA_OK;
+}
+
 // Batched SeedAndFilter (no single reference counterpart; each unit reproduces
 // one src/seed_filter.cu:654-778 call on the seeds of src/seeder.cpp:57-74).
 int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment** out, uint64_t* out_len,
@@ -1756,12 +1780,13 @@ int sa_set_tuning_param(const char* name, int value) {
         (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
         return SA_OK;
     }
-    if (n == "switch_now" || n == "rm_switch_now") {
+    if (n == "switch_now" || n == "rm_switch_now" || n == "refill" || n == "rm_refill") {
         if (value != 0 && value != 1) {
             sa_set_error(SA_ERR_ARG, "%s must be 0 or 1 (got %d)", name, value);
             return SA_ERR_ARG;
         }
-        (n == "switch_now" ? t.switch_now : t.rm_switch_now) = value;
+        (n == "switch_now" ? t.switch_now : n == "rm_switch_now" ? t.rm_switch_now : n == "refill" ? t.refill
+                                                                                                   : t.rm_refill) = value;
         return SA_OK;
     }
     if (n == "rm_substeps") {
@@ -1816,6 +1841,8 @@ int sa_get_tuning_param(const char* name) {
     if (n == "call_lane_ctas") return t.call_lane_ctas;
     if (n == "switch_now") return t.switch_now;
     if (n == "rm_switch_now") return t.rm_switch_now;
+    if (n == "refill") return t.refill;
+    if (n == "rm_refill") return t.rm_refill;
     if (n == "rm_substeps") return t.rm_substeps;
     if (n == "rm_lane_ctas") return t.rm_lane_ctas;
     return SA_ERR_ARG;

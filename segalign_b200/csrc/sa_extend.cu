@@ -48,6 +48,7 @@ struct SaExtK {
     uint32_t tile_hits;
     uint32_t substeps;  // steps per lane-kernel iteration (at most)
     uint32_t switch_now;  // 1: a lane starts its left side in the step after its right side ends
+    uint32_t refill;      // 1: a lane whose hit ends takes the tile's next hit within the iteration
 };
 
 // Reverse the order of the 8 nibbles of a word.
@@ -332,6 +333,78 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         bpos = 0;
     };
 
+    // Idle lanes take the next records of the warp tile, in order; true for a
+    // lane that got one.  Warp-collective.
+    auto take_records = [&](uint32_t idle) -> bool {
+        bool fresh = false;
+        if (tile_pos < tile_n) {
+            const uint32_t m = min((uint32_t)__popc(idle), tile_n - tile_pos);
+            const uint32_t rank = __popc(idle & lt);
+            if (!has && rank < m) {
+                const uint4 r = s_hits[tile_pos + rank];
+                rl = r.x;
+                ql = r.y;
+                scope = r.z;
+                unit_id = r.w;
+                fresh = true;
+            }
+            tile_pos += m;
+        }
+        return fresh;
+    };
+    // Start of a direction: a fresh hit (right), or the left side of the
+    // current hit after its right end.  Per lane.
+    auto start_lane = [&](bool fresh) {
+        const SaUnit U = a.units[unit_id];
+        if (fresh) {
+            // rm: hits outside [ref_start, ref_end] are never extended
+            // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
+            bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+            // Coordinates past either sequence end (a caller-supplied table or
+            // seed beyond the sequences) are rejected, not read.
+            if (rl > a.ref_len || ql > U.q_len) {
+                atomicCAS(&a.ctr->error, 0ull, 5ull);
+                skip = true;
+            }
+            if (!skip) {
+                has = true;
+                nocap = false;
+                setup = true;
+                dir = 0;
+                tiles = 0;
+                ++ext_acc;
+            }
+        }
+        if (setup) {
+            setup = false;
+            begin_dir(U.q_packed, U.q_len);
+        }
+    };
+    // Candidates of the lanes that finished a hit (total >= hspthresh; the
+    // entropy factor is at most 1, so lower totals are never kept) go into the
+    // warp's ring; every 32 of them are tested and inserted.  Warp-collective.
+    bool finished = false;
+    int Lpos = 0, total = 0;
+    auto emit_finished = [&]() {
+        const bool emit = finished && (int)(float)total >= a.hspthresh;
+        const uint32_t em = __ballot_sync(SA_FULL, emit);
+        if (em) {
+            if (emit) {
+                const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
+                // {ref_start, query_start (before the rm flip), len, scope}, {total, unit} (:606-608)
+                s_em[slot] = make_uint4(rl - (uint32_t)Lpos, ql - (uint32_t)Lpos, (uint32_t)(Rpos + Lpos), scope);
+                s_ex[slot] = make_uint2((uint32_t)total, unit_id);
+            }
+            em_tail += __popc(em);
+            while (em_tail - em_head >= 32) {
+                __syncwarp();
+                sa_flush_candidates(a, s_em, s_ex, em_head, 32);
+                em_head += 32;
+            }
+        }
+        finished = false;
+    };
+
     while (true) {
         // ---- idle lanes take the next hits of the warp tile, in order ----
         const uint32_t idle = __ballot_sync(SA_FULL, !has);
@@ -376,56 +449,14 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     tile_pos = 0;
                 }
             }
-            if (tile_pos < tile_n) {
-                const uint32_t m = min((uint32_t)__popc(idle), tile_n - tile_pos);
-                const uint32_t rank = __popc(idle & lt);
-                if (!has && rank < m) {
-                    const uint4 r = s_hits[tile_pos + rank];
-                    rl = r.x;
-                    ql = r.y;
-                    scope = r.z;
-                    unit_id = r.w;
-                    fresh = true;
-                }
-                tile_pos += m;
-            }
+            fresh = take_records(idle);
         }
-
-        // ---- start of a direction: a fresh hit (right), or the left side of
-        // the current hit after its right end ----
-        if (fresh || setup) {
-            const SaUnit U = a.units[unit_id];
-            if (fresh) {
-                // rm: hits outside [ref_start, ref_end] are never extended
-                // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
-                bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
-                // Coordinates past either sequence end (a caller-supplied table or
-                // seed beyond the sequences) are rejected, not read.
-                if (rl > a.ref_len || ql > U.q_len) {
-                    atomicCAS(&a.ctr->error, 0ull, 5ull);
-                    skip = true;
-                }
-                if (!skip) {
-                    has = true;
-                    nocap = false;
-                    setup = true;
-                    dir = 0;
-                    tiles = 0;
-                    ++ext_acc;
-                }
-            }
-            if (setup) {
-                setup = false;
-                begin_dir(U.q_packed, U.q_len);
-            }
-        }
-        const bool done = !__any_sync(SA_FULL, has) && exhausted && tile_pos >= tile_n;
+        if (fresh || setup) start_lane(fresh);
 
         // ---- up to `substeps` STEP-base steps per busy lane: the lanes still
         // scanning go on while any lane of the warp does; a lane stops for
-        // this iteration when its direction ends or it goes to the long queue ----
-        bool finished = false, to_long = false;
-        int Lpos = 0, total = 0;
+        // this iteration when it goes to the long queue ----
+        bool to_long = false;
         bool scanning = has;
 #pragma unroll 1
         for (uint32_t sub = 0; sub < a.substeps; ++sub) {
@@ -502,6 +533,10 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                         setup = true;
                     } else {
                         finished = true;
+                        Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
+                        total = Rbest + best;
+                        tiles_acc += tiles;
+                        has = false;
                     }
                     scanning = false;
                 } else {
@@ -511,25 +546,28 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                         scanning = false;
                     }
                 }
-                if (finished) {
-                    Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
-                    total = Rbest + best;
-                    tiles_acc += tiles;
-                    has = false;
-                }
             }
-            // switch_now: a lane whose right side ended in this step starts
-            // its left side at once and scans in the iteration's remaining
-            // steps instead of idling until the next iteration
-            if (a.switch_now && sub + 1 < a.substeps && __any_sync(SA_FULL, setup)) {
-                if (setup) {
-                    setup = false;
-                    const SaUnit U = a.units[unit_id];
-                    begin_dir(U.q_packed, U.q_len);
-                    scanning = true;
+            if (sub + 1 < a.substeps) {
+                // refill: a lane whose hit ended in this step emits it and takes
+                // the tile's next hit, to scan in the iteration's remaining
+                // steps; switch_now: a lane whose right side ended starts its
+                // left side at once
+                bool again = false;
+                if (a.refill) {
+                    emit_finished();
+                    const uint32_t idle2 = __ballot_sync(SA_FULL, !has);
+                    if (idle2 && tile_pos < tile_n) again = take_records(idle2);
+                }
+                const bool go = again || (a.switch_now && setup);
+                if (__any_sync(SA_FULL, go)) {
+                    if (go) {
+                        start_lane(again);
+                        scanning = has && !to_long;
+                    }
                 }
             }
         }
+        emit_finished();
 
         // ---- long queue pushes (warp-aggregated) ----
         {
@@ -556,27 +594,17 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
         }
-        // ---- candidate HSPs (total >= hspthresh; the entropy factor is at
-        // most 1, so lower totals are never kept) into the warp's ring ----
-        {
-            const bool emit = finished && (int)(float)total >= a.hspthresh;
-            const uint32_t em = __ballot_sync(SA_FULL, emit);
-            if (emit) {
-                const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
-                // {ref_start, query_start (before the rm flip), len, scope}, {total, unit} (:606-608)
-                s_em[slot] = make_uint4(rl - (uint32_t)Lpos, ql - (uint32_t)Lpos, (uint32_t)(Rpos + Lpos), scope);
-                s_ex[slot] = make_uint2((uint32_t)total, unit_id);
-            }
-            em_tail += __popc(em);
-            // full batches of 32; at the end, whatever is left
-            while (em_tail - em_head >= 32 || (done && em_tail != em_head)) {
+        const bool done = !__any_sync(SA_FULL, has || setup) && exhausted && tile_pos >= tile_n;
+        if (done) {
+            // whatever candidates are left
+            while (em_tail != em_head) {
                 const uint32_t n = min(em_tail - em_head, 32u);
                 __syncwarp();
                 sa_flush_candidates(a, s_em, s_ex, em_head, n);
                 em_head += n;
             }
+            break;
         }
-        if (done) break;
     }
     // flush statistics
     unsigned long long t = tiles_acc, e = ext_acc;
@@ -801,6 +829,7 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.tile_hits = (uint32_t)t.tile_hits;
     a.substeps = (uint32_t)t.substeps;
     a.switch_now = t.switch_now ? 1u : 0u;
+    a.refill = t.refill ? 1u : 0u;
     return a;
 }
 

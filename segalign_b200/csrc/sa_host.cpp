@@ -496,34 +496,6 @@ struct RmInterval {
     uint32_t block, start, end, ref_start, ref_end;
 };
 
-// Runs of coverage >= M over [0, block_len) for one interval's HSPs, with the
-// per-position uint8 counts of repeat_masker_src/seeder.cpp:151-186 (counts
-// wrap at 256) taken from a sweep over the sorted ends of the HSPs' query
-// ranges instead of a block-length array.  A run still open at block_len is
-// not reported, as the reference loop only closes runs in its else branch.
-void coverage_runs(std::vector<std::pair<uint32_t, int>>& ev, uint32_t block_len, uint32_t M, uint32_t block,
-                   uint32_t interval, std::vector<sa_rm_run>& out) {
-    std::sort(ev.begin(), ev.end());
-    int64_t count = 0;
-    bool run = false;
-    uint32_t run_start = 0;
-    size_t k = 0;
-    uint32_t pos = 0;
-    while (pos < block_len) {
-        while (k < ev.size() && ev[k].first <= pos) count += ev[k++].second;
-        const uint32_t next = k < ev.size() ? std::min(ev[k].first, block_len) : block_len;
-        const bool in = (uint32_t)(count & 255) >= M;
-        if (in && !run) {
-            run = true;
-            run_start = pos;
-        } else if (!in && run) {
-            run = false;
-            out.push_back({block, interval, run_start, pos - run_start});
-        }
-        pos = next;
-    }
-}
-
 }  // namespace
 
 extern "C" {
@@ -609,7 +581,7 @@ int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_
         auto worker = [&]() {
             const uint64_t per = 1 + (g_shape.transition ? (uint64_t)g_shape.kmer_size : 0);
             std::vector<uint64_t> seeds;
-            std::vector<std::pair<uint32_t, int>> ev;
+            std::vector<std::pair<uint32_t, uint32_t>> ev, cov;  // HSP (query_start, len); runs (start, len)
             while (!err) {
                 const size_t k = next.fetch_add(1);
                 if (k >= last) break;
@@ -629,10 +601,7 @@ int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_
                     nhits += (uint32_t)o[0].score;
                     nhsps += ol - 1;
                     ++ncalls;
-                    for (uint64_t h = 1; h < ol; ++h) {
-                        ev.emplace_back(o[h].query_start, 1);
-                        ev.emplace_back(o[h].query_start + o[h].len, -1);
-                    }
+                    for (uint64_t h = 1; h < ol; ++h) ev.emplace_back(o[h].query_start, o[h].len);
                     sa_free_segments(o);
                     return SA_OK;
                 };
@@ -646,7 +615,12 @@ int sa_rm_seeder_run(const sa_rm_seeder_cfg* cfg, const char* seq, uint64_t seq_
                     }
                     if (rr != SA_OK) err = rr;
                 }
-                if (!err) coverage_runs(ev, bl, M, blk, (uint32_t)k, out[k]);
+                if (!err) {
+                    // uint8 coverage counts and runs >= M on the GPU (repeat_masker_src/seeder.cpp:151-186)
+                    const int rr = sa_device_coverage_runs(ev, bl, M, cov);
+                    if (rr != SA_OK) err = rr;
+                    for (const auto& r : cov) out[k].push_back({blk, (uint32_t)k, r.first, r.second});
+                }
             }
         };
         std::vector<std::thread> th;

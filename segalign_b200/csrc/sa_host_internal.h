@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <vector>
 
 #include "../../include/segalign_b200.h"
@@ -37,6 +38,13 @@ int sa_host_run_calls(const std::vector<SaHostCall>& calls, const char* query, c
 // Seed size and K of the host shape (sa_host_set_shape).
 int sa_host_seed_size();
 int sa_host_kmer_size();
+
+// Repeat-masker coverage runs of one interval on the GPU (sa_coverage.cu,
+// repeat_masker_src/seeder.cpp:151-186): hsps = (query_start, len) pairs,
+// block-relative; runs = (start, len) of the stretches with uint8 coverage
+// >= M, in position order, without a run still open at block_len.
+int sa_device_coverage_runs(const std::vector<std::pair<uint32_t, uint32_t>>& hsps, uint32_t block_len, uint32_t M,
+                            std::vector<std::pair<uint32_t, uint32_t>>& runs);
 
 // Error state of the API layer (sa_last_error), defined in sa_api.cu.
 void sa_set_error(int code, const char* fmt, ...);

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from segalign_b200 import SeedFilter, host_seeds, host_revcomp, build_sub_mat
+from segalign_b200 import SeedFilter, build_sub_mat, host_revcomp, host_seeds, synth
 from tests.helpers import compare_segments, small_workload, random_text
 
 pytestmark = pytest.mark.gpu
@@ -280,3 +280,33 @@ def test_hsp_set_reused_after_overflow(setup):
             else:
                 os.environ[k] = v
         sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
+
+
+def test_transitions_repeat_rich_sample(built):
+    """The 600 Mbp workload's generator at 1% (6 Mbp target, GC 41%, 45%
+    repeats, Alu-like families) with transitions on: eight 100 kbp units, both
+    strands, GPU per call == oracle, header included."""
+    w = synth.make(4, seed=104, scale=0.01)
+    T, Q = w.target, w.query
+    p = oracle.params(transition=True)
+    idx, pos = oracle.build_table(T, p)
+    sf = SeedFilter()
+    sf.initialize_interface(1)
+    sf.generate_shape_pos("12of19")
+    sf.initialize_processor(True, 100_000, 19, build_sub_mat(910), 910, 3000, False)
+    sf.send_ref_write_request(T)
+    sf.generate_seed_pos_table(None, 1, 19, 12)
+    sf.send_query_write_request(Q, 0)
+    R, QF, QRC = oracle.encode(T), oracle.encode(Q), oracle.encode_rc(Q)
+    QR = host_revcomp(Q)
+    hits = hsps = 0
+    for rev, text in ((0, Q), (1, QR)):
+        for j0 in (0, 1_500_000, 3_000_000, 5_800_000):
+            j1 = min(j0 + 100_000, len(Q) - 19)
+            seeds = host_seeds(text, j0, j1, transition=True)
+            got = sf.seed_and_filter(seeds, bool(rev), 0)
+            want, st = oracle.seed_and_filter(p, R, QRC if rev else QF, idx, pos, seeds, bool(rev))
+            compare_segments(got, want, f"repeat-rich transition unit rev={rev} [{j0},{j1})")
+            hits += st["num_hits"]
+            hsps += len(want) - 1
+    assert hits > 5_000_000 and hsps > 50_000
