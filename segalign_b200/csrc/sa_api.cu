@@ -174,7 +174,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0, 1, 1};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0, 0, 0, 0};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -1780,6 +1780,14 @@ int sa_set_tuning_param(const char* name, int value) {
         (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
         return SA_OK;
     }
+    if (n == "wide_loads") {
+        if (value != 0 && value != 1) {
+            sa_set_error(SA_ERR_ARG, "wide_loads must be 0 or 1 (got %d)", value);
+            return SA_ERR_ARG;
+        }
+        t.wide_loads = value;
+        return SA_OK;
+    }
     if (n == "switch_now" || n == "rm_switch_now" || n == "refill" || n == "rm_refill") {
         if (value != 0 && value != 1) {
             sa_set_error(SA_ERR_ARG, "%s must be 0 or 1 (got %d)", name, value);
@@ -1843,6 +1851,7 @@ int sa_get_tuning_param(const char* name) {
     if (n == "rm_switch_now") return t.rm_switch_now;
     if (n == "refill") return t.refill;
     if (n == "rm_refill") return t.rm_refill;
+    if (n == "wide_loads") return t.wide_loads;
     if (n == "rm_substeps") return t.rm_substeps;
     if (n == "rm_lane_ctas") return t.rm_lane_ctas;
     return SA_ERR_ARG;

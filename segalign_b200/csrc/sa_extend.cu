@@ -164,7 +164,7 @@ __device__ __forceinline__ int sa_tbl(const char* tblb, uint32_t lo, uint32_t hi
 template <bool EDGE, int SH>
 __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, uint32_t hi, uint32_t off0,
                                                uint32_t avail, int neg, int xdrop, int& P, int& B, int& at,
-                                               bool& stop) {
+                                               bool& stop, int j, int& js) {
     int mn = INT_MAX;
     // Bases in pairs: the running best and minimum take both prefixes of a
     // pair with one 3-input max / min (DPX on sm_90 and later).
@@ -179,7 +179,10 @@ __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, ui
         B = __vimax3_s32(B, P0, P);
         mn = __vimin3_s32(mn, P0, P);
     }
-    if (!stop) at = B;
+    if (!stop) {
+        at = B;
+        js = j;
+    }
     stop = stop || ((B >> SH) - (mn >> SH) > xdrop);
 }
 
@@ -252,10 +255,18 @@ static size_t sa_lane_smem(uint32_t tile) {
     return SA_LANE_TABLES + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 8;
 }
 
-template <int MIN_CTAS, int STEP, bool EXACT>
+template <int MIN_CTAS, int STEP, bool EXACT, bool WIDE>
 __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
     constexpr int NW = STEP / 8;                  // 8-base windows per step
+    // WIDE: the target is read in aligned 16-byte chunks (one 128-bit load per
+    // 32-base step).  A direction's scan then starts at the chunk holding its
+    // first base: the `lead` bases before that base (0, 8, 16 or 24, whole
+    // 8-base windows) are skipped in the first step, and offsets, the best
+    // position and the stop tile are taken back by `lead`.  The query keeps
+    // word loads, shifted back by the same `lead` (into its padding at most).
+    static_assert(!WIDE || (STEP == 32 && !EXACT), "wide target loads: fast form, 32-base steps");
+    constexpr int NWR = WIDE ? 2 * NW : NW + 1;   // target words held
     constexpr int SCALE = 2 * STEP;               // packed score scale (fast form)
     constexpr int SH = STEP == 8 ? 4 : STEP == 16 ? 5 : 6;  // log2(SCALE)
     static_assert(STEP == 8 || STEP == 16 || STEP == 32, "8-, 16- or 32-base steps");
@@ -299,10 +310,12 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     int dir = 0;
     // scan of the current direction: offset, bases available, word shifts,
     // words w[0..NW] of the coming step, next word addresses
-    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0;
-    uint32_t w_r[NW + 1], w_q[NW + 1];
+    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0, lead = 0;
+    uint32_t w_r[NWR], w_q[NW + 1];
 #pragma unroll
-    for (int j = 0; j <= NW; ++j) w_r[j] = w_q[j] = 0;
+    for (int j = 0; j < NWR; ++j) w_r[j] = 0;
+#pragma unroll
+    for (int j = 0; j <= NW; ++j) w_q[j] = 0;
     const uint32_t* __restrict__ pr = ref;
     const uint32_t* __restrict__ pq = ref;
     // running score, best, offset of the first base reaching best
@@ -318,14 +331,29 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         avail = min(ref_len - sr, qlen - sq);
         sh_r = (sr & 7u) * 4u;
         sh_q = (sq & 7u) * 4u;
-        pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
-        pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
+        if (WIDE) {
+            const uint32_t dw = (sr >> 3) & 3u;  // words between the chunk start and the first base's word
+            lead = 8u * dw;
+            avail += lead;
+            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + ((sr >> 3) - dw);
+            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (int64_t)(sq >> 3) - (int64_t)dw;
+            const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(pr));
+            const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(pr) + 1);
+            w_r[0] = c0.x, w_r[1] = c0.y, w_r[2] = c0.z, w_r[3] = c0.w;
+            w_r[NWR - 4] = c1.x, w_r[NWR - 3] = c1.y, w_r[NWR - 2] = c1.z, w_r[NWR - 1] = c1.w;
+            pr += 8;
 #pragma unroll
-        for (int j = 0; j <= NW; ++j) {
-            w_r[j] = __ldg(pr + j);
-            w_q[j] = __ldg(pq + j);
+            for (int j = 0; j <= NW; ++j) w_q[j] = __ldg(pq + j);
+        } else {
+            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
+            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
+#pragma unroll
+            for (int j = 0; j <= NW; ++j) {
+                w_r[j] = __ldg(pr + j);
+                w_q[j] = __ldg(pq + j);
+            }
+            pr += NW + 1;
         }
-        pr += NW + 1;
         pq += NW + 1;
         o = 0;
         S = 0;
@@ -468,18 +496,25 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     rwin[j] = __funnelshift_r(w_r[j], w_r[j + 1], sh_r);
                     qwin[j] = __funnelshift_r(w_q[j], w_q[j + 1], sh_q);
                 }
-                w_r[0] = w_r[NW];
+                if (WIDE) {
+                    // the next chunk moves down; the one after it is loaded
+                    w_r[0] = w_r[4], w_r[1] = w_r[5], w_r[2] = w_r[6], w_r[3] = w_r[7];
+                    const uint4 c = __ldg(reinterpret_cast<const uint4*>(pr));
+                    w_r[4] = c.x, w_r[5] = c.y, w_r[6] = c.z, w_r[7] = c.w;
+                    pr += 4;
+                } else {
+                    w_r[0] = w_r[NW];
+    #pragma unroll
+                    for (int j = 1; j <= NW; ++j) w_r[j] = __ldg(pr + j - 1);
+                    pr += NW;
+                }
                 w_q[0] = w_q[NW];
     #pragma unroll
-                for (int j = 1; j <= NW; ++j) {
-                    w_r[j] = __ldg(pr + j - 1);
-                    w_q[j] = __ldg(pq + j - 1);
-                }
-                pr += NW;
+                for (int j = 1; j <= NW; ++j) w_q[j] = __ldg(pq + j - 1);
                 pq += NW;
                 const bool edge = o + STEP > avail;
                 bool stop = false;
-                uint32_t lo, hi;
+                uint32_t lo, hi, stop_off = 0;
                 if (EXACT) {
                     bool alive = true;
                     int pk = 0;
@@ -500,22 +535,28 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     if (best != best_in) bpos = (int)o + pk;
                     stop = !alive;
                 } else {
-                    int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
+                    // windows before the direction's first base (WIDE, first step only)
+                    const int skip = (WIDE && o == 0) ? (int)(lead >> 3) : 0;
+                    int Pk = ((S - best) << SH) + STEP - 8 * skip, B = SCALE - 1, at = 0, js = 0;
                     if (!edge) {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
+                            if (WIDE && j < skip) continue;
                             sa_merge8(rwin[j], qwin[j], lo, hi);
-                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
+                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop, j,
+                                                      js);
                         }
                     } else {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
+                            if (WIDE && j < skip) continue;
                             sa_merge8(rwin[j], qwin[j], lo, hi);
                             // a base past the sequence end scores -(xdrop + 1)
                             sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
-                                                     a.xdrop, Pk, B, at, stop);
+                                                     a.xdrop, Pk, B, at, stop, j, js);
                         }
                     }
+                    if (WIDE && stop) stop_off = o + 8u * (uint32_t)js;
                     const int low = at & (SCALE - 1);
                     if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
                     const int best_in = best;
@@ -524,16 +565,18 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
                 if (stop) {
                     // Steps start at multiples of STEP (8, 16 or 32), so the stop offset
-                    // lies in 32-base tile o >> 5 whichever base of the step it is.
-                    tiles += (o >> 5) + 1;
+                    // lies in 32-base tile o >> 5 whichever base of the step it is
+                    // (WIDE: the stopping 8-base window, taken back by lead, lies in
+                    // one tile).
+                    tiles += ((WIDE ? stop_off - lead : o) >> 5) + 1;
                     if (dir == 0) {
                         Rbest = best;
-                        Rpos = best > 0 ? bpos : -1;  // -1 when no positive score
+                        Rpos = best > 0 ? bpos - (int)lead : -1;  // -1 when no positive score
                         dir = 1;
                         setup = true;
                     } else {
                         finished = true;
-                        Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
+                        Lpos = best > 0 ? bpos - (int)lead + 1 : 0;  // left offsets are 1-based
                         total = Rbest + best;
                         tiles_acc += tiles;
                         has = false;
@@ -848,24 +891,26 @@ static bool sa_lane_fast_form(const SaParams& p, int step) {
     return x >= 0 && 7 * mx <= x && x * scale - low * step < (1ll << 31) && mx * scale * step < (1ll << 31);
 }
 
-template <int C, int STEP, bool EXACT>
+template <int C, int STEP, bool EXACT, bool WIDE>
 static void sa_lane_launch(const SaExtK& a, const SaParams& p, int grid, size_t smem, cudaStream_t st) {
-    if (grid > 0) sa_k_extend_lane<C, STEP, EXACT><<<grid, 256, smem, st>>>(a, p);
-    else cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (grid > 0) sa_k_extend_lane<C, STEP, EXACT, WIDE><<<grid, 256, smem, st>>>(a, p);
+    else cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem);
 }
 
 template <int C>
-static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, int grid, size_t smem,
-                             cudaStream_t st) {
+static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, bool wide, int grid,
+                             size_t smem, cudaStream_t st) {
     if (step == 32) {
-        if (exact) sa_lane_launch<C, 32, true>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 32, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 32, true, false>(a, p, grid, smem, st);
+        else if (wide) sa_lane_launch<C, 32, false, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 32, false, false>(a, p, grid, smem, st);
     } else if (step == 16) {
-        if (exact) sa_lane_launch<C, 16, true>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 16, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 16, true, false>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 16, false, false>(a, p, grid, smem, st);
     } else {
-        if (exact) sa_lane_launch<C, 8, true>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 8, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 8, true, false>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 8, false, false>(a, p, grid, smem, st);
     }
 }
 
@@ -882,11 +927,12 @@ void sa_prepare_extend_lane(const SaParams& p, const SaTuning& t) {
     const size_t smem = sa_lane_smem(1024);
     SaExtK none{};
     for (int step : {8, 16, 32})
-        for (bool exact : {false, true}) {
-            sa_lane_dispatch<2>(none, p, step, exact, 0, smem, 0);
-            sa_lane_dispatch<3>(none, p, step, exact, 0, smem, 0);
-            sa_lane_dispatch<4>(none, p, step, exact, 0, smem, 0);
-        }
+        for (bool exact : {false, true})
+            for (bool wide : {false, true}) {
+                sa_lane_dispatch<2>(none, p, step, exact, wide, 0, smem, 0);
+                sa_lane_dispatch<3>(none, p, step, exact, wide, 0, smem, 0);
+                sa_lane_dispatch<4>(none, p, step, exact, wide, 0, smem, 0);
+            }
     done[dev] = true;
 }
 
@@ -898,9 +944,10 @@ void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, 
     const int grid = grid_ctas > 0 ? grid_ctas : num_sms * t.ext_ctas_per_sm;
     const size_t smem = sa_lane_smem(a.tile_hits);
     const bool exact = !sa_lane_fast_form(p, t.step_bases);
-    if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, grid, smem, st);
-    else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, grid, smem, st);
-    else sa_lane_dispatch<2>(a, p, t.step_bases, exact, grid, smem, st);
+    const bool wide = t.wide_loads != 0;
+    if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, wide, grid, smem, st);
+    else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, wide, grid, smem, st);
+    else sa_lane_dispatch<2>(a, p, t.step_bases, exact, wide, grid, smem, st);
     sa_note_launch();
 }
 
