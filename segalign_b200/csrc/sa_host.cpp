@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -241,6 +242,8 @@ int sa_host_run_calls(const std::vector<SaHostCall>& calls, const char* query, c
     std::atomic<uint64_t> next{0}, nseeds{0}, nhits{0}, nhsps{0};
     std::atomic<uint64_t> ns_seed{0}, ns_call{0};
     std::atomic<int> err{0};
+    std::mutex err_mu;
+    std::string err_msg;  // the first failing worker's sa_last_error() text
     using SClock = std::chrono::steady_clock;
     auto ns_since = [](SClock::time_point t) {
         return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(SClock::now() - t).count();
@@ -264,7 +267,11 @@ int sa_host_run_calls(const std::vector<SaHostCall>& calls, const char* query, c
             int r = sa_seed_and_filter(seeds.data(), (uint32_t)need, cl.strand, buffer, &out, &ol);
             ns_call += ns_since(t_call);
             if (r != SA_OK) {
-                err = r;
+                std::lock_guard<std::mutex> lk(err_mu);
+                if (!err) {
+                    err_msg = sa_last_error();
+                    err = r;
+                }
                 break;
             }
             sa_call_stats cs;
@@ -282,6 +289,7 @@ int sa_host_run_calls(const std::vector<SaHostCall>& calls, const char* query, c
     if (err) {
         for (auto& r : res) sa_free_segments(r.p);
         res.clear();
+        sa_set_error(err, "%s", err_msg.c_str());  // the worker's message, in the calling thread
         return err;
     }
     if (st) {

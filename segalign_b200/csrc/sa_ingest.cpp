@@ -272,6 +272,8 @@ int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
         std::mutex mu;
         std::condition_variable cv;
         std::vector<int> loaded(nq, 0);  // 1 loaded, -1 failed
+        int load_err = SA_OK;
+        std::string load_msg;             // the loader's sa_last_error() text
         int done_upto = -1;               // blocks [0, done_upto] finished seeding
         bool abort = false;
         std::string rc_text[2];
@@ -297,6 +299,10 @@ int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
                     write_s += dt;
                     if (busy) overlap_s += dt;
                     loaded[k] = w == SA_OK ? 1 : -1;
+                    if (w != SA_OK) {
+                        load_err = w;
+                        load_msg = sa_last_error();
+                    }
                 }
                 cv.notify_all();
                 if (w != SA_OK) return;
@@ -307,7 +313,8 @@ int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
                 std::unique_lock<std::mutex> lk(mu);
                 cv.wait(lk, [&] { return loaded[k] != 0; });
                 if (loaded[k] < 0) {
-                    r = SA_ERR_STATE;
+                    r = load_err;
+                    sa_set_error(r, "query block %u: %s", k, load_msg.c_str());
                     break;
                 }
             }

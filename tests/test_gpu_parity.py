@@ -22,14 +22,20 @@ def setup(built):
     p = oracle.params()
     idx, pos = oracle.build_table(w.target, p)
     sf = SeedFilter()
-    sf.initialize_interface(1)
-    sf.generate_shape_pos("12of19")
-    sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
-    sf.send_ref_write_request(w.target)
-    sf.generate_seed_pos_table(None, 1, 19, 12)
-    sf.send_query_write_request(w.query, 0)
+
+    def restore():
+        """(Re)loads this module's workload: other tests load their own
+        targets into the same process-wide library state."""
+        sf.initialize_interface(1)
+        sf.generate_shape_pos("12of19")
+        sf.initialize_processor(False, CHUNK, 19, build_sub_mat(910), 910, 3000, False)
+        sf.send_ref_write_request(w.target)
+        sf.generate_seed_pos_table(None, 1, 19, 12)
+        sf.send_query_write_request(w.query, 0)
+
+    restore()
     return dict(w=w, p=p, idx=idx, pos=pos, sf=sf, R=oracle.encode(w.target), Q=oracle.encode(w.query),
-                QR=oracle.encode_rc(w.query), rctext=host_revcomp(w.query))
+                QR=oracle.encode_rc(w.query), rctext=host_revcomp(w.query), restore=restore)
 
 
 def test_device_table_matches_oracle(setup):
@@ -320,6 +326,7 @@ def test_refill_and_wide_loads_do_not_change_results(setup, refill, wide, ctas, 
     of their first base, skipping up to 24 leading bases) give the same HSPs
     and tile counts on both strands."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
+    setup["restore"]()
     saved = sf.get_tuning()
     sf.set_tuning(refill=refill, wide_loads=wide, ext_ctas_per_sm=ctas, substeps=sub)
     try:
@@ -341,6 +348,7 @@ def test_refill_and_wide_loads_batched_and_rm(setup, refill, wide):
     """The same settings on the batched path (units == plain calls) and on
     repeat-masker calls (rm_refill) against the oracle."""
     w, p, sf = setup["w"], setup["p"], setup["sf"]
+    setup["restore"]()
     saved = sf.get_tuning()
     sf.set_tuning(refill=refill, rm_refill=refill, wide_loads=wide)
     try:
