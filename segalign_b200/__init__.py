@@ -469,7 +469,7 @@ class SeedFilter:
 
     def get_tuning(self) -> dict:
         names = ("lane_cap", "ext_ctas_per_sm", "tile_hits", "step_bases", "range_ctas", "substeps", "call_range_ctas",
-                 "call_lane_ctas", "switch_now", "rm_lane_ctas", "rm_substeps", "rm_switch_now", "refill", "rm_refill", "wide_loads")
+                 "call_lane_ctas", "switch_now", "rm_lane_ctas", "rm_substeps", "rm_switch_now")
         return {n: int(self.lib.sa_get_tuning_param(n.encode())) for n in names}
 
     def set_timing(self, on: bool) -> None:

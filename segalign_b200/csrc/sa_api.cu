@@ -14,6 +14,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -26,6 +27,11 @@
 // Errors
 // ---------------------------------------------------------------------------
 static thread_local std::string t_err;
+// A slot's CUDA-graph capture (shared) against device-wide work from other
+// threads (exclusive): cudaDeviceSynchronize, cudaMalloc and cudaFree may not
+// run while any stream of the device is capturing, so query and target
+// uploads, table builds, key computation and frees wait for captures to end.
+static std::shared_mutex g_capture_mu;
 static thread_local sa_call_stats t_stats;
 static std::atomic<unsigned long long> g_launches{0};
 static std::atomic<int> g_timing{0};
@@ -174,7 +180,7 @@ struct Global {
     uint64_t max_hits_override = 0;
     uint64_t max_hits_default = 0;
     int rm_exclude_diag = 0;
-    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0, 0, 0, 0};  // autotuned on the genome-scale batch
+    SaTuning tuning{8192, 256, 3, 256, 592, 160, 32, 3, 1, 148, 0, 0, 2, 0};  // autotuned on the genome-scale batch
     // last target upload (to reuse it for the table build)
     const char* last_ref_ptr = nullptr;
     size_t last_ref_start = 0;
@@ -244,6 +250,7 @@ void make_rc_packed(const Packed& pk, Packed& rc) {
 
 // Uploads text[0, len) and packs it into pk (and its reverse complement into rc if given).
 int upload_pack(DevState& d, const char* text, uint64_t len, Packed& pk, Packed* rc) {
+    std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
     SA_CUDA_OK(cudaSetDevice(d.dev));
     SA_TRY(alloc_packed(pk, len));
     if (rc) SA_TRY(alloc_packed(*rc, len));
@@ -435,7 +442,6 @@ SaCallGrids sa_call_grids(const SaTuning& t, int num_sms, int mode) {
     if (mode == 1) {  // repeat-masker call
         c.lane_tuning.substeps = t.rm_substeps;
         c.lane_tuning.switch_now = t.rm_switch_now;
-        c.lane_tuning.refill = t.rm_refill;
         c.lane_ctas = t.rm_lane_ctas > 0 ? t.rm_lane_ctas : num_sms * t.ext_ctas_per_sm;
     }
     return c;
@@ -505,6 +511,7 @@ int run_chain(Slot* s, int mode, PhaseTimer& tm) {
         s->graph = nullptr;
         sa_prepare_extend_lane(g.params, g.tuning);  // kernel attributes are not set during capture
         const unsigned long long l0 = g_launches.load();
+        std::shared_lock<std::shared_mutex> capturing(g_capture_mu);
         SA_CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const int r = launch_call_chain(s, mode, tm);
         cudaGraph_t graph = nullptr;
@@ -633,6 +640,7 @@ int check_ready(bool need_query) {
 int ensure_keys(DevState& d, uint32_t buffer, int rev) {
     Global& g = G();
     if (d.qkeys[buffer][rev] && d.qkeys_ok[buffer][rev]) return SA_OK;
+    std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
     const Packed& q = rev ? d.qr[buffer] : d.qf[buffer];
     if (!q.data) {
         sa_set_error(SA_ERR_STATE, "query buffer %u is not resident", buffer);
@@ -1241,6 +1249,7 @@ int sa_send_ref_write_request(const char* seq, size_t start_addr, uint32_t len) 
 // common/seed_filter_interface.cu:103-113
 int sa_clear_ref(void) {
     invalidate_graphs();
+    std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
     Global& g = G();
     for (auto& d : g.devs) {
         cudaSetDevice(d.dev);
@@ -1256,6 +1265,7 @@ int sa_clear_ref(void) {
 }
 
 static int build_table_on(DevState& d, const Packed& ref, uint32_t step) {
+    std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
     Global& g = G();
     SA_CUDA_OK(cudaSetDevice(d.dev));
     const SaParams& p = g.params;
@@ -1515,6 +1525,7 @@ int sa_seed_and_filter(const uint64_t* seeds, uint32_t num_seeds, int rev, uint3
 int sa_clear_query(uint32_t buffer) {
     Global& g = G();
     if (buffer >= (uint32_t)kMaxBuffers) return SA_ERR_ARG;
+    std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
     for (auto& d : g.devs) {
         cudaSetDevice(d.dev);
         d.qf[buffer].release();
@@ -1533,6 +1544,7 @@ int sa_rm_send_query_write_request(void) {
             sa_set_error(SA_ERR_STATE, "no resident target");
             return SA_ERR_STATE;
         }
+        std::unique_lock<std::shared_mutex> dev_wide(g_capture_mu);
         SA_CUDA_OK(cudaSetDevice(d.dev));
         SA_TRY(alloc_packed(d.ref_rc, d.ref.len));
         make_rc_packed(d.ref, d.ref_rc);
@@ -1780,21 +1792,12 @@ int sa_set_tuning_param(const char* name, int value) {
         (n == "range_ctas" ? t.range_ctas : t.call_range_ctas) = value;
         return SA_OK;
     }
-    if (n == "wide_loads") {
-        if (value != 0 && value != 1) {
-            sa_set_error(SA_ERR_ARG, "wide_loads must be 0 or 1 (got %d)", value);
-            return SA_ERR_ARG;
-        }
-        t.wide_loads = value;
-        return SA_OK;
-    }
-    if (n == "switch_now" || n == "rm_switch_now" || n == "refill" || n == "rm_refill") {
+    if (n == "switch_now" || n == "rm_switch_now") {
         if (value != 0 && value != 1) {
             sa_set_error(SA_ERR_ARG, "%s must be 0 or 1 (got %d)", name, value);
             return SA_ERR_ARG;
         }
-        (n == "switch_now" ? t.switch_now : n == "rm_switch_now" ? t.rm_switch_now : n == "refill" ? t.refill
-                                                                                                   : t.rm_refill) = value;
+        (n == "switch_now" ? t.switch_now : t.rm_switch_now) = value;
         return SA_OK;
     }
     if (n == "rm_substeps") {
@@ -1849,9 +1852,7 @@ int sa_get_tuning_param(const char* name) {
     if (n == "call_lane_ctas") return t.call_lane_ctas;
     if (n == "switch_now") return t.switch_now;
     if (n == "rm_switch_now") return t.rm_switch_now;
-    if (n == "refill") return t.refill;
-    if (n == "rm_refill") return t.rm_refill;
-    if (n == "wide_loads") return t.wide_loads;
+
     if (n == "rm_substeps") return t.rm_substeps;
     if (n == "rm_lane_ctas") return t.rm_lane_ctas;
     return SA_ERR_ARG;

@@ -48,7 +48,6 @@ struct SaExtK {
     uint32_t tile_hits;
     uint32_t substeps;  // steps per lane-kernel iteration (at most)
     uint32_t switch_now;  // 1: a lane starts its left side in the step after its right side ends
-    uint32_t refill;      // 1: a lane whose hit ends takes the tile's next hit within the iteration
 };
 
 // Reverse the order of the 8 nibbles of a word.
@@ -164,7 +163,7 @@ __device__ __forceinline__ int sa_tbl(const char* tblb, uint32_t lo, uint32_t hi
 template <bool EDGE, int SH>
 __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, uint32_t hi, uint32_t off0,
                                                uint32_t avail, int neg, int xdrop, int& P, int& B, int& at,
-                                               bool& stop, int j, int& js) {
+                                               bool& stop) {
     int mn = INT_MAX;
     // Bases in pairs: the running best and minimum take both prefixes of a
     // pair with one 3-input max / min (DPX on sm_90 and later).
@@ -179,10 +178,7 @@ __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, ui
         B = __vimax3_s32(B, P0, P);
         mn = __vimin3_s32(mn, P0, P);
     }
-    if (!stop) {
-        at = B;
-        js = j;
-    }
+    if (!stop) at = B;
     stop = stop || ((B >> SH) - (mn >> SH) > xdrop);
 }
 
@@ -255,18 +251,10 @@ static size_t sa_lane_smem(uint32_t tile) {
     return SA_LANE_TABLES + 8 * (size_t)tile * 16 + 8 * (size_t)(tile + 1) * 8 + 8 * 64 * 16 + 8 * 64 * 8;
 }
 
-template <int MIN_CTAS, int STEP, bool EXACT, bool WIDE>
+template <int MIN_CTAS, int STEP, bool EXACT>
 __global__ void __launch_bounds__(256, MIN_CTAS)
 sa_k_extend_lane(SaExtK a, SaParams P) {
     constexpr int NW = STEP / 8;                  // 8-base windows per step
-    // WIDE: the target is read in aligned 16-byte chunks (one 128-bit load per
-    // 32-base step).  A direction's scan then starts at the chunk holding its
-    // first base: the `lead` bases before that base (0, 8, 16 or 24, whole
-    // 8-base windows) are skipped in the first step, and offsets, the best
-    // position and the stop tile are taken back by `lead`.  The query keeps
-    // word loads, shifted back by the same `lead` (into its padding at most).
-    static_assert(!WIDE || (STEP == 32 && !EXACT), "wide target loads: fast form, 32-base steps");
-    constexpr int NWR = WIDE ? 2 * NW : NW + 1;   // target words held
     constexpr int SCALE = 2 * STEP;               // packed score scale (fast form)
     constexpr int SH = STEP == 8 ? 4 : STEP == 16 ? 5 : 6;  // log2(SCALE)
     static_assert(STEP == 8 || STEP == 16 || STEP == 32, "8-, 16- or 32-base steps");
@@ -310,12 +298,10 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
     int dir = 0;
     // scan of the current direction: offset, bases available, word shifts,
     // words w[0..NW] of the coming step, next word addresses
-    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0, lead = 0;
-    uint32_t w_r[NWR], w_q[NW + 1];
+    uint32_t o = 0, avail = 0, sh_r = 0, sh_q = 0;
+    uint32_t w_r[NW + 1], w_q[NW + 1];
 #pragma unroll
-    for (int j = 0; j < NWR; ++j) w_r[j] = 0;
-#pragma unroll
-    for (int j = 0; j <= NW; ++j) w_q[j] = 0;
+    for (int j = 0; j <= NW; ++j) w_r[j] = w_q[j] = 0;
     const uint32_t* __restrict__ pr = ref;
     const uint32_t* __restrict__ pq = ref;
     // running score, best, offset of the first base reaching best
@@ -331,106 +317,19 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
         avail = min(ref_len - sr, qlen - sq);
         sh_r = (sr & 7u) * 4u;
         sh_q = (sq & 7u) * 4u;
-        if (WIDE) {
-            const uint32_t dw = (sr >> 3) & 3u;  // words between the chunk start and the first base's word
-            lead = 8u * dw;
-            avail += lead;
-            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + ((sr >> 3) - dw);
-            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (int64_t)(sq >> 3) - (int64_t)dw;
-            const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(pr));
-            const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(pr) + 1);
-            w_r[0] = c0.x, w_r[1] = c0.y, w_r[2] = c0.z, w_r[3] = c0.w;
-            w_r[NWR - 4] = c1.x, w_r[NWR - 3] = c1.y, w_r[NWR - 2] = c1.z, w_r[NWR - 1] = c1.w;
-            pr += 8;
+        pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
+        pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
 #pragma unroll
-            for (int j = 0; j <= NW; ++j) w_q[j] = __ldg(pq + j);
-        } else {
-            pr = (dir ? ref + sa_rev_words(ref_len) : ref) + (sr >> 3);
-            pq = (dir ? qp + sa_rev_words(qlen) : qp) + (sq >> 3);
-#pragma unroll
-            for (int j = 0; j <= NW; ++j) {
-                w_r[j] = __ldg(pr + j);
-                w_q[j] = __ldg(pq + j);
-            }
-            pr += NW + 1;
+        for (int j = 0; j <= NW; ++j) {
+            w_r[j] = __ldg(pr + j);
+            w_q[j] = __ldg(pq + j);
         }
+        pr += NW + 1;
         pq += NW + 1;
         o = 0;
         S = 0;
         best = 0;
         bpos = 0;
-    };
-
-    // Idle lanes take the next records of the warp tile, in order; true for a
-    // lane that got one.  Warp-collective.
-    auto take_records = [&](uint32_t idle) -> bool {
-        bool fresh = false;
-        if (tile_pos < tile_n) {
-            const uint32_t m = min((uint32_t)__popc(idle), tile_n - tile_pos);
-            const uint32_t rank = __popc(idle & lt);
-            if (!has && rank < m) {
-                const uint4 r = s_hits[tile_pos + rank];
-                rl = r.x;
-                ql = r.y;
-                scope = r.z;
-                unit_id = r.w;
-                fresh = true;
-            }
-            tile_pos += m;
-        }
-        return fresh;
-    };
-    // Start of a direction: a fresh hit (right), or the left side of the
-    // current hit after its right end.  Per lane.
-    auto start_lane = [&](bool fresh) {
-        const SaUnit U = a.units[unit_id];
-        if (fresh) {
-            // rm: hits outside [ref_start, ref_end] are never extended
-            // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
-            bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
-            // Coordinates past either sequence end (a caller-supplied table or
-            // seed beyond the sequences) are rejected, not read.
-            if (rl > a.ref_len || ql > U.q_len) {
-                atomicCAS(&a.ctr->error, 0ull, 5ull);
-                skip = true;
-            }
-            if (!skip) {
-                has = true;
-                nocap = false;
-                setup = true;
-                dir = 0;
-                tiles = 0;
-                ++ext_acc;
-            }
-        }
-        if (setup) {
-            setup = false;
-            begin_dir(U.q_packed, U.q_len);
-        }
-    };
-    // Candidates of the lanes that finished a hit (total >= hspthresh; the
-    // entropy factor is at most 1, so lower totals are never kept) go into the
-    // warp's ring; every 32 of them are tested and inserted.  Warp-collective.
-    bool finished = false;
-    int Lpos = 0, total = 0;
-    auto emit_finished = [&]() {
-        const bool emit = finished && (int)(float)total >= a.hspthresh;
-        const uint32_t em = __ballot_sync(SA_FULL, emit);
-        if (em) {
-            if (emit) {
-                const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
-                // {ref_start, query_start (before the rm flip), len, scope}, {total, unit} (:606-608)
-                s_em[slot] = make_uint4(rl - (uint32_t)Lpos, ql - (uint32_t)Lpos, (uint32_t)(Rpos + Lpos), scope);
-                s_ex[slot] = make_uint2((uint32_t)total, unit_id);
-            }
-            em_tail += __popc(em);
-            while (em_tail - em_head >= 32) {
-                __syncwarp();
-                sa_flush_candidates(a, s_em, s_ex, em_head, 32);
-                em_head += 32;
-            }
-        }
-        finished = false;
     };
 
     while (true) {
@@ -477,14 +376,56 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     tile_pos = 0;
                 }
             }
-            fresh = take_records(idle);
+            if (tile_pos < tile_n) {
+                const uint32_t m = min((uint32_t)__popc(idle), tile_n - tile_pos);
+                const uint32_t rank = __popc(idle & lt);
+                if (!has && rank < m) {
+                    const uint4 r = s_hits[tile_pos + rank];
+                    rl = r.x;
+                    ql = r.y;
+                    scope = r.z;
+                    unit_id = r.w;
+                    fresh = true;
+                }
+                tile_pos += m;
+            }
         }
-        if (fresh || setup) start_lane(fresh);
+
+        // ---- start of a direction: a fresh hit (right), or the left side of
+        // the current hit after its right end ----
+        if (fresh || setup) {
+            const SaUnit U = a.units[unit_id];
+            if (fresh) {
+                // rm: hits outside [ref_start, ref_end] are never extended
+                // (repeat_masker_src/seed_filter.cu:237-243, 304-333).
+                bool skip = (U.flags & 1u) && !(rl >= U.rm_lo && rl <= U.rm_hi);
+                // Coordinates past either sequence end (a caller-supplied table or
+                // seed beyond the sequences) are rejected, not read.
+                if (rl > a.ref_len || ql > U.q_len) {
+                    atomicCAS(&a.ctr->error, 0ull, 5ull);
+                    skip = true;
+                }
+                if (!skip) {
+                    has = true;
+                    nocap = false;
+                    setup = true;
+                    dir = 0;
+                    tiles = 0;
+                    ++ext_acc;
+                }
+            }
+            if (setup) {
+                setup = false;
+                begin_dir(U.q_packed, U.q_len);
+            }
+        }
+        const bool done = !__any_sync(SA_FULL, has) && exhausted && tile_pos >= tile_n;
 
         // ---- up to `substeps` STEP-base steps per busy lane: the lanes still
         // scanning go on while any lane of the warp does; a lane stops for
-        // this iteration when it goes to the long queue ----
-        bool to_long = false;
+        // this iteration when its direction ends or it goes to the long queue ----
+        bool finished = false, to_long = false;
+        int Lpos = 0, total = 0;
         bool scanning = has;
 #pragma unroll 1
         for (uint32_t sub = 0; sub < a.substeps; ++sub) {
@@ -496,25 +437,18 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     rwin[j] = __funnelshift_r(w_r[j], w_r[j + 1], sh_r);
                     qwin[j] = __funnelshift_r(w_q[j], w_q[j + 1], sh_q);
                 }
-                if (WIDE) {
-                    // the next chunk moves down; the one after it is loaded
-                    w_r[0] = w_r[4], w_r[1] = w_r[5], w_r[2] = w_r[6], w_r[3] = w_r[7];
-                    const uint4 c = __ldg(reinterpret_cast<const uint4*>(pr));
-                    w_r[4] = c.x, w_r[5] = c.y, w_r[6] = c.z, w_r[7] = c.w;
-                    pr += 4;
-                } else {
-                    w_r[0] = w_r[NW];
-    #pragma unroll
-                    for (int j = 1; j <= NW; ++j) w_r[j] = __ldg(pr + j - 1);
-                    pr += NW;
-                }
+                w_r[0] = w_r[NW];
                 w_q[0] = w_q[NW];
     #pragma unroll
-                for (int j = 1; j <= NW; ++j) w_q[j] = __ldg(pq + j - 1);
+                for (int j = 1; j <= NW; ++j) {
+                    w_r[j] = __ldg(pr + j - 1);
+                    w_q[j] = __ldg(pq + j - 1);
+                }
+                pr += NW;
                 pq += NW;
                 const bool edge = o + STEP > avail;
                 bool stop = false;
-                uint32_t lo, hi, stop_off = 0;
+                uint32_t lo, hi;
                 if (EXACT) {
                     bool alive = true;
                     int pk = 0;
@@ -535,28 +469,22 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     if (best != best_in) bpos = (int)o + pk;
                     stop = !alive;
                 } else {
-                    // windows before the direction's first base (WIDE, first step only)
-                    const int skip = (WIDE && o == 0) ? (int)(lead >> 3) : 0;
-                    int Pk = ((S - best) << SH) + STEP - 8 * skip, B = SCALE - 1, at = 0, js = 0;
+                    int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
                     if (!edge) {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
-                            if (WIDE && j < skip) continue;
                             sa_merge8(rwin[j], qwin[j], lo, hi);
-                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop, j,
-                                                      js);
+                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
                         }
                     } else {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
-                            if (WIDE && j < skip) continue;
                             sa_merge8(rwin[j], qwin[j], lo, hi);
                             // a base past the sequence end scores -(xdrop + 1)
                             sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
-                                                     a.xdrop, Pk, B, at, stop, j, js);
+                                                     a.xdrop, Pk, B, at, stop);
                         }
                     }
-                    if (WIDE && stop) stop_off = o + 8u * (uint32_t)js;
                     const int low = at & (SCALE - 1);
                     if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
                     const int best_in = best;
@@ -565,21 +493,15 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
                 if (stop) {
                     // Steps start at multiples of STEP (8, 16 or 32), so the stop offset
-                    // lies in 32-base tile o >> 5 whichever base of the step it is
-                    // (WIDE: the stopping 8-base window, taken back by lead, lies in
-                    // one tile).
-                    tiles += ((WIDE ? stop_off - lead : o) >> 5) + 1;
+                    // lies in 32-base tile o >> 5 whichever base of the step it is.
+                    tiles += (o >> 5) + 1;
                     if (dir == 0) {
                         Rbest = best;
-                        Rpos = best > 0 ? bpos - (int)lead : -1;  // -1 when no positive score
+                        Rpos = best > 0 ? bpos : -1;  // -1 when no positive score
                         dir = 1;
                         setup = true;
                     } else {
                         finished = true;
-                        Lpos = best > 0 ? bpos - (int)lead + 1 : 0;  // left offsets are 1-based
-                        total = Rbest + best;
-                        tiles_acc += tiles;
-                        has = false;
                     }
                     scanning = false;
                 } else {
@@ -589,28 +511,25 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                         scanning = false;
                     }
                 }
-            }
-            if (sub + 1 < a.substeps) {
-                // refill: a lane whose hit ended in this step emits it and takes
-                // the tile's next hit, to scan in the iteration's remaining
-                // steps; switch_now: a lane whose right side ended starts its
-                // left side at once
-                bool again = false;
-                if (a.refill) {
-                    emit_finished();
-                    const uint32_t idle2 = __ballot_sync(SA_FULL, !has);
-                    if (idle2 && tile_pos < tile_n) again = take_records(idle2);
+                if (finished) {
+                    Lpos = best > 0 ? bpos + 1 : 0;  // left offsets are 1-based
+                    total = Rbest + best;
+                    tiles_acc += tiles;
+                    has = false;
                 }
-                const bool go = again || (a.switch_now && setup);
-                if (__any_sync(SA_FULL, go)) {
-                    if (go) {
-                        start_lane(again);
-                        scanning = has && !to_long;
-                    }
+            }
+            // switch_now: a lane whose right side ended in this step starts
+            // its left side at once and scans in the iteration's remaining
+            // steps instead of idling until the next iteration
+            if (a.switch_now && sub + 1 < a.substeps && __any_sync(SA_FULL, setup)) {
+                if (setup) {
+                    setup = false;
+                    const SaUnit U = a.units[unit_id];
+                    begin_dir(U.q_packed, U.q_len);
+                    scanning = true;
                 }
             }
         }
-        emit_finished();
 
         // ---- long queue pushes (warp-aggregated) ----
         {
@@ -637,17 +556,27 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                 }
             }
         }
-        const bool done = !__any_sync(SA_FULL, has || setup) && exhausted && tile_pos >= tile_n;
-        if (done) {
-            // whatever candidates are left
-            while (em_tail != em_head) {
+        // ---- candidate HSPs (total >= hspthresh; the entropy factor is at
+        // most 1, so lower totals are never kept) into the warp's ring ----
+        {
+            const bool emit = finished && (int)(float)total >= a.hspthresh;
+            const uint32_t em = __ballot_sync(SA_FULL, emit);
+            if (emit) {
+                const uint32_t slot = (em_tail + __popc(em & lt)) & 63u;
+                // {ref_start, query_start (before the rm flip), len, scope}, {total, unit} (:606-608)
+                s_em[slot] = make_uint4(rl - (uint32_t)Lpos, ql - (uint32_t)Lpos, (uint32_t)(Rpos + Lpos), scope);
+                s_ex[slot] = make_uint2((uint32_t)total, unit_id);
+            }
+            em_tail += __popc(em);
+            // full batches of 32; at the end, whatever is left
+            while (em_tail - em_head >= 32 || (done && em_tail != em_head)) {
                 const uint32_t n = min(em_tail - em_head, 32u);
                 __syncwarp();
                 sa_flush_candidates(a, s_em, s_ex, em_head, n);
                 em_head += n;
             }
-            break;
         }
+        if (done) break;
     }
     // flush statistics
     unsigned long long t = tiles_acc, e = ext_acc;
@@ -872,7 +801,6 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.tile_hits = (uint32_t)t.tile_hits;
     a.substeps = (uint32_t)t.substeps;
     a.switch_now = t.switch_now ? 1u : 0u;
-    a.refill = t.refill ? 1u : 0u;
     return a;
 }
 
@@ -891,26 +819,24 @@ static bool sa_lane_fast_form(const SaParams& p, int step) {
     return x >= 0 && 7 * mx <= x && x * scale - low * step < (1ll << 31) && mx * scale * step < (1ll << 31);
 }
 
-template <int C, int STEP, bool EXACT, bool WIDE>
+template <int C, int STEP, bool EXACT>
 static void sa_lane_launch(const SaExtK& a, const SaParams& p, int grid, size_t smem, cudaStream_t st) {
-    if (grid > 0) sa_k_extend_lane<C, STEP, EXACT, WIDE><<<grid, 256, smem, st>>>(a, p);
-    else cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem);
+    if (grid > 0) sa_k_extend_lane<C, STEP, EXACT><<<grid, 256, smem, st>>>(a, p);
+    else cudaFuncSetAttribute(sa_k_extend_lane<C, STEP, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 template <int C>
-static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, bool wide, int grid,
-                             size_t smem, cudaStream_t st) {
+static void sa_lane_dispatch(const SaExtK& a, const SaParams& p, int step, bool exact, int grid, size_t smem,
+                             cudaStream_t st) {
     if (step == 32) {
-        if (exact) sa_lane_launch<C, 32, true, false>(a, p, grid, smem, st);
-        else if (wide) sa_lane_launch<C, 32, false, true>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 32, false, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 32, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 32, false>(a, p, grid, smem, st);
     } else if (step == 16) {
-        if (exact) sa_lane_launch<C, 16, true, false>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 16, false, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 16, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 16, false>(a, p, grid, smem, st);
     } else {
-        if (exact) sa_lane_launch<C, 8, true, false>(a, p, grid, smem, st);
-        else sa_lane_launch<C, 8, false, false>(a, p, grid, smem, st);
+        if (exact) sa_lane_launch<C, 8, true>(a, p, grid, smem, st);
+        else sa_lane_launch<C, 8, false>(a, p, grid, smem, st);
     }
 }
 
@@ -927,12 +853,11 @@ void sa_prepare_extend_lane(const SaParams& p, const SaTuning& t) {
     const size_t smem = sa_lane_smem(1024);
     SaExtK none{};
     for (int step : {8, 16, 32})
-        for (bool exact : {false, true})
-            for (bool wide : {false, true}) {
-                sa_lane_dispatch<2>(none, p, step, exact, wide, 0, smem, 0);
-                sa_lane_dispatch<3>(none, p, step, exact, wide, 0, smem, 0);
-                sa_lane_dispatch<4>(none, p, step, exact, wide, 0, smem, 0);
-            }
+        for (bool exact : {false, true}) {
+            sa_lane_dispatch<2>(none, p, step, exact, 0, smem, 0);
+            sa_lane_dispatch<3>(none, p, step, exact, 0, smem, 0);
+            sa_lane_dispatch<4>(none, p, step, exact, 0, smem, 0);
+        }
     done[dev] = true;
 }
 
@@ -944,10 +869,9 @@ void sa_launch_extend_lane(SaWork& w, const SaExtendArgs& x, const SaParams& p, 
     const int grid = grid_ctas > 0 ? grid_ctas : num_sms * t.ext_ctas_per_sm;
     const size_t smem = sa_lane_smem(a.tile_hits);
     const bool exact = !sa_lane_fast_form(p, t.step_bases);
-    const bool wide = t.wide_loads != 0;
-    if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, wide, grid, smem, st);
-    else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, wide, grid, smem, st);
-    else sa_lane_dispatch<2>(a, p, t.step_bases, exact, wide, grid, smem, st);
+    if (t.ext_ctas_per_sm >= 4) sa_lane_dispatch<4>(a, p, t.step_bases, exact, grid, smem, st);
+    else if (t.ext_ctas_per_sm == 3) sa_lane_dispatch<3>(a, p, t.step_bases, exact, grid, smem, st);
+    else sa_lane_dispatch<2>(a, p, t.step_bases, exact, grid, smem, st);
     sa_note_launch();
 }
 

@@ -140,11 +140,6 @@ struct SaTuning {
     // a repeat-masker call's lane kernel (its hits are windowed and its calls
     // large): CTAs (0: the batched grid), steps per iteration, switch_now
     int rm_lane_ctas, rm_substeps, rm_switch_now;
-    int refill;          // 1: a lane whose hit ends within an iteration takes the warp tile's
-                         // next hit and scans it in the iteration's remaining steps
-    int rm_refill;       // the same for a repeat-masker call's lane kernel
-    int wide_loads;      // 1: the lane kernel reads the target in aligned 16-byte chunks
-                         // (fast scoring form with 32-base steps; otherwise word loads)
 };
 
 // ---- sa_pack.cu ----

@@ -317,57 +317,3 @@ def test_transitions_repeat_rich_sample(built):
             hsps += len(want) - 1
     assert hits > 5_000_000 and hsps > 50_000
 
-
-@pytest.mark.parametrize("refill,wide,ctas,sub", [(1, 0, 3, 3), (0, 1, 3, 3), (1, 1, 3, 3), (1, 1, 2, 6), (1, 0, 4, 1),
-                                                  (0, 1, 2, 2), (1, 1, 3, 8)])
-def test_refill_and_wide_loads_do_not_change_results(setup, refill, wide, ctas, sub):
-    """A lane taking the tile's next hit within an iteration (refill) and the
-    aligned 16-byte target loads (wide_loads: scans start at the 16-byte chunk
-    of their first base, skipping up to 24 leading bases) give the same HSPs
-    and tile counts on both strands."""
-    w, p, sf = setup["w"], setup["p"], setup["sf"]
-    setup["restore"]()
-    saved = sf.get_tuning()
-    sf.set_tuning(refill=refill, wide_loads=wide, ext_ctas_per_sm=ctas, substeps=sub)
-    try:
-        for rev in (False, True):
-            text = setup["rctext"] if rev else w.query
-            for j0 in (0, 400_000, 750_000):
-                seeds = host_seeds(text, j0, min(j0 + 250_000, len(w.query) - 19))
-                want, st = oracle.seed_and_filter(p, setup["R"], setup["QR"] if rev else setup["Q"], setup["idx"],
-                                                  setup["pos"], seeds, rev)
-                compare_segments(sf.seed_and_filter(seeds, rev, 0), want,
-                                 f"refill={refill} wide={wide} ctas={ctas} sub={sub} rev={rev} j0={j0}")
-                assert sf.last_call_stats()["tiles"] == st["tiles_right"] + st["tiles_left"]
-    finally:
-        sf.set_tuning(**saved)
-
-
-@pytest.mark.parametrize("refill,wide", [(1, 0), (0, 1), (1, 1)])
-def test_refill_and_wide_loads_batched_and_rm(setup, refill, wide):
-    """The same settings on the batched path (units == plain calls) and on
-    repeat-masker calls (rm_refill) against the oracle."""
-    w, p, sf = setup["w"], setup["p"], setup["sf"]
-    setup["restore"]()
-    saved = sf.get_tuning()
-    sf.set_tuning(refill=refill, rm_refill=refill, wide_loads=wide)
-    try:
-        units = [(0, r, a, min(a + 250_000, len(w.query) - 19)) for r in (0, 1) for a in (0, 500_000)]
-        outs = sf.seed_and_filter_batch(units)
-        for (b, r, a, e), got in zip(units, outs):
-            seeds = host_seeds(setup["rctext"] if r else w.query, a, e)
-            want, _ = oracle.seed_and_filter(p, setup["R"], setup["QR"] if r else setup["Q"], setup["idx"],
-                                             setup["pos"], seeds, bool(r))
-            compare_segments(got, want, f"batched refill={refill} wide={wide} unit {(r, a, e)}")
-        sf.rm_send_query_write_request()
-        R = setup["R"]
-        RC = oracle.rc_codes(R)
-        t_rc = host_revcomp(w.target)
-        for rev in (0, 1):
-            seeds = host_seeds(t_rc if rev else w.target, 300_000, 400_000)
-            got = sf.rm_seed_and_filter(seeds, bool(rev), 200_000, 600_000)
-            want, _ = oracle.seed_and_filter(p, R, RC if rev else R, setup["idx"], setup["pos"], seeds, bool(rev), 1,
-                                             200_000, 600_000)
-            compare_segments(got, want, f"rm refill={refill} wide={wide} rev={rev}")
-    finally:
-        sf.set_tuning(**saved)
