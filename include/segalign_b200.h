@@ -226,6 +226,9 @@ int sa_serve_stop(void);
 
 /* ---- results, configuration, diagnostics (no reference counterpart) ---- */
 
+/* Releases an array the library returned.  The largest batched output freed
+ * (64 MiB or more) is kept for the next batched call's output, which then
+ * skips the page faults of a fresh allocation; sa_shutdown_processor() frees it. */
 void sa_free_segments(sa_segment* segments);
 
 /* MAX_HITS override (src/seed_filter.cu:18,784-791); 0 restores the default. */

@@ -1070,6 +1070,76 @@ int seed_and_filter_coalesced(const uint64_t* seeds, uint32_t num_seeds, int rev
 // header record {0, 0, HSP count, hit count} then its HSPs; a unit with an
 // empty window gets its header only.  One malloc'd block (grown by realloc,
 // which remaps rather than copies at these sizes), freed by sa_free_segments.
+// Batched outputs of at least kKeepBytes are remembered, and the last one the
+// caller frees is kept for the next batched output that fits: a fresh array of
+// hundreds of MB pays a page fault per 4 KiB page at its first write.
+constexpr uint64_t kKeepBytes = 64ull << 20;
+struct OutKeep {
+    std::mutex mu;
+    std::vector<std::pair<void*, uint64_t>> live;  // batched outputs handed out (pointer, bytes)
+    void* kept = nullptr;
+    uint64_t kept_bytes = 0;
+};
+OutKeep& out_keep() {
+    static OutKeep k;
+    return k;
+}
+
+// Allocation of a batched output array of `bytes` (or more, when a kept one fits).
+void* out_alloc(uint64_t bytes, uint64_t* got) {
+    OutKeep& k = out_keep();
+    std::lock_guard<std::mutex> lk(k.mu);
+    void* p = nullptr;
+    if (k.kept && k.kept_bytes >= bytes) {
+        p = k.kept;
+        *got = k.kept_bytes;
+        k.kept = nullptr;
+        k.kept_bytes = 0;
+    } else {
+        p = malloc(bytes);
+        *got = bytes;
+    }
+    if (p && *got >= kKeepBytes) k.live.emplace_back(p, *got);
+    return p;
+}
+
+void out_forget(void* p) {
+    OutKeep& k = out_keep();
+    for (size_t i = 0; i < k.live.size(); ++i)
+        if (k.live[i].first == p) {
+            k.live.erase(k.live.begin() + (std::ptrdiff_t)i);
+            return;
+        }
+}
+
+// Returns true when p was a remembered batched output (kept or freed here).
+bool out_release(void* p) {
+    OutKeep& k = out_keep();
+    std::lock_guard<std::mutex> lk(k.mu);
+    for (size_t i = 0; i < k.live.size(); ++i)
+        if (k.live[i].first == p) {
+            const uint64_t b = k.live[i].second;
+            k.live.erase(k.live.begin() + (std::ptrdiff_t)i);
+            if (b > k.kept_bytes) {
+                free(k.kept);
+                k.kept = p;
+                k.kept_bytes = b;
+            } else {
+                free(p);
+            }
+            return true;
+        }
+    return false;
+}
+
+void out_drop_kept() {
+    OutKeep& k = out_keep();
+    std::lock_guard<std::mutex> lk(k.mu);
+    free(k.kept);
+    k.kept = nullptr;
+    k.kept_bytes = 0;
+}
+
 struct SegmentWriter : SaBatchSink {
     const uint64_t n_units;
     uint64_t* offsets;
@@ -1082,7 +1152,9 @@ struct SegmentWriter : SaBatchSink {
         for (uint32_t i = 0; i < n; ++i)
             if (units[i].end > units[i].start) orig.push_back(i);
     }
-    ~SegmentWriter() override { free(o); }
+    ~SegmentWriter() override {
+        if (o && !out_release(o)) free(o);
+    }
 
     sa_segment* release() {
         sa_segment* p = o;
@@ -1093,7 +1165,22 @@ struct SegmentWriter : SaBatchSink {
     int reserve(uint64_t need) {
         if (need <= cap) return SA_OK;
         uint64_t c = std::max<uint64_t>(need, cap + cap / 2);
-        void* p = realloc(o, sizeof(sa_segment) * c);
+        void* p = nullptr;
+        if (!o) {
+            uint64_t got = 0;
+            p = out_alloc(sizeof(sa_segment) * c, &got);
+            c = got / sizeof(sa_segment);
+        } else {
+            {
+                std::lock_guard<std::mutex> lk(out_keep().mu);
+                out_forget(o);
+            }
+            p = realloc(o, sizeof(sa_segment) * c);
+            if (p && sizeof(sa_segment) * c >= kKeepBytes) {
+                std::lock_guard<std::mutex> lk(out_keep().mu);
+                out_keep().live.emplace_back(p, sizeof(sa_segment) * c);
+            }
+        }
         if (!p) {
             sa_set_error(SA_ERR_NOMEM, "cannot hold %llu HSP records", (unsigned long long)c);
             return SA_ERR_NOMEM;
@@ -1112,7 +1199,9 @@ struct SegmentWriter : SaBatchSink {
         if (!n) return SA_OK;
         uint64_t body = 0;
         for (uint32_t i = 0; i < n; ++i) body += cnt[i];
-        SA_TRY(reserve(at + body + (orig[u0 + n - 1] + 1 - next)));
+        // this group's records plus a header for every unit not yet written,
+        // so that finish() does not grow the array
+        SA_TRY(reserve(at + body + (n_units - next) + 1));
         std::vector<uint64_t> dst(n), src(n);
         uint64_t s = 0;
         for (uint32_t i = 0; i < n; ++i) {
@@ -1591,6 +1680,7 @@ int sa_rm_clear_query(void) {
 int sa_shutdown_processor(void) {
     Global& g = G();
     free_staging();
+    out_drop_kept();
     {
         std::lock_guard<std::mutex> lk(g.mu);
         for (auto& d : g.devs)
@@ -1689,7 +1779,9 @@ int sa_seed_and_filter_batch(const sa_unit* units, uint32_t n_units, sa_segment*
     return SA_OK;
 }
 
-void sa_free_segments(sa_segment* p) { free(p); }
+void sa_free_segments(sa_segment* p) {
+    if (p && !out_release(p)) free(p);
+}
 
 int sa_set_timing(int on) {
     invalidate_graphs();
