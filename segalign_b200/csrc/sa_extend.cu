@@ -220,29 +220,31 @@ __device__ __forceinline__ void sa_flush_candidates(const SaExtK& a, const uint4
     }
     __syncwarp();  // slots are rewritten by later appends
     int keep = 0, score = 0;
-    SaUnit U{};
+    bool known = false;
+    uint32_t qs = 0;
     if (on) {
-        U = a.units[x.y];
+        const SaUnit U = a.units[x.y];
         const int total = (int)x.x, ext = (int)r.z;
-        int cnt[4] = {0, 0, 0, 0};
-        const bool eb = sa_entropy_branch(a, total);
-        if (eb) {
-            const int64_t nb = (int64_t)ext + 1;
-            for (int64_t i = 0; i < nb; i += 8) {
-                uint32_t nm = (nb - i >= 8) ? 0xffu : ((1u << (uint32_t)(nb - i)) - 1u);
-                sa_count_matches8(sa_load8(a.ref, (int64_t)r.x + i), sa_load8(U.q_packed, (int64_t)r.y + i), nm, cnt);
-            }
+        qs = r.y;
+        if (U.flags & 2u) qs = a.ref_len - 1 - (qs + r.z);
+        // A candidate whose key the set already holds was kept with this same
+        // key (the scope fixes the unit, so the same bases): it is a survivor,
+        // and its match counts, logs and insertion are skipped.
+        known = sa_hash_contains(a.hset, a.ctr->hash_mask, r.w, r.x, qs, r.z);
+        if (known) {
+            keep = 1;
+        } else {
+            int cnt[4] = {0, 0, 0, 0};
+            const bool eb = sa_entropy_branch(a, total);
+            if (eb) sa_count_matches_span(a.ref, r.x, U.q_packed, r.y, (int64_t)ext + 1, cnt);
+            sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
         }
-        sa_keep_score(total, ext, cnt, eb, a.hspthresh, &keep, &score);
     }
     const uint32_t km = __ballot_sync(SA_FULL, keep != 0);
     if (lane == 0 && km) atomicAdd(&a.ctr->surv_count, (unsigned long long)__popc(km));
     unsigned long long claimed = ~0ull;
-    if (keep) {
-        uint32_t qs = r.y;
-        if (U.flags & 2u) qs = a.ref_len - 1 - (qs + r.z);
+    if (keep && !known)
         claimed = sa_hash_insert(a.hset, a.ctr->hash_mask, r.w, r.x, qs, r.z, score, &a.ctr->hash_overflow);
-    }
     sa_hash_note_used(a.hset, &a.ctr->hash_used, claimed);
 }
 

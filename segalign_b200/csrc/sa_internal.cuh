@@ -166,6 +166,29 @@ __device__ __forceinline__ unsigned long long sa_hash_insert(const SaHashSet& hs
     return ~0ull;
 }
 
+#define SA_HASH_LOOKUP_PROBES 64
+
+// Whether the set already holds the key (scope, rs, qs, len).  Read-only and
+// conservative.  Slots are read from L2 (.cg: no line from an earlier call can
+// answer), a key never changes once its 128-bit CAS has written it, and a
+// slot seen empty or half-written ends the search with false, as does a long
+// probe chain.  A true answer therefore means an HSP with exactly this key was
+// kept by this call; false only sends the caller down the full insert path.
+__device__ __forceinline__ bool sa_hash_contains(const SaHashSet& hs, unsigned long long mask, uint32_t scope,
+                                                 uint32_t rs, uint32_t qs, uint32_t len) {
+    const unsigned long long k0 = ((unsigned long long)scope << 32) | rs;
+    const unsigned long long k1 = ((unsigned long long)qs << 32) | len;
+    unsigned long long h = sa_hash_mix(k0, k1) & mask;
+    for (int probe = 0; probe < SA_HASH_LOOKUP_PROBES; ++probe) {
+        unsigned long long s0, s1;
+        asm volatile("ld.global.cg.v2.u64 {%0, %1}, [%2];" : "=l"(s0), "=l"(s1) : "l"(hs.keys + 2 * h));
+        if (s0 == k0 && s1 == k1) return true;
+        if (s0 == ~0ull || s1 == ~0ull) return false;
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+
 __device__ __forceinline__ uint32_t sa_lanemask_lt();
 
 // Appends the slots claimed by the lanes of a warp (slot != ~0) to the set's
@@ -202,6 +225,43 @@ __device__ __forceinline__ uint32_t sa_load8(const uint32_t* __restrict__ packed
     uint32_t lo = __ldg(packed + w);
     uint32_t hi = __ldg(packed + w + 1);
     return __funnelshift_r(lo, hi, sh);
+}
+
+// Per-base match counts over nb >= 1 consecutive positions from rp (target
+// R) and qp (query Q): c[b] += #positions whose codes are equal and == b, for
+// b in 0..3 (the A/C/G/T counts of src/seed_filter.cu:580-598).  One new word
+// per sequence per 8 bases; the counts come from bit planes of the target
+// codes at the matching nibbles (code bit 0, bit 1, both).
+__device__ __forceinline__ void sa_count_matches_span(const uint32_t* __restrict__ R, int64_t rp,
+                                                      const uint32_t* __restrict__ Q, int64_t qp, int64_t nb,
+                                                      int* c) {
+    const uint32_t* pr = R + (rp >> 3);
+    const uint32_t* pq = Q + (qp >> 3);
+    const uint32_t shr = (uint32_t)(rp & 7) * 4u, shq = (uint32_t)(qp & 7) * 4u;
+    uint32_t r0 = __ldg(pr), q0 = __ldg(pq);
+    int n = 0, n0 = 0, n1 = 0, n01 = 0;
+    for (int64_t i = 0; i < nb; i += 8) {
+        ++pr;
+        ++pq;
+        const uint32_t r1 = __ldg(pr), q1 = __ldg(pq);
+        const uint32_t rw = __funnelshift_r(r0, r1, shr), qw = __funnelshift_r(q0, q1, shq);
+        r0 = r1;
+        q0 = q1;
+        uint32_t d = rw ^ qw;
+        d |= d >> 1;
+        d |= d >> 2;  // bit 4k set: codes of base k differ
+        uint32_t v = ~(d | (rw >> 2) | (rw >> 3)) & 0x11111111u;  // equal codes in 0..3
+        if (nb - i < 8) v &= (1u << (4u * (uint32_t)(nb - i))) - 1u;
+        const uint32_t b0 = rw & v, b1 = (rw >> 1) & v;
+        n += __popc(v);
+        n0 += __popc(b0);
+        n1 += __popc(b1);
+        n01 += __popc(b0 & b1);
+    }
+    c[0] += n - n0 - n1 + n01;
+    c[1] += n0 - n01;
+    c[2] += n1 - n01;
+    c[3] += n01;
 }
 
 __device__ __forceinline__ uint32_t sa_code_at(const uint32_t* __restrict__ packed, int64_t p) {
