@@ -131,7 +131,7 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 //     P(k) = SCALE * (S(k) - best_in) + (STEP - 1 - k),   SCALE = 2 * STEP,
 // so a running max over P yields the best score together with the FIRST base
 // that reached it; the best carried in from earlier steps enters as
-// SCALE - 1, which no base of the step ties.  The X-drop stop test runs once
+// STEP, which no base of the step ties.  The X-drop stop test runs once
 // per 8-base window: with m = the window's minimum score and b = the best
 // score at the window's end, a base of the window stops the scan iff
 // b - m > xdrop, provided 7 * max(0, max_sub) <= xdrop (max_sub = largest
@@ -141,8 +141,10 @@ __device__ __forceinline__ bool sa_entropy_branch(const SaExtK& a, int total) {
 // bound shows that no base after a stop in the window can raise the best
 // (that takes a climb of more than xdrop), so the window's best is the best
 // at the stop.  Bases past the sequence end score -(xdrop + 1): the first of
-// them stops the scan.  Parameters outside the bound use the exact form,
-// which tests every base.
+// them stops the scan.  The test runs on the packed values themselves:
+// with B = SCALE * b + i (i in 0..STEP) and min = SCALE * m + j (j in
+// 0..STEP-1), b - m > xdrop  <=>  B - min > SCALE * xdrop + STEP.
+// Parameters outside the bound use the exact form, which tests every base.
 // ---------------------------------------------------------------------------
 // Byte b of lo (hi) = byte offset ((q << 3) | r) * 4 of the score of base 2b
 // (2b+1) in a 64-entry int table; codes are 0..7, so a byte never carries.
@@ -160,9 +162,9 @@ __device__ __forceinline__ int sa_tbl(const char* tblb, uint32_t lo, uint32_t hi
 // running best; `at` takes B at the end of each window up to and including
 // the one that stops; `stop` is set by that window.  EDGE: bases at
 // off0 + k >= avail score `neg`.
-template <bool EDGE, int SH>
+template <bool EDGE>
 __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, uint32_t hi, uint32_t off0,
-                                               uint32_t avail, int neg, int xdrop, int& P, int& B, int& at,
+                                               uint32_t avail, int neg, uint32_t T, int& P, int& B, int& at,
                                                bool& stop) {
     int mn = INT_MAX;
     // Bases in pairs: the running best and minimum take both prefixes of a
@@ -179,7 +181,7 @@ __device__ __forceinline__ void sa_window_fast(const char* tblb, uint32_t lo, ui
         mn = __vimin3_s32(mn, P0, P);
     }
     if (!stop) at = B;
-    stop = stop || ((B >> SH) - (mn >> SH) > xdrop);
+    stop = stop || (uint32_t)(B - mn) > T;
 }
 
 // Exact form, one 8-base window at step-relative indices k0..k0+7: S =
@@ -471,24 +473,27 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     if (best != best_in) bpos = (int)o + pk;
                     stop = !alive;
                 } else {
-                    int Pk = ((S - best) << SH) + STEP, B = SCALE - 1, at = 0;
+                    // B - min > SCALE * xdrop + STEP  <=>  (B >> SH) - (min >> SH) > xdrop, because
+                    // the low parts of B (0..STEP) and min (0..STEP-1) differ by less than SCALE
+                    const uint32_t T = (uint32_t)a.xdrop * SCALE + STEP;
+                    int Pk = ((S - best) << SH) + STEP, B = STEP, at = 0;
                     if (!edge) {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
                             sa_merge8(rwin[j], qwin[j], lo, hi);
-                            sa_window_fast<false, SH>(tblb, lo, hi, o + 8 * j, avail, 0, a.xdrop, Pk, B, at, stop);
+                            sa_window_fast<false>(tblb, lo, hi, o + 8 * j, avail, 0, T, Pk, B, at, stop);
                         }
                     } else {
     #pragma unroll
                         for (int j = 0; j < NW; ++j) {
                             sa_merge8(rwin[j], qwin[j], lo, hi);
                             // a base past the sequence end scores -(xdrop + 1)
-                            sa_window_fast<true, SH>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1,
-                                                     a.xdrop, Pk, B, at, stop);
+                            sa_window_fast<true>(tblb, lo, hi, o + 8 * j, avail, -(a.xdrop + 1) * SCALE - 1, T, Pk,
+                                                 B, at, stop);
                         }
                     }
                     const int low = at & (SCALE - 1);
-                    if (low != SCALE - 1) bpos = (int)o + (STEP - 1 - low);
+                    if (low != STEP) bpos = (int)o + (STEP - 1 - low);
                     const int best_in = best;
                     best = best_in + (at >> SH);
                     S = best_in + (Pk >> SH);  // exact after a full step without a stop

@@ -22,7 +22,7 @@
 
 // Words from word 0 of a packed sequence of `len` bases to word 0 of its
 // reversed copy: a multiple of 4, so that word 0 of both copies starts a
-// 16-byte chunk (the lane kernel reads the target in aligned 16-byte chunks).
+// 16-byte chunk.
 __host__ __device__ __forceinline__ uint64_t sa_rev_words(uint64_t len) {
     return ((len + 7) / 8 + 2 * SA_PADW + 3) & ~3ull;
 }
