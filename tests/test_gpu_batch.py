@@ -42,7 +42,7 @@ def test_batch_units_match_per_call_oracle(setup):
     units = _units(L, 103) + [(0, 0, 5, 5)]  # plus one empty window
     outs = sf.seed_and_filter_batch(units)
     assert len(outs) == len(units)
-    total_hits = 0
+    total_hits = total_surv = 0
     for (buf, rev, a, b), got in zip(units, outs):
         text = setup["rctext"] if rev else w.query
         seeds = host_seeds(text, a, b)
@@ -53,7 +53,9 @@ def test_batch_units_match_per_call_oracle(setup):
                                           setup["pos"], seeds, rev)
         compare_segments(got, want, f"unit {(rev, a, b)}")
         total_hits += st["num_hits"]
+        total_surv += st["survivors"]
     assert sf.last_call_stats()["num_hits"] == total_hits
+    assert sf.last_call_stats()["survivors"] == total_surv
 
 
 def test_batch_keep_on_device_counts(setup):

@@ -61,6 +61,9 @@ def test_seed_and_filter_per_chunk(setup, rev):
         cs = sf.last_call_stats()
         assert cs["num_hits"] == st["num_hits"]
         assert cs["tiles"] == st["tiles_right"] + st["tiles_left"]
+        # kept HSPs before dedup: candidates already in the call's HSP set
+        # count as kept without their keep test being rerun
+        assert cs["survivors"] == st["survivors"]
         total_hits += st["num_hits"]
     assert total_hits > 100_000
 
