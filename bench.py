@@ -23,9 +23,11 @@ Beside them: like-for-like batched/plain ratios, uneven windows, serving on
 the resident table, an unranked timing of the reference's own kernels on a
 sample of the same units, the CPU port on a bounded sample, and the 600 Mbp
 legs (batched and plain with transitions, serving on that table, repeat-masker
-self-alignment).  Ranks (torchrun) are weak-scaled: each rank runs its own
-genome pair of the same shape; value = all ranks' extensions / the slowest
-rank's time.
+self-alignment).  Ranks (torchrun) run one job: the target is replicated to
+every GPU and the query is split, with no collective on the data path.  By
+default (--scaling weak) the job's query is N blocks of the named size, drawn
+from the one target, block r on rank r; --scaling strong splits the named
+query into N slices.  value = all ranks' extensions / the slowest rank's time.
 
 --impl reference times the reference semantics on the host cores (the CPU
 port in oracle/), rank 0 only.
@@ -58,6 +60,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1.0 = named sizes)")
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="N>1: weak = one query block of the named size per rank against the one target; "
+                         "strong = the named query split across the ranks")
     ap.add_argument("--cpu-chunks", type=int, default=None,
                     help="units in the bounded CPU sample (default 64; 2 for --workload large)")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -403,21 +408,38 @@ def job_figures(ms_step: float, hits: float, hsps: float, dist=None, device: str
             "hsps_per_s": hs / (ms / 1000.0)}
 
 
-def make_workload(args, rank: int):
-    """(workload, transition, description) of --workload; ranks get their own seeds."""
+def make_workload(args, rank: int = 0, world: int = 1):
+    """(workload, transition, description) of --workload for one rank of a job
+    over `world` ranks.  The target is the same on every rank (replicated, as
+    the reference replicates it to every GPU).  Weak scaling: the job's query is
+    `world` blocks of the named size, drawn from that target, and rank r runs
+    block r (block 0 is the one-GPU workload).  Strong scaling: the job is the
+    named query and rank r runs its r-th contiguous slice."""
     from segalign_b200 import synth
 
+    weak = getattr(args, "scaling", "weak") == "weak"
+    block = rank if (weak and world > 1) else 0
     if args.workload == "large":
-        w = synth.make(4, seed=104 + 1000 * rank, scale=args.scale)
-        w = synth.Workload(w.target, w.query[: args.query_sample], w.target_chr, w.query_chr)
-        desc = (f"large: 600 Mbp target (12 chr) x the first {len(w.query) / 1e6:.0f} Mbp of a 600 Mbp query, "
+        w = synth.make(4, seed=104, scale=args.scale, block=block)
+        q = w.query[: args.query_sample]
+        desc = (f"large: 600 Mbp target (12 chr) x the first {len(q) / 1e6:.0f} Mbp of a 600 Mbp query, "
                 "GC 41%, 45% repeats, 12of19 with one transition, HOXD70, xdrop 910, hspthresh 3000, entropy, "
                 "both strands, 10 Mbp intervals + 50 kbp overlap, 250 kbp units")
-        return w, True, desc
-    w = synth.make(2, seed=102 + 1000 * rank, scale=args.scale)
-    desc = ("genome scale: 100 Mbp target (6 chr) x 108 Mbp query, GC 36%, 12of19, HOXD70, xdrop 910, "
-            "hspthresh 3000, entropy, both strands, 10 Mbp intervals + 50 kbp overlap, 250 kbp units")
-    return w, False, desc
+        transition = True
+    else:
+        w = synth.make(2, seed=102, scale=args.scale, block=block)
+        q = w.query
+        desc = ("genome scale: 100 Mbp target (6 chr) x 108 Mbp query, GC 36%, 12of19, HOXD70, xdrop 910, "
+                "hspthresh 3000, entropy, both strands, 10 Mbp intervals + 50 kbp overlap, 250 kbp units")
+        transition = False
+    if world > 1:
+        if weak:
+            desc += f"; job: {world} query blocks of this size against the one target, block r on rank r"
+        else:
+            a, b = len(q) * rank // world, len(q) * (rank + 1) // world
+            q = q[a:b]
+            desc += f"; job: this query split into {world} contiguous slices, slice r on rank r"
+    return synth.Workload(w.target, q, w.target_chr, [(0, len(q))]), transition, desc
 
 
 def run_reference(args):
@@ -529,8 +551,9 @@ def run_ours(args):
     def allreduce(x: float, op: str) -> float:
         return allreduce_value(x, op, dist)
 
-    # weak scaling: each rank its own genome pair of the same shape
-    w, transition, desc = make_workload(args, rank)
+    # one job over the ranks: the target replicated, the query in blocks
+    # (weak scaling) or slices (strong scaling), no data exchanged between ranks
+    w, transition, desc = make_workload(args, rank, world)
     sf = SeedFilter()
     sf.initialize_interface(1)
     sf.generate_shape_pos("12of19")
@@ -583,11 +606,14 @@ def run_ours(args):
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
         "dtype": "int32", "data": "synthetic",
         "config": {"workload": desc, "path": "batched: resident query text -> device seeding, lookup, X-drop, dedup "
                    "-> HSP lists on the host", "units": len(units), "target_bp": len(w.target),
-                   "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)", "scale": args.scale},
+                   "query_bp": len(w.query), "l2": "flushed between steps (512 MiB write)", "scale": args.scale,
+                   "parallelism": (f"{world} ranks, one job: target replicated, query "
+                                   f"{'blocks' if args.scaling == 'weak' else 'slices'} across ranks, "
+                                   "no collective on the data path" if world > 1 else "1 GPU")},
         "hsps_per_s": hsps_all / (ms_step_max / 1000.0),
         "extensions_per_step": hits_all, "hsps_per_step": hsps_all,
         "device_ms_per_step": tb["dev_ms"],

@@ -199,33 +199,19 @@ void add_repeats(Rng& r, std::vector<std::string*> seqs, double frac, double gc)
     }
 }
 
-// Plain method, genome scale: 100 Mbp target in 6 chromosomes (U[15,21] Mbp
-// rescaled) vs a 108 Mbp query, GC 36%.  ~60% of the query is target blocks of
-// U[1,50] kbp at U[15%,35%] divergence (5% of blocks inverted), the rest random;
-// 12% repeats; 8% soft-masking in runs of U[50,2000].
-Workload make_genome(uint64_t seed, double scale, uint64_t tlen_full, int nchr, uint64_t qlen_full,
-                     double gc, double rep_frac, double mask_frac, double hom_frac,
-                     double div_lo, double div_hi) {
-    Rng r(seed);
-    uint64_t TL = (uint64_t)(tlen_full * scale), QL = (uint64_t)(qlen_full * scale);
-    std::vector<double> w(nchr);
-    double ws = 0;
-    for (auto& x : w) { x = 15.0 + 6.0 * r.unit(); ws += x; }
-    Genome tg;
-    uint64_t acc = 0;
-    for (int i = 0; i < nchr; ++i) {
-        uint64_t l = (i + 1 == nchr) ? TL - acc : (uint64_t)(w[i] / ws * (double)TL);
-        acc += l;
-        tg.chroms.emplace_back(l, 'A');
-        random_bases(r, &tg.chroms.back()[0], l, gc);
-    }
+// A query of QL bases: pieces of U[1,50] kbp, each with probability hom_frac
+// a copy of a random stretch of a target chromosome at U[div_lo,div_hi]
+// divergence (5% reverse-complemented), else random bases.
+std::string draw_query(Rng& r, const std::vector<std::string>& chroms, uint64_t QL, double gc, double hom_frac,
+                       double div_lo, double div_hi) {
     std::string Q;
     Q.reserve(QL + 60000);
+    const int nchr = (int)chroms.size();
     while (Q.size() < QL) {
         uint64_t len = r.range(1000, 50000);
         if (r.unit() < hom_frac) {
             int c = (int)r.range(0, nchr - 1);
-            auto& ch = tg.chroms[c];
+            auto& ch = chroms[c];
             if (ch.size() <= len) continue;
             uint64_t src = r.range(0, ch.size() - len);
             std::string b = ch.substr(src, len);
@@ -239,11 +225,44 @@ Workload make_genome(uint64_t seed, double scale, uint64_t tlen_full, int nchr, 
         }
     }
     Q.resize(QL);
+    return Q;
+}
+
+// Plain method, genome scale: 100 Mbp target in 6 chromosomes (U[15,21] Mbp
+// rescaled) vs a 108 Mbp query, GC 36%.  ~60% of the query is target blocks of
+// U[1,50] kbp at U[15%,35%] divergence (5% of blocks inverted), the rest random;
+// 12% repeats; 8% soft-masking in runs of U[50,2000].
+// Query block b > 0 of the same job: the same final target (block 0's bytes),
+// and a query drawn the same way from that target with its own random stream,
+// soft-masked the same way (its repeats are the copies it draws from the
+// target; no repeat families are added to it).
+Workload make_genome(uint64_t seed, double scale, uint64_t tlen_full, int nchr, uint64_t qlen_full,
+                     double gc, double rep_frac, double mask_frac, double hom_frac,
+                     double div_lo, double div_hi, uint32_t block) {
+    Rng r(seed);
+    uint64_t TL = (uint64_t)(tlen_full * scale), QL = (uint64_t)(qlen_full * scale);
+    std::vector<double> w(nchr);
+    double ws = 0;
+    for (auto& x : w) { x = 15.0 + 6.0 * r.unit(); ws += x; }
+    Genome tg;
+    uint64_t acc = 0;
+    for (int i = 0; i < nchr; ++i) {
+        uint64_t l = (i + 1 == nchr) ? TL - acc : (uint64_t)(w[i] / ws * (double)TL);
+        acc += l;
+        tg.chroms.emplace_back(l, 'A');
+        random_bases(r, &tg.chroms.back()[0], l, gc);
+    }
+    std::string Q = draw_query(r, tg.chroms, QL, gc, hom_frac, div_lo, div_hi);
     std::vector<std::string*> all;
     for (auto& c : tg.chroms) all.push_back(&c);
     all.push_back(&Q);
     add_repeats(r, all, rep_frac, gc);
     for (auto* s : all) apply_runs(r, *s, mask_frac, 50, 2000, to_lower);
+    if (block > 0) {
+        Rng rb(seed * 0x9E3779B97F4A7C15ull + block);
+        Q = draw_query(rb, tg.chroms, QL, gc, hom_frac, div_lo, div_hi);
+        apply_runs(rb, Q, mask_frac, 50, 2000, to_lower);
+    }
     Workload wl;
     wl.target = join_block(tg.chroms, wl.tstart, wl.tlen);
     wl.query = join_block({Q}, wl.qstart, wl.qlen);
@@ -257,14 +276,19 @@ extern "C" {
 // config: 1 = plain small (1 Mbp x 1 Mbp), 2 = genome scale (100 x 108 Mbp,
 // 6 chromosomes), 4 = large (600 x 600 Mbp, 12 chromosomes, GC 41%, 45% repeats).
 // scale multiplies the sequence lengths (1.0 = the named sizes).
-void* synth_make(int config, uint64_t seed, double scale) {
+// block: query block of the job (0 = the workload's own query; b > 0 = another
+// query against the same target, genome configs only).
+void* synth_make_block(int config, uint64_t seed, double scale, uint32_t block) {
+    if (config == 1 && block > 0) return nullptr;
     Workload* w = new Workload();
     if (config == 1) *w = make_small(seed, scale, std::max(1, (int)(200 * std::min(1.0, scale))));
-    else if (config == 2) *w = make_genome(seed, scale, 100000000ull, 6, 108000000ull, 0.36, 0.12, 0.08, 0.60, 0.15, 0.35);
-    else if (config == 4) *w = make_genome(seed, scale, 600000000ull, 12, 600000000ull, 0.41, 0.45, 0.08, 0.60, 0.10, 0.30);
+    else if (config == 2) *w = make_genome(seed, scale, 100000000ull, 6, 108000000ull, 0.36, 0.12, 0.08, 0.60, 0.15, 0.35, block);
+    else if (config == 4) *w = make_genome(seed, scale, 600000000ull, 12, 600000000ull, 0.41, 0.45, 0.08, 0.60, 0.10, 0.30, block);
     else { delete w; return nullptr; }
     return w;
 }
+
+void* synth_make(int config, uint64_t seed, double scale) { return synth_make_block(config, seed, scale, 0); }
 
 uint64_t synth_len(void* h, int which) {
     Workload* w = (Workload*)h;

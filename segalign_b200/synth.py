@@ -26,6 +26,8 @@ def _load():
         lib = C.CDLL(SYNTH_PATH)
         lib.synth_make.restype = C.c_void_p
         lib.synth_make.argtypes = [C.c_int, C.c_uint64, C.c_double]
+        lib.synth_make_block.restype = C.c_void_p
+        lib.synth_make_block.argtypes = [C.c_int, C.c_uint64, C.c_double, C.c_uint32]
         lib.synth_len.restype = C.c_uint64
         lib.synth_len.argtypes = [C.c_void_p, C.c_int]
         lib.synth_copy.restype = None
@@ -49,12 +51,15 @@ class Workload:
         self.target, self.query, self.target_chr, self.query_chr = target, query, tchr, qchr
 
 
-def make(config: int, seed: int | None = None, scale: float = 1.0) -> Workload:
-    """config 1: 1 Mbp x 1 Mbp; 2: 100 Mbp (6 chr) x 108 Mbp; 4: 600 Mbp (12 chr) x 600 Mbp."""
+def make(config: int, seed: int | None = None, scale: float = 1.0, block: int = 0) -> Workload:
+    """config 1: 1 Mbp x 1 Mbp; 2: 100 Mbp (6 chr) x 108 Mbp; 4: 600 Mbp (12 chr) x 600 Mbp.
+
+    block > 0 (configs 2 and 4): the same target with another query block of the
+    same size, drawn from that target the same way (one job's query in blocks)."""
     lib = _load()
-    h = lib.synth_make(config, DEFAULT_SEEDS.get(config, 1) if seed is None else seed, scale)
+    h = lib.synth_make_block(config, DEFAULT_SEEDS.get(config, 1) if seed is None else seed, scale, block)
     if not h:
-        raise ValueError(f"unknown workload config {config}")
+        raise ValueError(f"unknown workload config {config} (block {block})")
     try:
         out = []
         chrs = []
