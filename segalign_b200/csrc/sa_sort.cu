@@ -294,15 +294,19 @@ static void sa_uniq(SaWork& w, SaUniqArgs u, const unsigned long long* d_n, cons
     sa_note_launch();
 }
 
-static SaSortSpec spec_of(std::initializer_list<std::pair<uint8_t, uint8_t>> fields_lsd_first) {
-    // each entry: (field, inverted); expanded to 4 byte digits, least significant first
+struct SaSortField {
+    uint8_t field, inv, bytes;  // bytes: low-order byte digits that can vary (the rest are zero)
+};
+
+static SaSortSpec spec_of(std::initializer_list<SaSortField> fields_lsd_first) {
+    // each field expands to its byte digits, least significant first
     SaSortSpec sp{};
     int n = 0;
     for (auto& f : fields_lsd_first)
-        for (int byte = 0; byte < 4; ++byte) {
-            sp.field[n] = f.first;
+        for (int byte = 0; byte < f.bytes; ++byte) {
+            sp.field[n] = f.field;
             sp.byte[n] = (uint8_t)byte;
-            sp.inv[n] = f.second;
+            sp.inv[n] = f.inv;
             ++n;
         }
     sp.npass = n;
@@ -321,8 +325,14 @@ void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s
     sa_note_launch();
     cudaMemsetAsync(w.scope_count, 0, sizeof(uint32_t) * SA_MAX_SCOPES, s);
 
+    // Scopes are MAX_HITS iterations (< SA_MAX_ITERS = 256: one byte) in a
+    // call, (unit << 4) | iteration (< SA_MAX_UNITS << 4 = 2^20: three bytes)
+    // in a batch; their high digits are never sorted on.  Every digit pass
+    // costs three launches even when the device plan skips it.
+    static_assert(SA_MAX_ITERS <= 256 && SA_MAX_UNITS <= (1 << 20), "scope digit counts");
+    const uint8_t sb = scope_shift ? 3 : 1;
     // hspComp order: (scope, query_start asc, len desc, ref_start asc).
-    const SaSortSpec plain = spec_of({{F_RS, 0}, {F_LEN, 1}, {F_QS, 0}, {F_SCOPE, 0}});
+    const SaSortSpec plain = spec_of({{F_RS, 0, 4}, {F_LEN, 1, 4}, {F_QS, 0, 4}, {F_SCOPE, 0, sb}});
     sa_radix_sort_recs(w, plain, n0, st, G, s);
     SaUniqArgs u{};
     u.rec[0] = w.rec[0];
@@ -345,14 +355,14 @@ void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s
     sa_k_flip_cur<<<1, 1, 0, s>>>(st, plain.npass);
     sa_note_launch();
     // hspDiagComp: (scope, diag asc, ref_start asc, score desc), stable
-    const SaSortSpec diag = spec_of({{F_SCORE, 1}, {F_RS, 0}, {F_DIAG, 0}, {F_SCOPE, 0}});
+    const SaSortSpec diag = spec_of({{F_SCORE, 1, 4}, {F_RS, 0, 4}, {F_DIAG, 0, 4}, {F_SCOPE, 0, sb}});
     sa_radix_sort_recs(w, diag, n1, st, G, s);
     u.mode = 1;
     sa_uniq(w, u, n1, st + 1 + diag.npass, n2, G, s);
     sa_k_flip_cur<<<1, 1, 0, s>>>(st, diag.npass);
     sa_note_launch();
     // hspFinalComp: (scope, query_start asc, score desc, ref_start desc), stable
-    const SaSortSpec fin = spec_of({{F_RS, 1}, {F_SCORE, 1}, {F_QS, 0}, {F_SCOPE, 0}});
+    const SaSortSpec fin = spec_of({{F_RS, 1, 4}, {F_SCORE, 1, 4}, {F_QS, 0, 4}, {F_SCOPE, 0, sb}});
     sa_radix_sort_recs(w, fin, n2, st, G, s);
     u.mode = 2;
     u.out_rec = w.out;
