@@ -114,6 +114,7 @@ struct Slot {
     SaRec* h_out = nullptr;
     uint64_t h_out_cap = 0;
     cudaEvent_t ev[6] = {};
+    cudaEvent_t part_ev[4] = {};  // batched output copied back in parts (created on first use)
     // CUDA graph of the per-call device chain (run_chain), valid for graph_key
     cudaGraphExec_t graph = nullptr;
     uint64_t graph_key = 0;
@@ -291,6 +292,8 @@ void free_slot(Slot* s) {
     if (s->h_scope_count) cudaFreeHost(s->h_scope_count);
     if (s->h_out) cudaFreeHost(s->h_out);
     for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : s->part_ev)
         if (e) cudaEventDestroy(e);
     delete s;
 }
@@ -777,11 +780,57 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
         SA_CUDA_OK(cudaMallocHost(&s->h_out, cap * sizeof(SaRec)));
         s->h_out_cap = cap;
     }
-    if (want_out && nh) SA_CUDA_OK(cudaMemcpyAsync(s->h_out, w.out, nh * sizeof(SaRec), cudaMemcpyDeviceToHost, st));
+    // A large output for a sink comes back in parts of whole units; the sink
+    // copies part k while part k + 1 is in flight.
+    constexpr int kParts = 4;
+    const bool parts = want_out && res.sink && nh >= (1u << 20);
+    if (parts) {
+        SA_CUDA_OK(cudaStreamSynchronize(st));  // the per-unit counts split the records
+        for (auto& e : s->part_ev)
+            if (!e) SA_CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    uint32_t part_u[kParts + 1] = {0};
+    uint64_t part_r[kParts + 1] = {0};
+    if (parts) {
+        uint32_t u = 0;
+        uint64_t r = 0;
+        for (int k = 0; k < kParts; ++k) {
+            const uint64_t goal = nh * (uint64_t)(k + 1) / kParts;
+            while (u < n && (r < goal || k + 1 == kParts)) r += cnt[u++];
+            part_u[k + 1] = u;
+            part_r[k + 1] = r;
+            if (r > part_r[k])
+                SA_CUDA_OK(cudaMemcpyAsync(s->h_out + part_r[k], w.out + part_r[k], (r - part_r[k]) * sizeof(SaRec),
+                                           cudaMemcpyDeviceToHost, st));
+            SA_CUDA_OK(cudaEventRecord(s->part_ev[k], st));
+        }
+    } else if (want_out && nh) {
+        SA_CUDA_OK(cudaMemcpyAsync(s->h_out, w.out, nh * sizeof(SaRec), cudaMemcpyDeviceToHost, st));
+    }
     tm.mark(5);
+    for (uint32_t i = 0; i < n; ++i) res.hits[u0 + i] = he[i] - hb[i];
+    if (parts) {
+        if (const int r = res.sink->expect(nh); r != SA_OK) {
+            cudaStreamSynchronize(st);
+            return r;
+        }
+        for (int k = 0; k < kParts; ++k) {
+            SA_CUDA_OK(cudaEventSynchronize(s->part_ev[k]));
+            const uint32_t a = part_u[k], b = part_u[k + 1];
+            const int r = b > a ? res.sink->put(u0 + a, b - a, s->h_out + part_r[k], cnt.data() + a,
+                                                 res.hits.data() + u0 + a)
+                                : SA_OK;
+            if (r != SA_OK) {
+                cudaStreamSynchronize(st);  // no copy into h_out outlives the call
+                return r;
+            }
+        }
+        SA_CUDA_OK(cudaStreamSynchronize(st));
+        tm.collect(res.timing);
+        return SA_OK;
+    }
     SA_CUDA_OK(cudaStreamSynchronize(st));
     tm.collect(res.timing);
-    for (uint32_t i = 0; i < n; ++i) res.hits[u0 + i] = he[i] - hb[i];
     if (want_out && res.sink) return res.sink->put(u0, n, s->h_out, cnt.data(), res.hits.data() + u0);
     uint64_t at = 0;
     for (uint32_t i = 0; i < n; ++i) {
@@ -1195,6 +1244,8 @@ struct SegmentWriter : SaBatchSink {
         o[at++] = sa_segment{0, 0, nb, (int32_t)(uint32_t)hits};
     }
 
+    int expect(uint64_t records) override { return reserve(at + records + (n_units - next) + 1); }
+
     int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) override {
         if (!n) return SA_OK;
         uint64_t body = 0;
@@ -1217,7 +1268,7 @@ struct SegmentWriter : SaBatchSink {
             for (uint32_t i = a; i < b; ++i)
                 if (cnt[i]) std::memcpy(o + dst[i], recs + src[i], cnt[i] * sizeof(sa_segment));
         };
-        const uint64_t kPer = 2u << 20;  // records per thread, at least
+        const uint64_t kPer = 1u << 19;  // records per thread, at least
         const uint32_t nt = (uint32_t)std::min<uint64_t>({8, n, body / kPer});
         if (nt < 2) {
             copy(0, n);

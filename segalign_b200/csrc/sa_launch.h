@@ -52,9 +52,12 @@ inline uint64_t sa_unit_slots(const SaResolvedUnit& u, uint64_t S) {
 // Receives the output of one completed device group of a batched run:
 // units [u0, u0 + n) of the run's non-empty units, in order, their HSP
 // records back to back in recs (cnt[i] each) and their hit counts.  Groups
-// arrive in unit order.  recs is valid only during the call.
+// arrive in unit order, a group possibly in several consecutive parts.  recs
+// is valid only during the call.  expect() announces the records of the
+// parts that follow (so that a sink can size its storage once).
 struct SaBatchSink {
     virtual ~SaBatchSink() = default;
+    virtual int expect(uint64_t records) { (void)records; return 0; }
     virtual int put(uint32_t u0, uint32_t n, const SaRec* recs, const uint32_t* cnt, const uint64_t* hits) = 0;
 };
 
