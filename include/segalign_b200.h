@@ -226,9 +226,10 @@ int sa_serve_stop(void);
 
 /* ---- results, configuration, diagnostics (no reference counterpart) ---- */
 
-/* Releases an array the library returned.  The largest batched output freed
- * (64 MiB or more) is kept for the next batched call's output, which then
- * skips the page faults of a fresh allocation; sa_shutdown_processor() frees it. */
+/* Releases an array the library returned.  The two largest batched outputs
+ * freed (64 MiB or more each) are kept for the next batched calls' outputs,
+ * which then skip the page faults of a fresh allocation (a caller may hold one
+ * call's lists while the next call runs); sa_shutdown_processor() frees them. */
 void sa_free_segments(sa_segment* segments);
 
 /* MAX_HITS override (src/seed_filter.cu:18,784-791); 0 restores the default. */

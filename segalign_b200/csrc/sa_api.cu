@@ -1119,16 +1119,18 @@ int seed_and_filter_coalesced(const uint64_t* seeds, uint32_t num_seeds, int rev
 // header record {0, 0, HSP count, hit count} then its HSPs; a unit with an
 // empty window gets its header only.  One malloc'd block (grown by realloc,
 // which remaps rather than copies at these sizes), freed by sa_free_segments.
-// Batched outputs of at least kKeepBytes are remembered, and the last one the
-// caller frees is kept for the next batched output that fits: a fresh array of
-// hundreds of MB pays a page fault per 4 KiB page at its first write.
+// Batched outputs of at least kKeepBytes are remembered, and the two largest
+// the caller has freed are kept for the next batched outputs that fit: a fresh
+// array of hundreds of MB pays a page fault per 4 KiB page at its first write.
 constexpr uint64_t kKeepBytes = 64ull << 20;
 struct OutKeep {
     std::mutex mu;
     std::vector<std::pair<void*, uint64_t>> live;  // batched outputs handed out (pointer, bytes)
-    void* kept = nullptr;
-    uint64_t kept_bytes = 0;
+    std::vector<std::pair<void*, uint64_t>> kept;  // freed ones kept for reuse (at most kKeepArrays)
 };
+// Two: a caller that holds one call's lists while the next call runs (a
+// steady loop over batches) then never allocates.
+constexpr size_t kKeepArrays = 2;
 OutKeep& out_keep() {
     static OutKeep k;
     return k;
@@ -1139,11 +1141,13 @@ void* out_alloc(uint64_t bytes, uint64_t* got) {
     OutKeep& k = out_keep();
     std::lock_guard<std::mutex> lk(k.mu);
     void* p = nullptr;
-    if (k.kept && k.kept_bytes >= bytes) {
-        p = k.kept;
-        *got = k.kept_bytes;
-        k.kept = nullptr;
-        k.kept_bytes = 0;
+    size_t best = k.kept.size();
+    for (size_t i = 0; i < k.kept.size(); ++i)  // the smallest kept array that fits
+        if (k.kept[i].second >= bytes && (best == k.kept.size() || k.kept[i].second < k.kept[best].second)) best = i;
+    if (best < k.kept.size()) {
+        p = k.kept[best].first;
+        *got = k.kept[best].second;
+        k.kept.erase(k.kept.begin() + (std::ptrdiff_t)best);
     } else {
         p = malloc(bytes);
         *got = bytes;
@@ -1167,14 +1171,14 @@ bool out_release(void* p) {
     std::lock_guard<std::mutex> lk(k.mu);
     for (size_t i = 0; i < k.live.size(); ++i)
         if (k.live[i].first == p) {
-            const uint64_t b = k.live[i].second;
+            k.kept.push_back(k.live[i]);
             k.live.erase(k.live.begin() + (std::ptrdiff_t)i);
-            if (b > k.kept_bytes) {
-                free(k.kept);
-                k.kept = p;
-                k.kept_bytes = b;
-            } else {
-                free(p);
+            if (k.kept.size() > kKeepArrays) {  // free the smallest
+                size_t s = 0;
+                for (size_t j = 1; j < k.kept.size(); ++j)
+                    if (k.kept[j].second < k.kept[s].second) s = j;
+                free(k.kept[s].first);
+                k.kept.erase(k.kept.begin() + (std::ptrdiff_t)s);
             }
             return true;
         }
@@ -1184,9 +1188,8 @@ bool out_release(void* p) {
 void out_drop_kept() {
     OutKeep& k = out_keep();
     std::lock_guard<std::mutex> lk(k.mu);
-    free(k.kept);
-    k.kept = nullptr;
-    k.kept_bytes = 0;
+    for (auto& e : k.kept) free(e.first);
+    k.kept.clear();
 }
 
 struct SegmentWriter : SaBatchSink {
