@@ -782,8 +782,10 @@ int run_batch_group(DevState& d, Slot* s, const SaResolvedUnit* units, uint32_t 
     }
     // A large output for a sink comes back in parts of whole units; the sink
     // copies part k while part k + 1 is in flight.
+    // (SA_OUT_PARTS_MIN: the smallest output, in records, copied in parts)
     constexpr int kParts = 4;
-    const bool parts = want_out && res.sink && nh >= (1u << 20);
+    static const uint64_t parts_min = env_u64("SA_OUT_PARTS_MIN", 1ull << 20);
+    const bool parts = want_out && res.sink && nh >= std::max<uint64_t>(parts_min, 1);
     if (parts) {
         SA_CUDA_OK(cudaStreamSynchronize(st));  // the per-unit counts split the records
         for (auto& e : s->part_ev)
