@@ -275,9 +275,16 @@ struct SaKvOps {
     static __device__ __forceinline__ uint32_t digit(const Ctx& c, int buf, uint64_t i, int pass) {
         return (c.k[buf][i] >> (8 * pass)) & 0xffu;
     }
-    static __device__ __forceinline__ void move(const Ctx& c, int buf, uint64_t i, uint32_t dst) {
-        c.k[buf ^ 1][dst] = c.k[buf][i];
-        c.v[buf ^ 1][dst] = c.v[buf][i];
+    struct Item {
+        uint32_t k, v;
+    };
+    static __device__ __forceinline__ Item load(const Ctx& c, int buf, uint64_t i) { return {c.k[buf][i], c.v[buf][i]}; }
+    static __device__ __forceinline__ uint32_t digit_of(const Ctx&, const Item& x, int pass) {
+        return (x.k >> (8 * pass)) & 0xffu;
+    }
+    static __device__ __forceinline__ void store(const Ctx& c, int buf, const Item& x, uint32_t dst) {
+        c.k[buf ^ 1][dst] = x.k;
+        c.v[buf ^ 1][dst] = x.v;
     }
 };
 

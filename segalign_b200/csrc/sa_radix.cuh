@@ -93,9 +93,11 @@ struct SaRadixCtl {
 };
 
 // Ops must provide:
-//   struct Ctx;
+//   struct Ctx;  struct Item;  (one item: its key and payload)
 //   static __device__ uint32_t digit(const Ctx&, int buf, uint64_t i, int pass);
-//   static __device__ void move(const Ctx&, int buf, uint64_t i, uint32_t dst);
+//   static __device__ Item load(const Ctx&, int buf, uint64_t i);
+//   static __device__ uint32_t digit_of(const Ctx&, const Item&, int pass);
+//   static __device__ void store(const Ctx&, int buf, const Item&, uint32_t dst);  (into buffer buf ^ 1)
 template <class Ops>
 __global__ void __launch_bounds__(SA_RADIX_BLOCK)
 sa_k_radix_up(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, unsigned int* hist) {
@@ -133,10 +135,15 @@ sa_k_radix_down(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, const unsigned 
     uint64_t a, b;
     sa_radix_range(n, A, a, b);
     const uint32_t lt = sa_lanemask_lt();
+    // Items are loaded one round ahead, so that the load of round r + 1
+    // overlaps the ranking and scatter of round r.
+    typename Ops::Item cur{}, nxt{};
+    if (a + t < b) cur = Ops::load(ctx, buf, a + t);
     for (uint64_t base = a; base < b; base += SA_RADIX_BLOCK) {
         const uint64_t i = base + t;
         const bool valid = i < b;
-        const uint32_t d = valid ? Ops::digit(ctx, buf, i, pass) : 256u;
+        if (i + SA_RADIX_BLOCK < b) nxt = Ops::load(ctx, buf, i + SA_RADIX_BLOCK);
+        const uint32_t d = valid ? Ops::digit_of(ctx, cur, pass) : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t rank = __popc(peers & lt);
         if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
@@ -150,7 +157,8 @@ sa_k_radix_down(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, const unsigned 
         }
         offs[t] = run;
         __syncthreads();
-        if (valid) Ops::move(ctx, buf, i, wcnt[warp][d] + rank);
+        if (valid) Ops::store(ctx, buf, cur, wcnt[warp][d] + rank);
+        cur = nxt;
         __syncthreads();
 #pragma unroll
         for (int w = 0; w < SA_RADIX_BLOCK / 32; ++w) wcnt[w][t] = 0;

@@ -54,9 +54,21 @@ struct SaRecOps {
         if (c.spec.inv[pass]) v = ~v;
         return (v >> (8 * c.spec.byte[pass])) & 0xffu;
     }
-    static __device__ __forceinline__ void move(const Ctx& c, int buf, uint64_t i, uint32_t dst) {
-        c.rec[buf ^ 1][dst] = c.rec[buf][i];
-        c.scope[buf ^ 1][dst] = c.scope[buf][i];
+    struct Item {
+        SaRec r;
+        uint32_t scope;
+    };
+    static __device__ __forceinline__ Item load(const Ctx& c, int buf, uint64_t i) {
+        return {c.rec[buf][i], c.scope[buf][i]};
+    }
+    static __device__ __forceinline__ uint32_t digit_of(const Ctx& c, const Item& x, int pass) {
+        uint32_t v = field_value(x.r, x.scope, c.spec.field[pass]);
+        if (c.spec.inv[pass]) v = ~v;
+        return (v >> (8 * c.spec.byte[pass])) & 0xffu;
+    }
+    static __device__ __forceinline__ void store(const Ctx& c, int buf, const Item& x, uint32_t dst) {
+        c.rec[buf ^ 1][dst] = x.r;
+        c.scope[buf ^ 1][dst] = x.scope;
     }
 };
 
