@@ -398,9 +398,9 @@ def allreduce_value(x: float, op: str, dist=None, device: str = "cuda") -> float
 
 
 def job_figures(ms_step: float, hits: float, hsps: float, dist=None, device: str = "cuda") -> dict:
-    """Whole-job figures of a weak-scaled step: every rank runs its own
-    workload, so the step lasts as long as the slowest rank and the work of
-    all ranks adds up."""
+    """Whole-job figures of a step: every rank runs its share of the job, so
+    the step lasts as long as the slowest rank and the work of all ranks adds
+    up."""
     ms = allreduce_value(ms_step, "max", dist, device)
     h = allreduce_value(hits, "sum", dist, device)
     hs = allreduce_value(hsps, "sum", dist, device)
