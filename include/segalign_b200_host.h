@@ -124,6 +124,14 @@ int sa_format_segments(const sa_chrom_table* ref, uint64_t ref_block_start, cons
                        const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len, char** minus_text,
                        uint64_t* minus_len);
 
+/* The same writer on the current GPU: the same arguments and the same text,
+ * byte for byte (one line per HSP formatted by its own thread).  Returns
+ * SA_ERR_CUDA when the device work fails. */
+int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                           uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
+                           const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len,
+                           char** minus_text, uint64_t* minus_len);
+
 /* Interval writer of the repeat masker, repeat_masker_src/segment_printer.cpp:24-62:
  * "chr start end" per run (start 0-based, end = start + len + 1 as the
  * reference prints it), and an end-of-file marker line when markend. */

@@ -51,7 +51,7 @@ EXPORTS = [
     "sa_set_tuning_param", "sa_get_tuning_param",
     "sa_serve_start", "sa_serve_submit", "sa_serve_wait", "sa_serve_stop", "sa_autotune", "sa_get_timing",
     "sa_rm_seeder_run", "sa_free_rm_runs", "sa_format_segments", "sa_format_rm_intervals", "sa_free_text",
-    "sa_fasta_load", "sa_seq_set_free", "sa_align_fasta", "sa_refresh_query_keys",
+    "sa_fasta_load", "sa_seq_set_free", "sa_align_fasta", "sa_refresh_query_keys", "sa_format_segments_gpu",
 ]
 
 
@@ -231,6 +231,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                            _P(RmSeederStats)]),
             "sa_free_rm_runs": (None, [_P(C.c_uint8)]),
             "sa_format_segments": (C.c_int, [_P(ChromTable), C.c_uint64, _P(ChromTable), C.c_uint64, C.c_uint32,
+                                             _P(C.c_uint8), C.c_uint64, _P(C.c_uint8), C.c_uint64,
+                                             _P(C.c_void_p), u64p, _P(C.c_void_p), u64p]),
+            "sa_format_segments_gpu": (C.c_int, [_P(ChromTable), C.c_uint64, _P(ChromTable), C.c_uint64, C.c_uint32,
                                              _P(C.c_uint8), C.c_uint64, _P(C.c_uint8), C.c_uint64,
                                              _P(C.c_void_p), u64p, _P(C.c_void_p), u64p]),
             "sa_format_rm_intervals": (C.c_int, [_P(ChromTable), C.c_uint64, _P(C.c_uint8), C.c_uint64, C.c_int,
@@ -568,19 +571,21 @@ def _take_text(lib, ptr: C.c_void_p, n: int) -> str:
 
 
 def format_segments(ref_chroms, ref_block_start: int, query_chroms, query_block_start: int, query_block_len: int,
-                    fw: np.ndarray, rc: np.ndarray):
-    """lastz --segments lines of one interval's HSP lists (sa_format_segments):
-    (plus-strand text, minus-strand text).  Chromosome tables are
-    [(name, global start, length), ...]."""
+                    fw: np.ndarray, rc: np.ndarray, gpu: bool = False):
+    """lastz --segments lines of one interval's HSP lists (sa_format_segments,
+    or sa_format_segments_gpu with gpu=True; the same text): (plus-strand
+    text, minus-strand text).  Chromosome tables are [(name, global start,
+    length), ...]."""
     lib = load_library()
     rt, keep1 = _chrom_table(ref_chroms)
     qt, keep2 = _chrom_table(query_chroms)
     f = np.ascontiguousarray(fw, dtype=SEGMENT_DTYPE)
     r = np.ascontiguousarray(rc, dtype=SEGMENT_DTYPE)
     pt, pl, mt, ml = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_uint64()
-    st = lib.sa_format_segments(C.byref(rt), ref_block_start, C.byref(qt), query_block_start, query_block_len,
-                                f.ctypes.data_as(_P(C.c_uint8)), len(f), r.ctypes.data_as(_P(C.c_uint8)), len(r),
-                                C.byref(pt), C.byref(pl), C.byref(mt), C.byref(ml))
+    fn = lib.sa_format_segments_gpu if gpu else lib.sa_format_segments
+    st = fn(C.byref(rt), ref_block_start, C.byref(qt), query_block_start, query_block_len,
+            f.ctypes.data_as(_P(C.c_uint8)), len(f), r.ctypes.data_as(_P(C.c_uint8)), len(r),
+            C.byref(pt), C.byref(pl), C.byref(mt), C.byref(ml))
     if st != 0:
         raise SegAlignError(st, "format_segments", "")
     return _take_text(lib, pt, pl.value), _take_text(lib, mt, ml.value)

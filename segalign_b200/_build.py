@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libsegalign_b200.so")
 SYNTH = os.path.join(HERE, "libsa_synth.so")
 
 CU_SOURCES = ["sa_pack.cu", "sa_lookup.cu", "sa_extend.cu", "sa_sort.cu", "sa_api.cu", "sa_host.cpp", "sa_noalloc.cu", "sa_serve.cu", "sa_tune.cu",
-              "sa_ingest.cpp", "sa_coverage.cu"]
+              "sa_ingest.cpp", "sa_coverage.cu", "sa_segwrite.cu"]
 HEADERS = ["sa_internal.cuh", "sa_launch.h", "sa_radix.cuh", "sa_host_internal.h", "sa_slot_pool.h"]
 
 NVCC_FLAGS = [

@@ -371,8 +371,8 @@ int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
                         if (seg && (fw.size() || rc.size())) {
                             char *pt = nullptr, *mt = nullptr;
                             uint64_t pl = 0, ml = 0;
-                            int f = sa_format_segments(&ttab, rstart, &qtab, qs, ql, fw.data(), fw.size(), rc.data(),
-                                                       rc.size(), &pt, &pl, &mt, &ml);
+                            int f = sa_format_segments_gpu(&ttab, rstart, &qtab, qs, ql, fw.data(), fw.size(),
+                                                           rc.data(), rc.size(), &pt, &pl, &mt, &ml);
                             if (f == SA_OK) {
                                 fwrite(pt, 1, pl, seg);
                                 fwrite(mt, 1, ml, seg);
