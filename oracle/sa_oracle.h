@@ -7,13 +7,16 @@
  * --impl reference leg, always as the checker or the timed CPU baseline,
  * never as the product path.
  *
- * Pinning: the seeding half (character coding, shape parsing, k-mer keys,
- * host reverse complement) is pinned against the reference's own
- * common/ntcoding.cpp compiled from its source (oracle/build_ref.sh ->
- * oracle/_ref/).  The extension / compaction / dedup half is pinned only by
- * the reference source semantics: the reference ships no tests or golden
- * vectors, and its kernel translation units need TBB headers to compile, so
- * that half is "parity unpinned" in the strict sense.
+ * Pinning: the reference ships no tests or golden vectors, so both halves are
+ * pinned against the reference's own code, compiled from its sources where
+ * they lie (oracle/Makefile, outputs in oracle/_ref/).  The seeding half
+ * (character coding, shape parsing, k-mer keys, host reverse complement) is
+ * checked against its common/ntcoding.cpp ("make ref").  The table /
+ * extension / compaction / dedup half is checked against its SeedAndFilter
+ * (src/seed_filter.cu, repeat_masker_src/seed_filter.cu and the interface
+ * files, built for sm_100a with "make ref_kernels" and driven by
+ * ref_harness.cu): live on a GPU, and through the reference outputs recorded
+ * in tests/golden/ref_calls.npz on the CPU.
  */
 #pragma once
 #include <stdint.h>

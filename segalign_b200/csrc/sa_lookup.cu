@@ -160,15 +160,13 @@ struct SaSlotInfo {
     uint32_t unit, j, lo, cnt;
 };
 
-// Slot s of batch unit u: its query position, bucket start and hit count.
+// Slot s of batch unit B: its query position, bucket start and hit count.
 // An explicit word whose key is outside the table sets bad_key (a plain call
 // reports it as SA_ERR_BAD_SEED, src/seed_filter.cu:129-154 reads past the
 // table there); a device-seeded slot never has such a key.
-__device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu, uint32_t u, uint64_t s,
-                                              const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
-                                              bool& bad_key) {
+__device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit& B, uint64_t s, const uint32_t* __restrict__ index,
+                                              uint32_t nbuckets, int S, bool& bad_key) {
     SaSlotInfo r;
-    const SaBatchUnit B = bu[u];
     const uint64_t off = s - B.slot_begin;
     r.unit = B.unit;
     uint32_t key;
@@ -199,19 +197,35 @@ __device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit* __restrict__ bu
     return r;
 }
 
+// The unit holding slot s, kept per thread: a thread's slots only increase,
+// so the binary search runs only when s passes the current unit's end.
+struct SaUnitCursor {
+    uint32_t u = 0;
+    uint64_t end = 0;  // one past the unit's last slot (0: not located yet)
+    SaBatchUnit B{};
+    __device__ __forceinline__ void seek(const SaBatchUnit* __restrict__ bu, uint32_t nu, uint64_t n, uint64_t s) {
+        if (s < end) return;
+        u = sa_find_unit(bu, nu, s);
+        B = bu[u];
+        end = (u + 1 < nu) ? bu[u + 1].slot_begin : n;
+    }
+};
+
 __global__ void __launch_bounds__(256)
 sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc,
                    const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
                    uint32_t* __restrict__ s_lo, uint32_t* __restrict__ s_cnt, unsigned long long* cta_a,
                    unsigned long long* cta_b, SaCounters* ctr) {
+    const uint64_t n = desc->num_seeds;
     uint64_t a, b;
-    sa_cta_range(desc->num_seeds, a, b);
+    sa_cta_range(n, a, b);
     const uint32_t nu = desc->num_units;
     unsigned long long hits = 0, nz = 0;
     bool bad_key = false;
+    SaUnitCursor cur;
     for (uint64_t s = a + threadIdx.x; s < b; s += 256) {
-        const uint32_t u = sa_find_unit(bu, nu, s);
-        const SaSlotInfo si = sa_slot(bu, u, s, index, nbuckets, S, bad_key);
+        cur.seek(bu, nu, n, s);
+        const SaSlotInfo si = sa_slot(cur.B, s, index, nbuckets, S, bad_key);
         s_lo[s] = si.lo;
         s_cnt[s] = si.cnt;
         hits += si.cnt;
@@ -227,43 +241,59 @@ sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restr
 }
 
 // Compaction of hit-bearing slots; also records each unit's hit range
-// [unit_hit_base, unit_hit_end) in the global hit prefix.
+// [unit_hit_base, unit_hit_end) in the global hit prefix.  A round covers
+// 256 x SA_EMIT_ITEMS consecutive slots, SA_EMIT_ITEMS per thread, with one
+// block scan of the packed (hits << 16 | hit-bearing slots) per round (a
+// round has at most 2^12 hit-bearing slots, so the low field never carries).
+#define SA_EMIT_ITEMS 4
 __global__ void __launch_bounds__(256)
 sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc, int S,
                   const uint32_t* __restrict__ s_lo, const uint32_t* __restrict__ s_cnt, SaSeedList cs,
                   const unsigned long long* cta_a, const unsigned long long* cta_b, unsigned long long* unit_hit_base,
                   unsigned long long* unit_hit_end, SaCounters* ctr) {
+    static_assert(256 * SA_EMIT_ITEMS < (1 << 16), "packed scan field");
     const uint64_t n = desc->num_seeds;
     const uint32_t nu = desc->num_units;
     uint64_t a, b;
     sa_cta_range(n, a, b);
     unsigned long long hbase = cta_a[blockIdx.x], cbase = cta_b[blockIdx.x];
     __shared__ unsigned long long ws[9];
-    for (uint64_t r = a; r < b; r += 256) {
-        const uint64_t s = r + threadIdx.x;
-        const uint32_t cnt = s < b ? s_cnt[s] : 0u;
-        unsigned long long th, tc;
-        const unsigned long long eh = sa_block_excl_sum<unsigned long long, 256>(cnt, ws, &th);
-        const unsigned long long ec = sa_block_excl_sum<unsigned long long, 256>(cnt != 0, ws, &tc);
-        if (s < b) {
-            const uint32_t u = sa_find_unit(bu, nu, s);
-            const SaBatchUnit B = bu[u];
-            const uint64_t end = (u + 1 < nu) ? bu[u + 1].slot_begin : n;
-            if (s == B.slot_begin) unit_hit_base[u] = hbase + eh;
-            if (s + 1 == end) unit_hit_end[u] = hbase + eh + cnt;
-            if (cnt) {
-                const uint64_t c = cbase + ec;
-                cs.E[c] = hbase + eh;
-                cs.lo[c] = s_lo[s];
-                cs.qpos[c] = B.seeds ? (uint32_t)__ldg(reinterpret_cast<const unsigned long long*>(B.seeds) +
-                                                       B.q_start + (s - B.slot_begin))
-                                     : B.q_start + (uint32_t)((s - B.slot_begin) / S);
-                cs.unit[c] = B.unit;
-                cs.scope[c] = u;  // batch unit index; turned into (unit, iteration) by sa_k_bscope
+    SaUnitCursor cur;
+    for (uint64_t r = a; r < b; r += 256 * SA_EMIT_ITEMS) {
+        const uint64_t s0 = r + (uint64_t)threadIdx.x * SA_EMIT_ITEMS;
+        uint32_t cnt[SA_EMIT_ITEMS];
+        unsigned long long mine = 0;
+#pragma unroll
+        for (int k = 0; k < SA_EMIT_ITEMS; ++k) {
+            cnt[k] = s0 + k < b ? s_cnt[s0 + k] : 0u;
+            mine += ((unsigned long long)cnt[k] << 16) | (cnt[k] != 0);
+        }
+        unsigned long long tot;
+        const unsigned long long e = sa_block_excl_sum<unsigned long long, 256>(mine, ws, &tot);
+        unsigned long long eh = hbase + (e >> 16), ec = cbase + (e & 0xffffu);
+#pragma unroll
+        for (int k = 0; k < SA_EMIT_ITEMS; ++k) {
+            const uint64_t s = s0 + k;
+            if (s < b) {
+                cur.seek(bu, nu, n, s);
+                const SaBatchUnit& B = cur.B;
+                if (s == B.slot_begin) unit_hit_base[cur.u] = eh;
+                if (s + 1 == cur.end) unit_hit_end[cur.u] = eh + cnt[k];
+                if (cnt[k]) {
+                    cs.E[ec] = eh;
+                    cs.lo[ec] = s_lo[s];
+                    cs.qpos[ec] = B.seeds ? (uint32_t)__ldg(reinterpret_cast<const unsigned long long*>(B.seeds) +
+                                                            B.q_start + (s - B.slot_begin))
+                                          : B.q_start + (uint32_t)((s - B.slot_begin) / S);
+                    cs.unit[ec] = B.unit;
+                    cs.scope[ec] = cur.u;  // batch unit index; turned into (unit, iteration) by sa_k_bscope
+                    ++ec;
+                }
+                eh += cnt[k];
             }
         }
-        hbase += th;
-        cbase += tc;
+        hbase += tot >> 16;
+        cbase += tot & 0xffffu;
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) cs.E[ctr->nnz] = ctr->num_hits;
 }

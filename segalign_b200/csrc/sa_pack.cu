@@ -272,16 +272,15 @@ struct SaKvOps {
         uint32_t* k[2];
         uint32_t* v[2];
     };
-    static __device__ __forceinline__ uint32_t digit(const Ctx& c, int buf, uint64_t i, int pass) {
-        return (c.k[buf][i] >> (8 * pass)) & 0xffu;
-    }
+    struct Pass {
+        uint32_t shift;
+    };
+    static __device__ __forceinline__ Pass pass_of(const Ctx&, int pass) { return {8u * (uint32_t)pass}; }
     struct Item {
         uint32_t k, v;
     };
     static __device__ __forceinline__ Item load(const Ctx& c, int buf, uint64_t i) { return {c.k[buf][i], c.v[buf][i]}; }
-    static __device__ __forceinline__ uint32_t digit_of(const Ctx&, const Item& x, int pass) {
-        return (x.k >> (8 * pass)) & 0xffu;
-    }
+    static __device__ __forceinline__ uint32_t digit_of(const Pass& p, const Item& x) { return (x.k >> p.shift) & 0xffu; }
     static __device__ __forceinline__ void store(const Ctx& c, int buf, const Item& x, uint32_t dst) {
         c.k[buf ^ 1][dst] = x.k;
         c.v[buf ^ 1][dst] = x.v;

@@ -94,9 +94,10 @@ struct SaRadixCtl {
 
 // Ops must provide:
 //   struct Ctx;  struct Item;  (one item: its key and payload)
-//   static __device__ uint32_t digit(const Ctx&, int buf, uint64_t i, int pass);
+//   struct Pass;  (what selects the digit of one pass, resolved once per kernel)
+//   static __device__ Pass pass_of(const Ctx&, int pass);
 //   static __device__ Item load(const Ctx&, int buf, uint64_t i);
-//   static __device__ uint32_t digit_of(const Ctx&, const Item&, int pass);
+//   static __device__ uint32_t digit_of(const Pass&, const Item&);
 //   static __device__ void store(const Ctx&, int buf, const Item&, uint32_t dst);  (into buffer buf ^ 1)
 template <class Ops>
 __global__ void __launch_bounds__(SA_RADIX_BLOCK)
@@ -112,56 +113,95 @@ sa_k_radix_up(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, unsigned int* his
     __syncthreads();
     uint64_t a, b;
     sa_radix_range(n, A, a, b);
-    for (uint64_t i = a + t; i < b; i += SA_RADIX_BLOCK) atomicAdd(&h[Ops::digit(ctx, buf, i, pass)], 1u);
+    const typename Ops::Pass P = Ops::pass_of(ctx, pass);
+    for (uint64_t i = a + t; i < b; i += SA_RADIX_BLOCK) atomicAdd(&h[Ops::digit_of(P, Ops::load(ctx, buf, i))], 1u);
     __syncthreads();
     hist[(uint64_t)t * A + blockIdx.x] = h[t];
 }
 
+// Down-sweep: tiles of SA_RADIX_TILE = 256 x SA_RADIX_ITEMS items.  Warp w
+// ranks the tile's items [w * 32 * ITEMS, (w + 1) * 32 * ITEMS) row by row
+// (coalesced loads, __match_any_sync within a row, a per-warp digit count
+// carried across rows); per-digit warp prefixes and the tile's digit starts
+// then place every item in digit order in shared memory, and the tile is
+// written back in that order, so items of one digit leave as runs of
+// consecutive addresses.  Items keep their input order within a digit
+// (stable).
+#define SA_RADIX_ITEMS 4
+#define SA_RADIX_TILE (SA_RADIX_BLOCK * SA_RADIX_ITEMS)
+
 template <class Ops>
 __global__ void __launch_bounds__(SA_RADIX_BLOCK)
 sa_k_radix_down(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, const unsigned int* hist) {
+    constexpr int NWARP = SA_RADIX_BLOCK / 32;
+    constexpr int K = SA_RADIX_ITEMS;
+    using Item = typename Ops::Item;
     const int buf = ctl.in_buf[pass];
     if (buf < 0) return;
     const uint64_t n = *ctl.d_n;
     const uint32_t A = sa_radix_active(n, gridDim.x);
     if (blockIdx.x >= A) return;
-    __shared__ unsigned int offs[256];
-    __shared__ unsigned int wcnt[SA_RADIX_BLOCK / 32][256];
-    const int t = threadIdx.x, warp = t >> 5;
+    __shared__ unsigned int offs[256];           // next output index of each digit (this CTA)
+    __shared__ unsigned int wcnt[NWARP][256];    // per-warp digit counts, then their exclusive prefixes
+    __shared__ unsigned int tstart[256];         // tile-local start of each digit
+    __shared__ unsigned int ws[NWARP + 1];
+    __shared__ Item stage[SA_RADIX_TILE];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     offs[t] = hist[(uint64_t)t * A + blockIdx.x];
-#pragma unroll
-    for (int w = 0; w < SA_RADIX_BLOCK / 32; ++w) wcnt[w][t] = 0;
-    __syncthreads();
     uint64_t a, b;
     sa_radix_range(n, A, a, b);
     const uint32_t lt = sa_lanemask_lt();
-    // Items are loaded one round ahead, so that the load of round r + 1
-    // overlaps the ranking and scatter of round r.
-    typename Ops::Item cur{}, nxt{};
-    if (a + t < b) cur = Ops::load(ctx, buf, a + t);
-    for (uint64_t base = a; base < b; base += SA_RADIX_BLOCK) {
-        const uint64_t i = base + t;
-        const bool valid = i < b;
-        if (i + SA_RADIX_BLOCK < b) nxt = Ops::load(ctx, buf, i + SA_RADIX_BLOCK);
-        const uint32_t d = valid ? Ops::digit_of(ctx, cur, pass) : 256u;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t rank = __popc(peers & lt);
-        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-        __syncthreads();
-        uint32_t run = offs[t];
+    const typename Ops::Pass P = Ops::pass_of(ctx, pass);
+    for (uint64_t base = a; base < b; base += SA_RADIX_TILE) {
 #pragma unroll
-        for (int w = 0; w < SA_RADIX_BLOCK / 32; ++w) {
-            uint32_t c = wcnt[w][t];
+        for (int w = 0; w < NWARP; ++w) wcnt[w][t] = 0;
+        __syncthreads();
+        Item it[K];
+        uint32_t d[K], r[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t i = base + (uint64_t)warp * 32 * K + (uint64_t)k * 32 + lane;
+            const bool valid = i < b;
+            if (valid) it[k] = Ops::load(ctx, buf, i);
+            d[k] = valid ? Ops::digit_of(P, it[k]) : 256u;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint32_t peers = __match_any_sync(0xffffffffu, d[k]);
+            const uint32_t rank = __popc(peers & lt);
+            const bool valid = d[k] < 256u;
+            r[k] = valid ? wcnt[warp][d[k]] + rank : 0u;
+            __syncwarp();
+            if (valid && rank == 0) wcnt[warp][d[k]] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        // digit t: prefixes over the warps, the tile's count, and its start in the tile
+        unsigned int run = 0;
+#pragma unroll
+        for (int w = 0; w < NWARP; ++w) {
+            const unsigned int c = wcnt[w][t];
             wcnt[w][t] = run;
             run += c;
         }
-        offs[t] = run;
-        __syncthreads();
-        if (valid) Ops::store(ctx, buf, cur, wcnt[warp][d] + rank);
-        cur = nxt;
+        unsigned int tot;
+        tstart[t] = sa_block_excl_sum<unsigned int, SA_RADIX_BLOCK>(run, ws, &tot);
         __syncthreads();
 #pragma unroll
-        for (int w = 0; w < SA_RADIX_BLOCK / 32; ++w) wcnt[w][t] = 0;
+        for (int k = 0; k < K; ++k)
+            if (d[k] < 256u) stage[tstart[d[k]] + wcnt[warp][d[k]] + r[k]] = it[k];
         __syncthreads();
+        const uint32_t tile_n = (uint32_t)min((uint64_t)SA_RADIX_TILE, b - base);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint32_t s = (uint32_t)k * SA_RADIX_BLOCK + t;
+            if (s < tile_n) {
+                const Item x = stage[s];
+                const uint32_t dd = Ops::digit_of(P, x);
+                Ops::store(ctx, buf, x, offs[dd] + (s - tstart[dd]));
+            }
+        }
+        __syncthreads();
+        offs[t] += run;
     }
 }

@@ -48,11 +48,11 @@ struct SaRecOps {
             default: return r.ref_start - r.query_start;      // uint32 diagonal
         }
     }
-    static __device__ __forceinline__ uint32_t digit(const Ctx& c, int buf, uint64_t i, int pass) {
-        const SaRec r = c.rec[buf][i];
-        uint32_t v = field_value(r, c.scope[buf][i], c.spec.field[pass]);
-        if (c.spec.inv[pass]) v = ~v;
-        return (v >> (8 * c.spec.byte[pass])) & 0xffu;
+    struct Pass {
+        uint32_t field, shift, inv;
+    };
+    static __device__ __forceinline__ Pass pass_of(const Ctx& c, int pass) {
+        return {c.spec.field[pass], 8u * c.spec.byte[pass], c.spec.inv[pass] ? ~0u : 0u};
     }
     struct Item {
         SaRec r;
@@ -61,10 +61,8 @@ struct SaRecOps {
     static __device__ __forceinline__ Item load(const Ctx& c, int buf, uint64_t i) {
         return {c.rec[buf][i], c.scope[buf][i]};
     }
-    static __device__ __forceinline__ uint32_t digit_of(const Ctx& c, const Item& x, int pass) {
-        uint32_t v = field_value(x.r, x.scope, c.spec.field[pass]);
-        if (c.spec.inv[pass]) v = ~v;
-        return (v >> (8 * c.spec.byte[pass])) & 0xffu;
+    static __device__ __forceinline__ uint32_t digit_of(const Pass& p, const Item& x) {
+        return ((field_value(x.r, x.scope, (int)p.field) ^ p.inv) >> p.shift) & 0xffu;
     }
     static __device__ __forceinline__ void store(const Ctx& c, int buf, const Item& x, uint32_t dst) {
         c.rec[buf ^ 1][dst] = x.r;
@@ -219,6 +217,36 @@ sa_k_uniq_emit(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, 
     }
 }
 
+// Plain-mode output.  The records of a plain sort are the distinct keys
+// (scope, ref_start, query_start, len) of the HSP set, and within a scope the
+// score is a function of the key, so no two records of a scope are equal:
+// unique_copy(hspEqual) keeps every record.  The sorted records are copied
+// to the output as they are, and each count[s] (s = scope >> shift, counts
+// zeroed beforehand) gets end(s) - start(s) from the two records at its
+// boundaries: count[s] -= first index, count[s] += one past the last (the
+// counts wrap through unsigned arithmetic), two atomics per count.
+__global__ void __launch_bounds__(256)
+sa_k_out_copy(SaUniqArgs u, const unsigned long long* d_n, const int* src_buf, unsigned long long* d_out_n) {
+    const unsigned long long n = *d_n;
+    const int buf = *src_buf;
+    const SaRec* __restrict__ rec = u.rec[buf];
+    const uint32_t* __restrict__ sc = u.scope[buf];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_out_n = n;
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t s = sc[i];
+        u.out_rec[i] = rec[i];
+        u.out_scope[i] = s;
+        const uint32_t g = s >> u.scope_shift;
+        const uint32_t gp = i > 0 ? sc[i - 1] >> u.scope_shift : ~0u;
+        if (g != gp) {
+            atomicSub(&u.scope_count[g], (uint32_t)i);
+            if (i > 0) atomicAdd(&u.scope_count[gp], (uint32_t)i);
+        }
+        if (i + 1 == n) atomicAdd(&u.scope_count[g], (uint32_t)n);
+    }
+}
+
 // st[0] <- 1 - final buffer of the last sort (the buffer the unique step wrote).
 __global__ void sa_k_flip_cur(int* st, int np) { st[0] = st[1 + np] ^ 1; }
 
@@ -358,7 +386,8 @@ void sa_launch_dedup(SaWork& w, int mode, int scope_shift, int G, cudaStream_t s
         u.out_rec = w.out;
         u.out_scope = w.out_scope;
         u.scope_count = w.scope_count;
-        sa_uniq(w, u, n0, st + 1 + plain.npass, &w.ctr->uniq_count, G, s);
+        sa_k_out_copy<<<148 * 8, 256, 0, s>>>(u, n0, st + 1 + plain.npass, &w.ctr->uniq_count);
+        sa_note_launch();
         return;
     }
     // rm: unique(hspEqual) into the other buffer
