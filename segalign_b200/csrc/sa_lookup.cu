@@ -286,7 +286,7 @@ sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restri
                                                             B.q_start + (s - B.slot_begin))
                                           : B.q_start + (uint32_t)((s - B.slot_begin) / S);
                     cs.unit[ec] = B.unit;
-                    cs.scope[ec] = cur.u;  // batch unit index; turned into (unit, iteration) by sa_k_bscope
+                    cs.scope[ec] = cur.u << 4;  // (batch unit, iteration 0); sa_k_bscope sets later iterations
                     ++ec;
                 }
                 eh += cnt[k];
@@ -354,27 +354,48 @@ __global__ void sa_k_bgroups(const SaCallDesc* __restrict__ desc, SaSeedList cs,
     }
 }
 
-// Compacted seed -> scope = (batch unit << 4) | iteration.
-__global__ void sa_k_bscope(SaSeedList cs, const unsigned long long* __restrict__ unit_hit_base,
-                            const unsigned long long* __restrict__ bounds, const uint32_t* __restrict__ unit_iters,
-                            SaCounters* ctr) {
+// Compacted seed -> scope = (batch unit << 4) | iteration, for the units with
+// more than one MAX_HITS iteration (the emit wrote iteration 0).  One CTA per
+// such unit: its compacted seeds are those with E in [base, base + H).
+__global__ void __launch_bounds__(256)
+sa_k_bscope(const SaCallDesc* __restrict__ desc, SaSeedList cs, const unsigned long long* __restrict__ unit_hit_base,
+            const unsigned long long* __restrict__ unit_hit_end, const unsigned long long* __restrict__ bounds,
+            const uint32_t* __restrict__ unit_iters, SaCounters* ctr) {
+    const uint32_t nu = desc->num_units;
     const uint64_t nnz = ctr->nnz;
-    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < nnz; c += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t u = cs.scope[c];
+    for (uint32_t u = blockIdx.x; u < nu; u += gridDim.x) {
         const uint32_t it = unit_iters[u];
-        uint32_t g = 0;
-        if (it > 1) {
-            const uint64_t p = cs.E[c + 1] - unit_hit_base[u];
-            const unsigned long long* B = bounds + (uint64_t)u * SA_BATCH_ITERS;
-            while (g + 1 < it && p > B[g]) ++g;
+        if (it <= 1) continue;
+        const uint64_t base = unit_hit_base[u], H = unit_hit_end[u] - base;
+        uint64_t lo = 0, hi = nnz;
+        while (lo < hi) {
+            const uint64_t m = (lo + hi) >> 1;
+            if (cs.E[m] < base) lo = m + 1;
+            else hi = m;
         }
-        cs.scope[c] = (u << 4) | g;
+        const uint64_t c0 = lo;
+        hi = nnz;
+        while (lo < hi) {
+            const uint64_t m = (lo + hi) >> 1;
+            if (cs.E[m] < base + H) lo = m + 1;
+            else hi = m;
+        }
+        const unsigned long long* B = bounds + (uint64_t)u * SA_BATCH_ITERS;
+        for (uint64_t c = c0 + threadIdx.x; c < lo; c += blockDim.x) {
+            const uint64_t p = cs.E[c + 1] - base;
+            uint32_t g = 0;
+            while (g + 1 < it && p > B[g]) ++g;
+            cs.scope[c] = (u << 4) | g;
+        }
     }
 }
 
 void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets, uint32_t n_bunits, const SaParams& p,
                             int G, cudaStream_t st) {
     const int S = p.transition ? 1 + p.kmer_size : 1;
+    // a unit without slots (an empty window) gets the empty hit range [0, 0)
+    cudaMemsetAsync(w.unit_hit_base, 0, 8ull * n_bunits, st);
+    cudaMemsetAsync(w.unit_hit_end, 0, 8ull * n_bunits, st);
     sa_k_blookup_count<<<G, 256, 0, st>>>(w.bunits, w.desc, index, nbuckets, S, w.s_lo, w.s_cnt, w.cta_a, w.cta_b,
                                           w.ctr);
     sa_note_launch();
@@ -387,6 +408,7 @@ void sa_launch_lookup_batch(SaWork& w, const uint32_t* index, uint32_t nbuckets,
     sa_k_bgroups<<<ub > 0 ? ub : 1, 256, 0, st>>>(w.desc, w.cs, w.unit_hit_base, w.unit_hit_end, w.bounds,
                                                   w.unit_iters, w.ctr);
     sa_note_launch();
-    sa_k_bscope<<<148 * 4, 256, 0, st>>>(w.cs, w.unit_hit_base, w.bounds, w.unit_iters, w.ctr);
+    sa_k_bscope<<<(int)std::min<uint32_t>(std::max<uint32_t>(n_bunits, 1u), 1024u), 256, 0, st>>>(w.desc, w.cs, w.unit_hit_base, w.unit_hit_end,
+                                                                      w.bounds, w.unit_iters, w.ctr);
     sa_note_launch();
 }

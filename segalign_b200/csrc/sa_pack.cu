@@ -321,15 +321,60 @@ void sa_launch_sort_kv(uint32_t* keys, uint32_t* vals, uint32_t* keys_tmp, uint3
 // src/seeder.cpp:57-74 without the host loop): keys[j] = key of the window at
 // j, SA_INVALID_KEY unless all seed_size bases are uppercase ACGT.
 // ---------------------------------------------------------------------------
-__global__ void sa_k_query_keys(const uint32_t* __restrict__ packed, uint64_t len, SaParams P,
-                                uint32_t* __restrict__ keys) {
-    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < len; j += (uint64_t)gridDim.x * blockDim.x)
-        keys[j] = sa_key_at(packed, (int64_t)j, P);
+//
+// One thread takes the 8 positions of one packed word, p0 = 8g .. 8g + 7, and
+// the five words from word g on, which hold every base their windows reach
+// (seed_size <= 32 bases, padding after the last word).  Validity: a 40-bit
+// mask of the windows' non-ACGT bases (code bit 2), tested against the
+// seed_size bits from each position.  Keys: for each shape position s in
+// increasing order (the shape's order, common/ntcoding.cpp:21-37), the word
+// of bases p0 + s .. p0 + s + 7 gives the next 2-bit code of all 8 keys at once.
+__device__ __forceinline__ uint32_t sa_nonacgt8(uint32_t w) {
+    uint32_t t = (w >> 2) & 0x11111111u;  // bit 4k = code bit 2 of base k
+    t = (t | (t >> 3)) & 0x03030303u;
+    t = (t | (t >> 6)) & 0x000f000fu;
+    return (t | (t >> 12)) & 0xffu;
+}
+
+__global__ void __launch_bounds__(256)
+sa_k_query_keys(const uint32_t* __restrict__ packed, uint64_t len, SaParams P, uint32_t* __restrict__ keys) {
+    uint64_t smask = 0;  // bit s set: shape position s is a care position
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        if (i < P.kmer_size) smask |= 1ull << P.shape_pos[i];
+    const uint32_t ss = (uint32_t)P.seed_size;
+    const uint64_t wmask = ss >= 64 ? ~0ull : (1ull << ss) - 1;
+    const uint64_t ngroups = (len + 7) / 8;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t* pw = packed + g;
+        const uint32_t W0 = __ldg(pw), W1 = __ldg(pw + 1), W2 = __ldg(pw + 2), W3 = __ldg(pw + 3), W4 = __ldg(pw + 4);
+        const uint64_t bad = (uint64_t)sa_nonacgt8(W0) | ((uint64_t)sa_nonacgt8(W1) << 8) |
+                             ((uint64_t)sa_nonacgt8(W2) << 16) | ((uint64_t)sa_nonacgt8(W3) << 24) |
+                             ((uint64_t)sa_nonacgt8(W4) << 32);
+        uint32_t key[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) key[k] = 0;
+        for (uint64_t m = smask; m; m &= m - 1) {
+            const uint32_t sp = (uint32_t)(__ffsll((long long)m) - 1);
+            const uint32_t q = sp >> 3;
+            const uint32_t a = q == 0 ? W0 : q == 1 ? W1 : q == 2 ? W2 : W3;
+            const uint32_t b = q == 0 ? W1 : q == 1 ? W2 : q == 2 ? W3 : W4;
+            const uint32_t win = __funnelshift_r(a, b, 4u * (sp & 7u));
+#pragma unroll
+            for (int k = 0; k < 8; ++k) key[k] = (key[k] << 2) | ((win >> (4 * k)) & 3u);
+        }
+        const uint64_t p0 = 8 * g;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (p0 + k < len) keys[p0 + k] = ((bad >> k) & wmask) ? SA_INVALID_KEY : key[k];
+    }
 }
 
 void sa_launch_query_keys(const uint32_t* packed, uint64_t len, const SaParams& p, uint32_t* keys, cudaStream_t st) {
     if (!len) return;
-    int blocks = (int)std::min<uint64_t>((len + 255) / 256, 148ull * 16);
+    const uint64_t groups = (len + 7) / 8;
+    int blocks = (int)std::min<uint64_t>((groups + 255) / 256, 148ull * 16);
     sa_k_query_keys<<<blocks, 256, 0, st>>>(packed, len, p, keys);
     sa_note_launch();
 }

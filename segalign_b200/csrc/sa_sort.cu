@@ -268,25 +268,46 @@ __global__ void sa_k_hash_init(SaHashSet hs, SaCounters* ctr, unsigned long long
 
 // Distinct HSPs out of the set into rec/scope, in claim order (the sort that
 // follows is total), emptying their slots.  *n_out = slots claimed; more than
-// `cap` is a capacity error (sa_k_dedup_prep).
+// `cap` is a capacity error (sa_k_dedup_prep).  A thread gathers
+// SA_COMPACT_ITEMS slots before it writes any (the slots of the list are
+// distinct), so their scattered loads are in flight together.
+#define SA_COMPACT_ITEMS 4
 __global__ void __launch_bounds__(256)
 sa_k_hash_compact(SaHashSet hs, SaCounters* ctr, SaRec* rec, uint32_t* scope, uint64_t cap, unsigned long long* n_out) {
+    constexpr int J = SA_COMPACT_ITEMS;
     const unsigned long long used = ctr->hash_used;
     unsigned long long n = used < hs.used_cap ? used : hs.used_cap;
     if (n > cap) n = cap;
     if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = used;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long h = hs.used[i];
-        const ulonglong2 k = *reinterpret_cast<const ulonglong2*>(hs.keys + 2 * h);
-        SaRec r;
-        r.ref_start = (uint32_t)k.x;
-        r.query_start = (uint32_t)(k.y >> 32);
-        r.len = (uint32_t)k.y;
-        r.score = hs.score[h];
-        rec[i] = r;
-        scope[i] = (uint32_t)(k.x >> 32);
-        *reinterpret_cast<ulonglong2*>(hs.keys + 2 * h) = make_ulonglong2(~0ull, ~0ull);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i0 < n; i0 += J * stride) {
+        unsigned long long h[J];
+        ulonglong2 k[J];
+        int32_t sc[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const unsigned long long i = i0 + j * stride;
+            h[j] = i < n ? hs.used[i] : ~0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            if (h[j] != ~0ull) {
+                k[j] = *reinterpret_cast<const ulonglong2*>(hs.keys + 2 * h[j]);
+                sc[j] = hs.score[h[j]];
+            }
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            if (h[j] != ~0ull) {
+                const unsigned long long i = i0 + j * stride;
+                SaRec r;
+                r.ref_start = (uint32_t)k[j].x;
+                r.query_start = (uint32_t)(k[j].y >> 32);
+                r.len = (uint32_t)k[j].y;
+                r.score = sc[j];
+                rec[i] = r;
+                scope[i] = (uint32_t)(k[j].x >> 32);
+                *reinterpret_cast<ulonglong2*>(hs.keys + 2 * h[j]) = make_ulonglong2(~0ull, ~0ull);
+            }
     }
 }
 
