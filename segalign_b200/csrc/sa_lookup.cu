@@ -156,47 +156,6 @@ __device__ __forceinline__ uint32_t sa_find_unit(const SaBatchUnit* __restrict__
     return lo;
 }
 
-struct SaSlotInfo {
-    uint32_t unit, j, lo, cnt;
-};
-
-// Slot s of batch unit B: its query position, bucket start and hit count.
-// An explicit word whose key is outside the table sets bad_key (a plain call
-// reports it as SA_ERR_BAD_SEED, src/seed_filter.cu:129-154 reads past the
-// table there); a device-seeded slot never has such a key.
-__device__ __forceinline__ SaSlotInfo sa_slot(const SaBatchUnit& B, uint64_t s, const uint32_t* __restrict__ index,
-                                              uint32_t nbuckets, int S, bool& bad_key) {
-    SaSlotInfo r;
-    const uint64_t off = s - B.slot_begin;
-    r.unit = B.unit;
-    uint32_t key;
-    uint32_t v = 0;
-    if (B.seeds) {  // find_num_hits (src/seed_filter.cu:129-154) on the call's own words
-        const uint64_t word = __ldg(reinterpret_cast<const unsigned long long*>(B.seeds) + B.q_start + off);
-        key = (uint32_t)(word >> 32);
-        r.j = (uint32_t)word;
-        if (key >= nbuckets) {
-            bad_key = true;
-            key = SA_INVALID_KEY;
-        }
-    } else {
-        r.j = B.q_start + (uint32_t)(off / S);
-        v = (uint32_t)(off % S);
-        key = __ldg(B.keys + r.j);
-    }
-    r.lo = 0;
-    r.cnt = 0;
-    if (key != SA_INVALID_KEY) {
-        if (v) key ^= 2u << (2 * (v - 1));
-        if (key < nbuckets) {
-            uint32_t hi = __ldg(index + key);
-            r.lo = key ? __ldg(index + key - 1) : 0u;
-            r.cnt = hi - r.lo;
-        }
-    }
-    return r;
-}
-
 // The unit holding slot s, kept per thread: a thread's slots only increase,
 // so the binary search runs only when s passes the current unit's end.
 struct SaUnitCursor {
@@ -211,11 +170,17 @@ struct SaUnitCursor {
     }
 };
 
+// Per CTA: hits and hit-bearing slots of its range.  A thread takes
+// SA_COUNT_ITEMS slots 256 apart per round and issues all their key loads,
+// then all their bucket-bound loads, then the stores (the loads of one round
+// are in flight together).
+#define SA_COUNT_ITEMS 4
 __global__ void __launch_bounds__(256)
 sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restrict__ desc,
                    const uint32_t* __restrict__ index, uint32_t nbuckets, int S,
                    uint32_t* __restrict__ s_lo, uint32_t* __restrict__ s_cnt, unsigned long long* cta_a,
                    unsigned long long* cta_b, SaCounters* ctr) {
+    constexpr int J = SA_COUNT_ITEMS;
     const uint64_t n = desc->num_seeds;
     uint64_t a, b;
     sa_cta_range(n, a, b);
@@ -223,13 +188,50 @@ sa_k_blookup_count(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restr
     unsigned long long hits = 0, nz = 0;
     bool bad_key = false;
     SaUnitCursor cur;
-    for (uint64_t s = a + threadIdx.x; s < b; s += 256) {
-        cur.seek(bu, nu, n, s);
-        const SaSlotInfo si = sa_slot(cur.B, s, index, nbuckets, S, bad_key);
-        s_lo[s] = si.lo;
-        s_cnt[s] = si.cnt;
-        hits += si.cnt;
-        nz += si.cnt != 0;
+    for (uint64_t s0 = a + threadIdx.x; s0 < b; s0 += 256 * J) {
+        uint32_t key[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const uint64_t s = s0 + 256ull * j;
+            key[j] = SA_INVALID_KEY;
+            if (s < b) {
+                cur.seek(bu, nu, n, s);
+                const SaBatchUnit& B = cur.B;
+                const uint64_t off = s - B.slot_begin;
+                // find_num_hits (src/seed_filter.cu:129-154) on a call's own words; a key
+                // outside the table is reported (a plain call's SA_ERR_BAD_SEED), never read
+                if (B.seeds) {
+                    const uint32_t k = (uint32_t)(__ldg(reinterpret_cast<const unsigned long long*>(B.seeds) +
+                                                        B.q_start + off) >> 32);
+                    if (k >= nbuckets) bad_key = true;
+                    else key[j] = k;
+                } else {
+                    const uint32_t v = (uint32_t)(off % S);
+                    const uint32_t k = __ldg(B.keys + B.q_start + (uint32_t)(off / S));
+                    key[j] = (k == SA_INVALID_KEY || !v) ? k : k ^ (2u << (2 * (v - 1)));
+                }
+            }
+        }
+        uint32_t lo[J], hi[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            lo[j] = hi[j] = 0;
+            if (key[j] < nbuckets) {
+                hi[j] = __ldg(index + key[j]);
+                lo[j] = key[j] ? __ldg(index + key[j] - 1) : 0u;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const uint64_t s = s0 + 256ull * j;
+            if (s < b) {
+                const uint32_t c = hi[j] - lo[j];
+                s_lo[s] = lo[j];
+                s_cnt[s] = c;
+                hits += c;
+                nz += c != 0;
+            }
+        }
     }
     if (bad_key) atomicCAS(&ctr->error, 0ull, (unsigned long long)SA_DERR_BAD_KEY);
     __shared__ unsigned long long ws[9];
@@ -259,15 +261,25 @@ sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restri
     unsigned long long hbase = cta_a[blockIdx.x], cbase = cta_b[blockIdx.x];
     __shared__ unsigned long long ws[9];
     SaUnitCursor cur;
-    for (uint64_t r = a; r < b; r += 256 * SA_EMIT_ITEMS) {
+    // each round's counts and bucket starts are loaded during the round before
+    uint32_t cnt[SA_EMIT_ITEMS], lo[SA_EMIT_ITEMS];
+    auto fetch = [&](uint64_t r, uint32_t* c, uint32_t* l) {
         const uint64_t s0 = r + (uint64_t)threadIdx.x * SA_EMIT_ITEMS;
-        uint32_t cnt[SA_EMIT_ITEMS];
-        unsigned long long mine = 0;
 #pragma unroll
         for (int k = 0; k < SA_EMIT_ITEMS; ++k) {
-            cnt[k] = s0 + k < b ? s_cnt[s0 + k] : 0u;
-            mine += ((unsigned long long)cnt[k] << 16) | (cnt[k] != 0);
+            const bool in = s0 + k < b;
+            c[k] = in ? s_cnt[s0 + k] : 0u;
+            l[k] = in ? s_lo[s0 + k] : 0u;
         }
+    };
+    fetch(a, cnt, lo);
+    for (uint64_t r = a; r < b; r += 256 * SA_EMIT_ITEMS) {
+        const uint64_t s0 = r + (uint64_t)threadIdx.x * SA_EMIT_ITEMS;
+        uint32_t ncnt[SA_EMIT_ITEMS], nlo[SA_EMIT_ITEMS];
+        fetch(r + 256 * SA_EMIT_ITEMS, ncnt, nlo);
+        unsigned long long mine = 0;
+#pragma unroll
+        for (int k = 0; k < SA_EMIT_ITEMS; ++k) mine += ((unsigned long long)cnt[k] << 16) | (cnt[k] != 0);
         unsigned long long tot;
         const unsigned long long e = sa_block_excl_sum<unsigned long long, 256>(mine, ws, &tot);
         unsigned long long eh = hbase + (e >> 16), ec = cbase + (e & 0xffffu);
@@ -281,7 +293,7 @@ sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restri
                 if (s + 1 == cur.end) unit_hit_end[cur.u] = eh + cnt[k];
                 if (cnt[k]) {
                     cs.E[ec] = eh;
-                    cs.lo[ec] = s_lo[s];
+                    cs.lo[ec] = lo[k];
                     cs.qpos[ec] = B.seeds ? (uint32_t)__ldg(reinterpret_cast<const unsigned long long*>(B.seeds) +
                                                             B.q_start + (s - B.slot_begin))
                                           : B.q_start + (uint32_t)((s - B.slot_begin) / S);
@@ -294,6 +306,11 @@ sa_k_blookup_emit(const SaBatchUnit* __restrict__ bu, const SaCallDesc* __restri
         }
         hbase += tot >> 16;
         cbase += tot & 0xffffu;
+#pragma unroll
+        for (int k = 0; k < SA_EMIT_ITEMS; ++k) {
+            cnt[k] = ncnt[k];
+            lo[k] = nlo[k];
+        }
     }
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) cs.E[ctr->nnz] = ctr->num_hits;
 }

@@ -127,7 +127,9 @@ sa_k_radix_up(typename Ops::Ctx ctx, int pass, SaRadixCtl ctl, unsigned int* his
 // written back in that order, so items of one digit leave as runs of
 // consecutive addresses.  Items keep their input order within a digit
 // (stable).
+#ifndef SA_RADIX_ITEMS
 #define SA_RADIX_ITEMS 4
+#endif
 #define SA_RADIX_TILE (SA_RADIX_BLOCK * SA_RADIX_ITEMS)
 
 template <class Ops>
