@@ -78,6 +78,8 @@ def parse_args():
     ap.add_argument("--large-cpu-units", type=int, default=0,
                     help="units of the 600 Mbp leg also run through the CPU port (0 = none: its table build "
                          "takes minutes on the host)")
+    ap.add_argument("--no-fasta", action="store_true",
+                    help="skip the whole-file leg (the workload as FASTA through sa_align_fasta to a segments file)")
     ap.add_argument("--no-ref-gpu", action="store_true",
                     help="skip the unranked timing of the reference's own kernels (oracle/_ref)")
     ap.add_argument("--ref-gpu-units", type=int, default=16,
@@ -730,6 +732,10 @@ def run_ours(args):
             and np.array_equal(gf.view(np.uint32), r["fw"].view(np.uint32))
             and np.array_equal(gr.view(np.uint32), r["rc"].view(np.uint32)))
 
+    # ---- whole files: the same workload as FASTA through sa_align_fasta (one GPU) ----
+    if world == 1 and args.workload == "genome" and not args.no_fasta:
+        out["fasta"] = run_fasta(sf, w, None if args.no_e2e else sst)
+
     # ---- the 600 Mbp legs (one GPU): config 4 batched and plain, config 5 serving, repeat masker ----
     if world == 1 and args.workload == "genome" and not args.no_large:
         del w, outs
@@ -743,6 +749,46 @@ def run_ours(args):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def run_fasta(sf, w, e2e_stats) -> dict:
+    """Whole-file leg: the workload written as FASTA (one record per target
+    chromosome, the query as one record) and run through sa_align_fasta, the
+    path of the reference's main.cpp minus lastz: parse, '&'-joined blocks,
+    target upload and seed-table build, double-buffered query upload, the C++
+    seeder over plain calls on 16 host threads, and the segment writer on the
+    GPU into a segments file.  Host wall time of the one call.  Its hits and
+    HSPs equal the e2e leg's (same text, intervals and chunks)."""
+    import shutil
+    import tempfile
+
+    d = tempfile.mkdtemp(prefix="sa_fasta_")
+    try:
+        tp, qp, sp = (os.path.join(d, n) for n in ("target.fa", "query.fa", "out.segments"))
+        for path, text, chrs, tag in ((tp, w.target, w.target_chr, b"chr"), (qp, w.query, w.query_chr, b"q")):
+            with open(path, "wb") as f:
+                for i, (a, n) in enumerate(chrs):
+                    f.write(b">%s%d\n" % (tag, i + 1))
+                    f.write(text[a:a + n])
+                    f.write(b"\n")
+        threads = min(16, os.cpu_count() or 8)
+        t0 = time.perf_counter()
+        st = sf.align_fasta(tp, qp, segments_path=sp, interval_size=INTERVAL, interval_overlap=OVERLAP,
+                            chunk_size=CHUNK, num_threads=threads)
+        dt = time.perf_counter() - t0
+        res = {"workload": f"the genome-scale workload as FASTA files ({len(w.target_chr)} target records, "
+                           f"{len(w.query_chr)} query record) to a lastz --segments file, {threads} host threads",
+               "seconds": dt, "read_s": st["read_seconds"], "table_s": st["table_seconds"],
+               "query_write_s": st["query_write_seconds"], "calls_s": st["calls_seconds"],
+               "output_s": st["output_seconds"], "hits": st["num_hits"], "hsps": st["num_hsps"],
+               "extensions_per_s": st["num_hits"] / dt, "segments_bytes": os.path.getsize(sp),
+               "fasta_bytes": os.path.getsize(tp) + os.path.getsize(qp)}
+        if e2e_stats is not None:
+            res["same_hits_and_hsps_as_e2e"] = bool(st["num_hits"] == e2e_stats["num_hits"]
+                                                    and st["num_hsps"] == e2e_stats["num_hsps"])
+        return res
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def run_rm(sf, target: bytes, n_intervals: int, transition: bool) -> dict:

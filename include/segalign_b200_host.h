@@ -176,7 +176,8 @@ void sa_seq_set_free(sa_seq_set* s);
  * SeedAndFilter calls per strand (src/seeder.cpp:47-121).  Per interval, the
  * lastz --segments lines of its HSPs (sa_format_segments: plus strand, then
  * minus) go to segments_path, and its HSP records to hsp_path as
- * {u32 target block, u32 query block, u32 interval, u32 strand, sa_segment}.
+ * {u32 target block, u32 query block, u32 interval, u32 strand, sa_segment};
+ * a writer thread puts out interval i while the seeders run interval i + 1. 
  * Needs sa_initialize_interface, sa_generate_shape_pos, sa_host_set_shape and
  * sa_initialize_processor first; replaces the resident target and query
  * buffers 0 and 1. */
@@ -207,6 +208,8 @@ typedef struct {
     double table_seconds;        /* target uploads and seed-table builds         */
     double query_write_seconds;  /* query block uploads (loader thread)          */
     double overlap_seconds;      /* of those, while the seeders ran the other buffer */
+    double calls_seconds;        /* seeding and SeedAndFilter calls, interval by interval */
+    double output_seconds;       /* HSP records and segment lines (writer thread, overlaps the calls) */
 } sa_align_stats;
 
 int sa_align_fasta(const sa_align_cfg* cfg, sa_align_stats* stats);

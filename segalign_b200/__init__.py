@@ -162,7 +162,8 @@ class AlignStats(C.Structure):
     _fields_ = [("ref_blocks", C.c_uint64), ("query_blocks", C.c_uint64), ("intervals", C.c_uint64),
                 ("num_seeds", C.c_uint64), ("num_hits", C.c_uint64), ("num_hsps", C.c_uint64),
                 ("seconds", C.c_double), ("read_seconds", C.c_double), ("table_seconds", C.c_double),
-                ("query_write_seconds", C.c_double), ("overlap_seconds", C.c_double)]
+                ("query_write_seconds", C.c_double), ("overlap_seconds", C.c_double), ("calls_seconds", C.c_double),
+                ("output_seconds", C.c_double)]
 
 
 _lib = None

@@ -29,6 +29,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -42,7 +44,7 @@ namespace {
 
 class FastaReader {
   public:
-    explicit FastaReader(const char* path) : f_(gzopen(path, "r")) {}
+    explicit FastaReader(const char* path) : f_(gzopen(path, "r")), buf_(new char[kBuf]) {}
     ~FastaReader() {
         if (f_) gzclose(f_);
     }
@@ -73,8 +75,7 @@ class FastaReader {
         while ((c = getc()) >= 0 && c != '>' && c != '+' && c != '@') {
             if (c == '\n') continue;
             seq.push_back((char)c);
-            int d;
-            while ((d = getc()) >= 0 && d != '\n') seq.push_back((char)d);
+            append_line(seq);
             if (seq.size() > 1 && seq.back() == '\r') seq.pop_back();
         }
         if (c == '>' || c == '@') pending_ = true;
@@ -100,21 +101,39 @@ class FastaReader {
     }
 
   private:
-    int getc() {
-        if (pos_ >= len_) {
-            if (eof_) return -1;
-            int n = gzread(f_, buf_, sizeof buf_);
-            if (n <= 0) {
-                eof_ = true;
-                return -1;
-            }
-            len_ = n;
-            pos_ = 0;
+    bool refill() {
+        if (eof_) return false;
+        int n = gzread(f_, buf_.get(), kBuf);
+        if (n <= 0) {
+            eof_ = true;
+            return false;
         }
+        len_ = n;
+        pos_ = 0;
+        return true;
+    }
+    int getc() {
+        if (pos_ >= len_ && !refill()) return -1;
         return (unsigned char)buf_[pos_++];
     }
+    // Appends the rest of the current line to s and consumes its '\n' (the
+    // same characters as reading them one at a time, a buffer span at a time).
+    void append_line(std::string& s) {
+        while (pos_ < len_ || refill()) {
+            const char* b = buf_.get() + pos_;
+            const char* e = static_cast<const char*>(std::memchr(b, '\n', (size_t)(len_ - pos_)));
+            if (e) {
+                s.append(b, (size_t)(e - b));
+                pos_ += (int)(e - b) + 1;
+                return;
+            }
+            s.append(b, (size_t)(len_ - pos_));
+            pos_ = len_;
+        }
+    }
+    static constexpr unsigned kBuf = 1u << 20;
     gzFile f_;
-    char buf_[1 << 16];
+    std::unique_ptr<char[]> buf_;
     int pos_ = 0, len_ = 0;
     bool eof_ = false, pending_ = false;
 };
@@ -193,6 +212,128 @@ sa_chrom_table table_of(const SeqSetImpl& s) {
 double secs_since(std::chrono::steady_clock::time_point t) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
 }
+
+// Puts out the finished intervals of one query block on a thread of its own,
+// in interval order, while the seeders run the next interval: per interval
+// its HSP records {target block, query block, interval, strand, sa_segment}
+// (plus strand first) and the lastz --segments lines of both strands from the
+// GPU segment writer.  Takes ownership of each interval's call outputs.
+class IntervalWriter {
+  public:
+    IntervalWriter(FILE* seg, FILE* hsp, const sa_chrom_table* ttab, uint64_t rstart, const sa_chrom_table* qtab,
+                   uint64_t qs, uint32_t ql, uint32_t rb, uint32_t qb)
+        : seg_(seg), hsp_(hsp), ttab_(ttab), qtab_(qtab), rstart_(rstart), qs_(qs), ql_(ql), rb_(rb), qb_(qb),
+          th_([this] { run(); }) {}
+    ~IntervalWriter() { finish(nullptr); }
+
+    // Queues interval iv; returns the writer's first error, if it failed.
+    int push(uint32_t iv, std::vector<SaHostCall>&& calls, std::vector<SaHostCallOut>&& res) {
+        std::lock_guard<std::mutex> lk(mu_);
+        q_.push_back(Item{iv, std::move(calls), std::move(res)});
+        cv_.notify_all();
+        return err_;
+    }
+
+    // Waits until every queued interval is out; returns the first error (its
+    // message becomes the calling thread's sa_last_error()).
+    int finish(double* seconds) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            closed_ = true;
+        }
+        cv_.notify_all();
+        if (th_.joinable()) {
+            th_.join();
+            if (err_ != SA_OK) sa_set_error(err_, "%s", msg_.c_str());
+            if (seconds) *seconds += busy_;
+        }
+        return err_;
+    }
+
+  private:
+    struct Item {
+        uint32_t iv = 0;
+        std::vector<SaHostCall> calls;
+        std::vector<SaHostCallOut> res;
+    };
+
+    void run() {
+        while (true) {
+            Item it;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return closed_ || !q_.empty(); });
+                if (q_.empty()) return;
+                it = std::move(q_.front());
+                q_.pop_front();
+            }
+            const auto t0 = std::chrono::steady_clock::now();
+            const int e = err_ == SA_OK ? write(it) : err_;  // after a failure the rest is only freed
+            for (auto& x : it.res) sa_free_segments(x.p);
+            busy_ += secs_since(t0);
+            if (e != SA_OK && err_ == SA_OK) {
+                msg_ = sa_last_error();
+                std::lock_guard<std::mutex> lk(mu_);
+                err_ = e;
+            }
+        }
+    }
+
+    int write(const Item& it) {
+        std::vector<sa_segment> fw, rc;
+        for (size_t c = 0; c < it.calls.size(); ++c) {
+            if (!it.res[c].p) continue;
+            auto& dst = it.calls[c].strand ? rc : fw;
+            dst.insert(dst.end(), it.res[c].p + 1, it.res[c].p + 1 + it.res[c].n);
+        }
+        if (hsp_) {
+            struct Rec {
+                uint32_t key[4];
+                sa_segment h;
+            };
+            static_assert(sizeof(Rec) == 32, "HSP record layout");
+            std::vector<Rec> out;
+            out.reserve(fw.size() + rc.size());
+            for (int sd = 0; sd < 2; ++sd)
+                for (const sa_segment& h : sd ? rc : fw) out.push_back(Rec{{rb_, qb_, it.iv, (uint32_t)sd}, h});
+            if (!out.empty() && fwrite(out.data(), sizeof(Rec), out.size(), hsp_) != out.size()) {
+                sa_set_error(SA_ERR_ARG, "writing the HSP record file failed");
+                return SA_ERR_ARG;
+            }
+        }
+        if (seg_ && (fw.size() || rc.size())) {
+            char *pt = nullptr, *mt = nullptr;
+            uint64_t pl = 0, ml = 0;
+            const int f = sa_format_segments_gpu(ttab_, rstart_, qtab_, qs_, ql_, fw.data(), fw.size(), rc.data(),
+                                                 rc.size(), &pt, &pl, &mt, &ml);
+            bool ok = f == SA_OK;
+            if (ok) ok = fwrite(pt, 1, pl, seg_) == pl && fwrite(mt, 1, ml, seg_) == ml;
+            sa_free_text(pt);
+            sa_free_text(mt);
+            if (f != SA_OK) return f;
+            if (!ok) {
+                sa_set_error(SA_ERR_ARG, "writing the segments file failed");
+                return SA_ERR_ARG;
+            }
+        }
+        return SA_OK;
+    }
+
+    FILE* seg_;
+    FILE* hsp_;
+    const sa_chrom_table* ttab_;
+    const sa_chrom_table* qtab_;
+    uint64_t rstart_, qs_;
+    uint32_t ql_, rb_, qb_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<Item> q_;
+    bool closed_ = false;
+    int err_ = SA_OK;
+    std::string msg_;
+    double busy_ = 0;
+    std::thread th_;  // last: starts once the members above are set
+};
 
 }  // namespace
 
@@ -322,68 +463,44 @@ int sa_align_fasta(const sa_align_cfg* cfg_in, sa_align_stats* stats) {
             const uint64_t qs = Q.block_start[k];
             const uint32_t ql = Q.block_len[k];
             if (ql > (uint32_t)seed_size) {
-                // intervals over [0, Lq - seed_size) (src/main.cpp:373-386, :707)
+                // intervals over [0, Lq - seed_size) (src/main.cpp:373-386, :707),
+                // each with its plus-strand then its minus-strand calls
                 const uint32_t qlen_s = ql - (uint32_t)seed_size;
-                std::vector<SaHostCall> calls;
-                std::vector<uint32_t> call_iv;
-                uint32_t niv = 0;
-                for (uint64_t cur = 0; cur < qlen_s; cur += cfg.interval_size, ++niv) {
+                std::vector<std::vector<SaHostCall>> iv_calls;
+                for (uint64_t cur = 0; cur < qlen_s; cur += cfg.interval_size) {
                     const uint32_t s = (uint32_t)cur;
                     const uint32_t e = (uint32_t)std::min<uint64_t>(qlen_s, cur + cfg.interval_size + cfg.interval_overlap);
+                    std::vector<SaHostCall> calls;
                     if (cfg.strand & 1)
-                        for (uint64_t i = s; i < e; i += cfg.chunk_size) {
+                        for (uint64_t i = s; i < e; i += cfg.chunk_size)
                             calls.push_back({0, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg.chunk_size, e)});
-                            call_iv.push_back(niv);
-                        }
                     if (cfg.strand & 2) {
                         const uint32_t rs = qlen_s - e, re = qlen_s - s;
-                        for (uint64_t i = rs; i < re; i += cfg.chunk_size) {
+                        for (uint64_t i = rs; i < re; i += cfg.chunk_size)
                             calls.push_back({1, (uint32_t)i, (uint32_t)std::min<uint64_t>(i + cfg.chunk_size, re)});
-                            call_iv.push_back(niv);
-                        }
                     }
+                    iv_calls.push_back(std::move(calls));
                 }
-                std::vector<SaHostCallOut> res;
-                SaHostRunStats rs;
-                r = sa_host_run_calls(calls, Q.text.data() + qs, rc_text[b].data(), b, cfg.num_threads, res, &rs);
-                if (r == SA_OK) {
+                // The seeders run interval i + 1 while the writer thread puts
+                // out interval i: its HSP records, then its segment lines
+                // (plus strand, then minus), in interval order.
+                IntervalWriter wr(seg, hsp, &ttab, rstart, &qtab, qs, ql, rb, k);
+                for (uint32_t iv = 0; iv < iv_calls.size() && r == SA_OK; ++iv) {
+                    std::vector<SaHostCallOut> res;
+                    SaHostRunStats rs;
+                    auto t_calls = std::chrono::steady_clock::now();
+                    r = sa_host_run_calls(iv_calls[iv], Q.text.data() + qs, rc_text[b].data(), b, cfg.num_threads, res,
+                                          &rs);
+                    st.calls_seconds += secs_since(t_calls);
+                    if (r != SA_OK) break;
                     st.num_seeds += rs.num_seeds;
                     st.num_hits += rs.num_hits;
                     st.num_hsps += rs.num_hsps;
-                    st.intervals += niv;
-                    // per interval: plus-strand lists then minus-strand lists, call order
-                    size_t c = 0;
-                    for (uint32_t iv = 0; iv < niv; ++iv) {
-                        std::vector<sa_segment> fw, rc;
-                        for (; c < calls.size() && call_iv[c] == iv; ++c) {
-                            if (!res[c].p) continue;
-                            auto& dst = calls[c].strand ? rc : fw;
-                            dst.insert(dst.end(), res[c].p + 1, res[c].p + 1 + res[c].n);
-                        }
-                        if (hsp) {
-                            for (int sd = 0; sd < 2; ++sd)
-                                for (const sa_segment& h : sd ? rc : fw) {
-                                    const uint32_t key[4] = {rb, k, iv, (uint32_t)sd};
-                                    fwrite(key, 4, 4, hsp);
-                                    fwrite(&h, sizeof h, 1, hsp);
-                                }
-                        }
-                        if (seg && (fw.size() || rc.size())) {
-                            char *pt = nullptr, *mt = nullptr;
-                            uint64_t pl = 0, ml = 0;
-                            int f = sa_format_segments_gpu(&ttab, rstart, &qtab, qs, ql, fw.data(), fw.size(),
-                                                           rc.data(), rc.size(), &pt, &pl, &mt, &ml);
-                            if (f == SA_OK) {
-                                fwrite(pt, 1, pl, seg);
-                                fwrite(mt, 1, ml, seg);
-                            }
-                            sa_free_text(pt);
-                            sa_free_text(mt);
-                            if (f != SA_OK) r = f;
-                        }
-                    }
-                    for (auto& x : res) sa_free_segments(x.p);
+                    r = wr.push(iv, std::move(iv_calls[iv]), std::move(res));
                 }
+                const int w_r = wr.finish(&st.output_seconds);
+                if (r == SA_OK) r = w_r;
+                st.intervals += iv_calls.size();
             }
             {
                 std::lock_guard<std::mutex> lk(mu);
