@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/segalign_b200.h"
+#include "../../include/segalign_b200_host.h"
 
 // One SeedAndFilter call of a seeder: strand 0 seeds query positions
 // [j0, j1) of the block, strand 1 the same positions of its reverse
@@ -45,6 +46,15 @@ int sa_host_kmer_size();
 // >= M, in position order, without a run still open at block_len.
 int sa_device_coverage_runs(const std::vector<std::pair<uint32_t, uint32_t>>& hsps, uint32_t block_len, uint32_t M,
                             std::vector<std::pair<uint32_t, uint32_t>>& runs);
+
+// sa_format_segments_gpu into a pinned host buffer of the caller (*pinned,
+// *cap bytes, reallocated with cudaMallocHost when the text is longer): plus
+// lines at [0, plus_len), minus lines at [plus_len, plus_len + minus_len).
+// Release the buffer with cudaFreeHost.
+int sa_format_segments_pinned(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                              uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw,
+                              uint64_t n_fw, const sa_segment* rc, uint64_t n_rc, char** pinned, uint64_t* cap,
+                              uint64_t* plus_len, uint64_t* minus_len);
 
 // Error state of the API layer (sa_last_error), defined in sa_api.cu.
 void sa_set_error(int code, const char* fmt, ...);

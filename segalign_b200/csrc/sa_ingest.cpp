@@ -20,6 +20,7 @@
 //   * after a '+' line (FASTQ) quality lines are read until they are as long
 //     as the sequence; a missing or mismatched quality ends the input;
 //   * gzip-compressed and plain files are read alike (zlib).
+#include <cuda_runtime.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -217,13 +218,15 @@ double secs_since(std::chrono::steady_clock::time_point t) {
 // in interval order, while the seeders run the next interval: per interval
 // its HSP records {target block, query block, interval, strand, sa_segment}
 // (plus strand first) and the lastz --segments lines of both strands from the
-// GPU segment writer.  Takes ownership of each interval's call outputs.
+// GPU segment writer.  The lines come back into one of two pinned buffers,
+// and a file thread writes a buffer out while the next interval is formatted
+// into the other.  Takes ownership of each interval's call outputs.
 class IntervalWriter {
   public:
     IntervalWriter(FILE* seg, FILE* hsp, const sa_chrom_table* ttab, uint64_t rstart, const sa_chrom_table* qtab,
                    uint64_t qs, uint32_t ql, uint32_t rb, uint32_t qb)
         : seg_(seg), hsp_(hsp), ttab_(ttab), qtab_(qtab), rstart_(rstart), qs_(qs), ql_(ql), rb_(rb), qb_(qb),
-          th_([this] { run(); }) {}
+          file_th_([this] { file_run(); }), th_([this] { run(); }) {}
     ~IntervalWriter() { finish(nullptr); }
 
     // Queues interval iv; returns the writer's first error, if it failed.
@@ -244,6 +247,18 @@ class IntervalWriter {
         cv_.notify_all();
         if (th_.joinable()) {
             th_.join();
+            {
+                std::lock_guard<std::mutex> lk(fmu_);
+                fclosed_ = true;
+            }
+            fcv_.notify_all();
+            file_th_.join();
+            for (char* b : pbuf_)
+                if (b) cudaFreeHost(b);
+            if (err_ == SA_OK && ferr_ != SA_OK) {
+                err_ = ferr_;
+                msg_ = "writing the segments file failed";
+            }
             if (err_ != SA_OK) sa_set_error(err_, "%s", msg_.c_str());
             if (seconds) *seconds += busy_;
         }
@@ -302,21 +317,42 @@ class IntervalWriter {
             }
         }
         if (seg_ && (fw.size() || rc.size())) {
-            char *pt = nullptr, *mt = nullptr;
-            uint64_t pl = 0, ml = 0;
-            const int f = sa_format_segments_gpu(ttab_, rstart_, qtab_, qs_, ql_, fw.data(), fw.size(), rc.data(),
-                                                 rc.size(), &pt, &pl, &mt, &ml);
-            bool ok = f == SA_OK;
-            if (ok) ok = fwrite(pt, 1, pl, seg_) == pl && fwrite(mt, 1, ml, seg_) == ml;
-            sa_free_text(pt);
-            sa_free_text(mt);
-            if (f != SA_OK) return f;
-            if (!ok) {
-                sa_set_error(SA_ERR_ARG, "writing the segments file failed");
-                return SA_ERR_ARG;
+            const int b = next_;
+            next_ ^= 1;
+            {
+                std::unique_lock<std::mutex> lk(fmu_);
+                fcv_.wait(lk, [&] { return !pbusy_[b]; });  // its previous text is on file
+                if (ferr_ != SA_OK) return SA_OK;            // finish() reports the file error
             }
+            uint64_t pl = 0, ml = 0;
+            const int f = sa_format_segments_pinned(ttab_, rstart_, qtab_, qs_, ql_, fw.data(), fw.size(), rc.data(),
+                                                    rc.size(), &pbuf_[b], &pcap_[b], &pl, &ml);
+            if (f != SA_OK) return f;
+            std::lock_guard<std::mutex> lk(fmu_);
+            pbusy_[b] = true;
+            fq_.push_back({b, pl + ml});
+            fcv_.notify_all();
         }
         return SA_OK;
+    }
+
+    // File thread: writes the formatted buffers in the order they were queued.
+    void file_run() {
+        while (true) {
+            std::pair<int, uint64_t> job;
+            {
+                std::unique_lock<std::mutex> lk(fmu_);
+                fcv_.wait(lk, [&] { return fclosed_ || !fq_.empty(); });
+                if (fq_.empty()) return;
+                job = fq_.front();
+                fq_.pop_front();
+            }
+            const bool ok = ferr_ == SA_OK && fwrite(pbuf_[job.first], 1, job.second, seg_) == job.second;
+            std::lock_guard<std::mutex> lk(fmu_);
+            if (!ok && ferr_ == SA_OK) ferr_ = SA_ERR_ARG;
+            pbusy_[job.first] = false;
+            fcv_.notify_all();
+        }
     }
 
     FILE* seg_;
@@ -332,6 +368,17 @@ class IntervalWriter {
     int err_ = SA_OK;
     std::string msg_;
     double busy_ = 0;
+    // pinned text buffers and the file thread's queue of (buffer, bytes)
+    char* pbuf_[2] = {nullptr, nullptr};
+    uint64_t pcap_[2] = {0, 0};
+    bool pbusy_[2] = {false, false};
+    int next_ = 0;
+    std::mutex fmu_;
+    std::condition_variable fcv_;
+    std::deque<std::pair<int, uint64_t>> fq_;
+    bool fclosed_ = false;
+    int ferr_ = SA_OK;
+    std::thread file_th_;
     std::thread th_;  // last: starts once the members above are set
 };
 

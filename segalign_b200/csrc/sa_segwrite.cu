@@ -212,13 +212,16 @@ int dev_copy(const T* src, uint64_t n, T** dst, cudaStream_t st) {
 
 }  // namespace
 
-extern "C" int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_block_start,
-                                      const sa_chrom_table* query, uint64_t query_block_start,
-                                      uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
-                                      const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len,
-                                      char** minus_text, uint64_t* minus_len) {
-    if (!ref || !query || !ref->count || !query->count || (n_fw && !fw) || (n_rc && !rc) || !plus_text ||
-        !plus_len || !minus_text || !minus_len)
+// The writer.  With `pin` the text (plus lines, then minus lines) goes into
+// the caller's pinned buffer *pin, reallocated when it holds fewer than the
+// text's bytes (*pin_cap), and plus_text / minus_text are not set; without
+// it, into two malloc'd strings.
+static int seg_format(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                      uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
+                      const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len, char** minus_text,
+                      uint64_t* minus_len, char** pin, uint64_t* pin_cap) {
+    if (!ref || !query || !ref->count || !query->count || (n_fw && !fw) || (n_rc && !rc) || !plus_len ||
+        !minus_len || (pin ? !pin_cap : (!plus_text || !minus_text)))
         return SA_ERR_ARG;
     // reverse-complement chromosome table of the block (src/main.cpp:355-362),
     // as the host writer builds it
@@ -235,9 +238,10 @@ extern "C" int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_bl
         hc.idx.push_back(i);
     }
     if (hc.starts.empty()) return SA_ERR_ARG;
-    *plus_text = *minus_text = nullptr;
     *plus_len = *minus_len = 0;
     const uint64_t n = n_fw + n_rc;
+    if (pin && n == 0) return SA_OK;
+    if (!pin) *plus_text = *minus_text = nullptr;
     if (n == 0) {
         *plus_text = (char*)calloc(1, 1);
         *minus_text = (char*)calloc(1, 1);
@@ -330,6 +334,27 @@ extern "C" int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_bl
             rcode = SA_ERR_CUDA;
             break;
         }
+        if (pin) {
+            if (*pin_cap < total) {
+                if (*pin) cudaFreeHost(*pin);
+                *pin = nullptr;
+                *pin_cap = 0;
+                if (cudaMallocHost(pin, total) != cudaSuccess) {
+                    *pin = nullptr;
+                    rcode = SA_ERR_NOMEM;
+                    break;
+                }
+                *pin_cap = total;
+            }
+            if (cudaMemcpyAsync(*pin, text, total, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess) {
+                rcode = SA_ERR_CUDA;
+                break;
+            }
+            *plus_len = split;
+            *minus_len = total - split;
+            break;
+        }
         text_h = (char*)malloc(total + 1);
         char* minus_h = (char*)malloc(total - split + 1);
         if (!text_h || !minus_h) {
@@ -357,5 +382,23 @@ extern "C" int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_bl
         if (p) cudaFreeAsync(p, st);
     cudaStreamSynchronize(st);
     if (rcode == SA_ERR_CUDA) sa_set_error(SA_ERR_CUDA, "segment writer: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rcode == SA_ERR_NOMEM) sa_set_error(SA_ERR_NOMEM, "segment writer: host allocation failed");
     return rcode;
+}
+
+extern "C" int sa_format_segments_gpu(const sa_chrom_table* ref, uint64_t ref_block_start,
+                                      const sa_chrom_table* query, uint64_t query_block_start,
+                                      uint32_t query_block_len, const sa_segment* fw, uint64_t n_fw,
+                                      const sa_segment* rc, uint64_t n_rc, char** plus_text, uint64_t* plus_len,
+                                      char** minus_text, uint64_t* minus_len) {
+    return seg_format(ref, ref_block_start, query, query_block_start, query_block_len, fw, n_fw, rc, n_rc, plus_text,
+                      plus_len, minus_text, minus_len, nullptr, nullptr);
+}
+
+int sa_format_segments_pinned(const sa_chrom_table* ref, uint64_t ref_block_start, const sa_chrom_table* query,
+                              uint64_t query_block_start, uint32_t query_block_len, const sa_segment* fw,
+                              uint64_t n_fw, const sa_segment* rc, uint64_t n_rc, char** pinned, uint64_t* cap,
+                              uint64_t* plus_len, uint64_t* minus_len) {
+    return seg_format(ref, ref_block_start, query, query_block_start, query_block_len, fw, n_fw, rc, n_rc, nullptr,
+                      plus_len, nullptr, minus_len, pinned, cap);
 }
