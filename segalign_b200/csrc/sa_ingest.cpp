@@ -327,11 +327,35 @@ class IntervalWriter {
             uint64_t pl = 0, ml = 0;
             const int f = sa_format_segments_pinned(ttab_, rstart_, qtab_, qs_, ql_, fw.data(), fw.size(), rc.data(),
                                                     rc.size(), &pbuf_[b], &pcap_[b], &pl, &ml);
+            if (f == SA_ERR_NOMEM) return write_unpinned(fw, rc);
             if (f != SA_OK) return f;
             std::lock_guard<std::mutex> lk(fmu_);
             pbusy_[b] = true;
             fq_.push_back({b, pl + ml});
             fcv_.notify_all();
+        }
+        return SA_OK;
+    }
+
+    // An interval whose text does not fit in pinned memory: formatted into
+    // ordinary host memory and written here, after the queued buffers.
+    int write_unpinned(const std::vector<sa_segment>& fw, const std::vector<sa_segment>& rc) {
+        {
+            std::unique_lock<std::mutex> lk(fmu_);
+            fcv_.wait(lk, [&] { return fq_.empty() && !pbusy_[0] && !pbusy_[1]; });
+            if (ferr_ != SA_OK) return SA_OK;  // finish() reports the file error
+        }
+        char *pt = nullptr, *mt = nullptr;
+        uint64_t pl = 0, ml = 0;
+        const int f = sa_format_segments_gpu(ttab_, rstart_, qtab_, qs_, ql_, fw.data(), fw.size(), rc.data(), rc.size(),
+                                             &pt, &pl, &mt, &ml);
+        const bool ok = f == SA_OK && fwrite(pt, 1, pl, seg_) == pl && fwrite(mt, 1, ml, seg_) == ml;
+        sa_free_text(pt);
+        sa_free_text(mt);
+        if (f != SA_OK) return f;
+        if (!ok) {
+            sa_set_error(SA_ERR_ARG, "writing the segments file failed");
+            return SA_ERR_ARG;
         }
         return SA_OK;
     }

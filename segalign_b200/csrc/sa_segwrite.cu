@@ -340,6 +340,7 @@ static int seg_format(const sa_chrom_table* ref, uint64_t ref_block_start, const
                 *pin = nullptr;
                 *pin_cap = 0;
                 if (cudaMallocHost(pin, total) != cudaSuccess) {
+                    cudaGetLastError();  // an allocation failure is reported, not left pending
                     *pin = nullptr;
                     rcode = SA_ERR_NOMEM;
                     break;
