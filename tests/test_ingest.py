@@ -66,6 +66,35 @@ def _read_hsps(path):
     return keys, recs
 
 
+@pytest.mark.parametrize("crlf,gz", [(False, False), (True, False), (True, True)])
+def test_fasta_long_lines_across_read_buffers(built, tmp_path, crlf, gz):
+    """Lines of one base up to 1.5 Mbp, so that lines (and their CRLF pairs)
+    start, end and break at many offsets of the reader's 1 MiB buffers, which
+    it appends a span at a time; empty lines and records of one line.  Blocks
+    equal the restatement's."""
+    rng = np.random.default_rng(17 + crlf + 2 * gz)
+    nl = b"\r\n" if crlf else b"\n"
+    alph = np.frombuffer(b"ACGTacgtN", dtype=np.uint8)
+    out = []
+    for k in range(9):
+        out.append(b">r%d comment" % k + nl)
+        for _ in range(int(rng.integers(1, 6))):
+            n = int(rng.choice([1, 2, int(rng.integers(3, 5000)), int(rng.integers(200_000, 1_500_000))]))
+            out.append(rng.choice(alph, size=n).tobytes() + nl)
+            if rng.random() < 0.3:
+                out.append(nl)
+    data = b"".join(out)
+    assert len(data) > 2 * (1 << 20)
+    path = tmp_path / ("long.fa.gz" if gz else "long.fa")
+    path.write_bytes(gzip.compress(data, compresslevel=1) if gz else data)
+    for bs in (1_000_000, 500_000_000):
+        got = fasta_load(str(path), bs)
+        text, chroms, blocks = oracle.fasta_blocks(data, bs)
+        assert got["text"] == text, bs
+        assert got["chroms"] == chroms, bs
+        assert got["blocks"] == blocks, bs
+
+
 @pytest.mark.gpu
 def test_align_fasta_two_blocks_matches_oracle(built, tmp_path):
     rng = np.random.default_rng(11)
