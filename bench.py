@@ -21,7 +21,8 @@ One step = one pass of the hot path over the whole query (both strands):
   e2e_batched  host query text -> GPU -> batched call -> HSP lists on the host.
 Beside them: like-for-like batched/plain ratios, uneven windows, serving on
 the resident table, an unranked timing of the reference's own kernels on a
-sample of the same units, the CPU port on a bounded sample, and the 600 Mbp
+sample of the same units, the CPU port on a bounded sample, the same workload
+as FASTA files through sa_align_fasta to a segments file, and the 600 Mbp
 legs (batched and plain with transitions, serving on that table, repeat-masker
 self-alignment).  Ranks (torchrun) run one job: the target is replicated to
 every GPU and the query is split, with no collective on the data path.  By
