@@ -485,6 +485,7 @@ int launch_call_chain(Slot* s, int mode, PhaseTimer& tm) {
     xa.xdrop = g.params.xdrop;
     xa.hspthresh = g.params.hspthresh;
     xa.noentropy = g.params.noentropy;
+    xa.windowed = mode == 1 ? 1 : 0;
     sa_launch_extend_lane(w, xa, g.params, cg.lane_tuning, d.num_sms, st, cg.lane_ctas);
     tm.mark(2);
     sa_launch_extend_warp(w, xa, g.params, g.tuning, d.num_sms, st);

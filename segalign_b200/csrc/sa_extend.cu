@@ -48,6 +48,7 @@ struct SaExtK {
     uint32_t tile_hits;
     uint32_t substeps;  // steps per lane-kernel iteration (at most)
     uint32_t switch_now;  // 1: a lane starts its left side in the step after its right side ends
+    uint32_t windowed;    // 1: hits outside their unit's rm window are dropped from the tiles
 };
 
 // Reverse the order of the 8 nibbles of a word.
@@ -354,12 +355,13 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                     exhausted = true;
                     tile_n = tile_pos = 0;
                 } else {
-                    const uint32_t n = (uint32_t)min((unsigned long long)TILE, H - t0);
+                    uint32_t n = (uint32_t)min((unsigned long long)TILE, H - t0);
                     const uint64_t c0 = sa_warp_find_seed(a.cs.E, nnz, t0);
                     const uint32_t nw = (uint32_t)min((uint64_t)n, nnz - c0);  // seeds of the window
                     for (uint32_t i = lane; i <= nw; i += 32) s_E[i] = a.cs.E[c0 + i];  // E[nnz] == H
                     __syncwarp();
-                    for (uint32_t i = lane; i < n; i += 32) {
+                    // record of hit t0 + i: its seed by binary search in the E window
+                    auto record = [&](uint32_t i) {
                         const unsigned long long h = t0 + i;
                         uint32_t lo = 0, hi = nw;  // last k in [0, nw) with E[c0+k] <= h
                         while (hi - lo > 1) {
@@ -373,7 +375,31 @@ sa_k_extend_lane(SaExtK a, SaParams P) {
                         r.y = a.cs.qpos[c] + a.seed_size;                                                 // find_hits :176
                         r.z = a.cs.scope[c];
                         r.w = a.cs.unit[c];
-                        s_hits[i] = r;
+                        return r;
+                    };
+                    if (!a.windowed) {
+                        for (uint32_t i = lane; i < n; i += 32) s_hits[i] = record(i);
+                    } else {
+                        // rm: hits outside [ref_start, ref_end] are never extended
+                        // (repeat_masker_src/seed_filter.cu:237-243, 304-333); the
+                        // tile keeps only the others, in order, so that no lane is
+                        // handed a hit it would skip.  Coordinates past either
+                        // sequence end are rejected here too.
+                        uint32_t kept = 0;
+                        for (uint32_t i0 = 0; i0 < n; i0 += 32) {
+                            bool live = false;
+                            uint4 r = make_uint4(0, 0, 0, 0);
+                            if (i0 + lane < n) {
+                                r = record(i0 + lane);
+                                const SaUnit U = a.units[r.w];
+                                live = !(U.flags & 1u) || (r.x >= U.rm_lo && r.x <= U.rm_hi);
+                                if (!live && (r.x > a.ref_len || r.y > U.q_len)) atomicCAS(&a.ctr->error, 0ull, 5ull);
+                            }
+                            const uint32_t m = __ballot_sync(SA_FULL, live);
+                            if (live) s_hits[kept + __popc(m & lt)] = r;
+                            kept += __popc(m);
+                        }
+                        n = kept;
                     }
                     __syncwarp();
                     tile_n = n;
@@ -808,6 +834,7 @@ static SaExtK sa_ext_args(SaWork& w, const SaExtendArgs& x, const SaTuning& t) {
     a.tile_hits = (uint32_t)t.tile_hits;
     a.substeps = (uint32_t)t.substeps;
     a.switch_now = t.switch_now ? 1u : 0u;
+    a.windowed = x.windowed ? 1u : 0u;
     return a;
 }
 

@@ -175,6 +175,9 @@ struct SaExtendArgs {
     const uint32_t* pos_table;
     uint32_t seed_size;
     int32_t xdrop, hspthresh, noentropy;
+    // 1: units may restrict their hits to a target window (repeat-masker
+    // calls); the lane kernel drops the others when it expands a tile
+    int32_t windowed = 0;
 };
 // Phase A (lane per hit) and phase B (warp per long hit); B must follow A.
 // grid: CTAs of the persistent launch (0: num_sms x ext_ctas_per_sm).
