@@ -21,6 +21,7 @@
 //     as the sequence; a missing or mismatched quality ends the input;
 //   * gzip-compressed and plain files are read alike (zlib).
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 #include <zlib.h>
 
 #include <algorithm>
@@ -51,8 +52,11 @@ class FastaReader {
     }
     bool ok() const { return f_ != nullptr; }
 
-    // Next record; false at the end of the input (or on a truncated FASTQ record).
-    bool next(std::string& name, std::string& seq) {
+    // Next record: its name, and its sequence appended to `out`; false at the
+    // end of the input (or on a truncated FASTQ record, whose bases are then
+    // taken off `out` again).
+    bool next(std::string& name, std::string& out) {
+        const size_t st = out.size();
         int c;
         if (!pending_) {  // skip to the next header character
             while ((c = getc()) >= 0 && c != '>' && c != '@') {
@@ -61,7 +65,6 @@ class FastaReader {
         }
         pending_ = false;
         name.clear();
-        seq.clear();
         // name: up to the first white space
         bool any = false;
         while ((c = getc()) >= 0 && !std::isspace(c)) {
@@ -75,30 +78,34 @@ class FastaReader {
         // sequence lines
         while ((c = getc()) >= 0 && c != '>' && c != '+' && c != '@') {
             if (c == '\n') continue;
-            seq.push_back((char)c);
-            append_line(seq);
-            if (seq.size() > 1 && seq.back() == '\r') seq.pop_back();
+            out.push_back((char)c);
+            append_line(out);
+            if (out.size() - st > 1 && out.back() == '\r') out.pop_back();
         }
         if (c == '>' || c == '@') pending_ = true;
         if (c != '+') return true;
         // FASTQ quality: skip the '+' line, then quality lines up to the sequence length
+        const size_t n = out.size() - st;
         while ((c = getc()) >= 0 && c != '\n') {
         }
-        if (c < 0) return false;
         size_t ql = 0;
-        while (ql < seq.size()) {
-            size_t line = 0;
-            int d;
-            bool got = false;
-            while ((d = getc()) >= 0 && d != '\n') {
-                ++line;
-                got = true;
+        if (c >= 0) {
+            while (ql < n) {
+                size_t line = 0;
+                int d;
+                bool got = false;
+                while ((d = getc()) >= 0 && d != '\n') {
+                    ++line;
+                    got = true;
+                }
+                if (!got && d < 0) break;
+                ql += line;
+                if (d < 0) break;
             }
-            if (!got && d < 0) break;
-            ql += line;
-            if (d < 0) break;
         }
-        return ql == seq.size();
+        if (c >= 0 && ql == n) return true;
+        out.resize(st);
+        return false;
     }
 
   private:
@@ -160,15 +167,21 @@ int load_fasta(const char* path, uint64_t block_size, SeqSetImpl& s) {
         sa_set_error(SA_ERR_ARG, "cannot open FASTA file %s", path);
         return SA_ERR_ARG;
     }
-    std::string name, seq;
+    {
+        struct stat sb;
+        if (stat(path, &sb) == 0 && sb.st_size > 0) s.text.reserve((size_t)sb.st_size + 16);
+    }
+    std::string name;
     uint64_t blk_len = 0;
     s.block_start.push_back(0);
-    while (rd.next(name, seq)) {
+    while (true) {
+        const size_t at = s.text.size();
+        if (!rd.next(name, s.text)) break;  // records are read straight into the joined text
+        const uint64_t len = s.text.size() - at;
         s.names.push_back(name);
-        s.chrom_start.push_back(s.text.size());
-        s.chrom_len.push_back((uint32_t)seq.size());
-        s.text += seq;
-        blk_len += seq.size();
+        s.chrom_start.push_back(at);
+        s.chrom_len.push_back((uint32_t)len);
+        blk_len += len;
         if (blk_len > block_size) {
             s.block_len.push_back((uint32_t)blk_len);
             s.block_start.push_back(s.text.size());

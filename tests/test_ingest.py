@@ -95,6 +95,20 @@ def test_fasta_long_lines_across_read_buffers(built, tmp_path, crlf, gz):
         assert got["blocks"] == blocks, bs
 
 
+def test_fastq_records_known_answers(built, tmp_path):
+    """kseq's FASTQ rules, worked out by hand: a '+' line ends the sequence,
+    quality lines are read until they are as long as it, and a record whose
+    quality runs out first ends the input without being kept; records are
+    joined with '&' as FASTA records are."""
+    data = b"@r1 c\nACG\nT\n+\nII\nII\n@r2\nGG\n+r2\nII\n>r3\nTTA\n@r4\nACGTACGT\n+\nIII\n"
+    path = tmp_path / "x.fq"
+    path.write_bytes(data)
+    got = fasta_load(str(path), 500_000_000)
+    assert got["text"][:got["blocks"][0][1]] == b"ACGT&GG&TTA"
+    assert got["chroms"] == [("r1", 0, 4), ("r2", 5, 2), ("r3", 8, 3)]
+    assert got["blocks"] == [(0, 11)]
+
+
 @pytest.mark.gpu
 def test_align_fasta_two_blocks_matches_oracle(built, tmp_path):
     rng = np.random.default_rng(11)
