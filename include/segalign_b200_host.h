@@ -174,8 +174,9 @@ void sa_seq_set_free(sa_seq_set* s);
  * block k - 1 from the other buffer.  Each query block is cut into intervals
  * of interval_size over [0, len - seed_size) and each interval into chunk_size
  * SeedAndFilter calls per strand (src/seeder.cpp:47-121).  Per interval, the
- * lastz --segments lines of its HSPs (sa_format_segments: plus strand, then
- * minus) go to segments_path, and its HSP records to hsp_path as
+ * lastz --segments lines of its HSPs (plus strand, then minus; the text
+ * sa_format_segments gives, written by the GPU segment writer) go to
+ * segments_path, and its HSP records to hsp_path as
  * {u32 target block, u32 query block, u32 interval, u32 strand, sa_segment};
  * a writer thread puts out interval i while the seeders run interval i + 1. 
  * Needs sa_initialize_interface, sa_generate_shape_pos, sa_host_set_shape and
